@@ -1,0 +1,15 @@
+// Stand-in for escript::AbstractSystemMatrix: a CSR matrix view the shim domain
+// scatters element matrices into (see ref_driver.cpp).
+#pragma once
+namespace escript {
+class AbstractSystemMatrix {
+public:
+    virtual ~AbstractSystemMatrix() {}
+    int getRowBlockSize() const { return 1; }
+    int getColumnBlockSize() const { return 1; }
+    const int* ptr = nullptr;
+    const int* idx = nullptr;
+    double* val = nullptr;
+    long n = 0;
+};
+}  // namespace escript
