@@ -1,0 +1,472 @@
+#!/usr/bin/env python
+"""Time-to-solution benchmark of the ripley/paso hot path on B200.
+
+Workload (one step = one pass of the hot path over one synthetic input): ripley Brick
+128^3 Q1 elements on [0,1]^3, A = kappa*I with kappa = exp(g), g a Gaussian random field
+(white noise smoothed with a Gaussian of 8 cells, standardised, periodic), Y = sum of 4
+Gaussian blobs (width 3 cells, amplitudes U(-1,1), centres uniform) at the Gauss points,
+u = 0 on the top face z = 1, PCG + Jacobi to relative residual 1e-8.  A step is: reset
+the matrix, assemble A and Y, insert the Dirichlet constraint, solve.  The timed path is
+the FP32-inner / FP64-refinement PCG on the band layout; the plain FP64 paso PCG on the
+CSR matrix (the reference algorithm) is timed beside it on the same input.
+
+Usage (driver contract):
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+N>1 runs as one process per GPU under torch.distributed.run; every rank solves its
+own independent instance (weak scaling, no collective on the data path).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+PKG_DIR = os.path.join(REPO, "esys-escript.github.io_b200")
+for p in (PKG_DIR, REPO):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+METRIC = "time-to-1e-8 residual, Brick 128^3: learned+FP32 refine vs plain FP64 PCG, B200"
+RTOL = 1e-8
+
+
+# ----------------------------------------------------------------------------------------------
+# synthetic inputs (seeded)
+# ----------------------------------------------------------------------------------------------
+
+def make_inputs(ne: int, seed: int, corr_cells: float):
+    """kappa per element (element order k0 + NE k1 + NE^2 k2), Y at the Gauss points
+    (NE^3 x 8, q x-fastest) and the Dirichlet mask of the top face."""
+    from scipy.ndimage import gaussian_filter
+    rng = np.random.default_rng(seed)
+    g = gaussian_filter(rng.standard_normal((ne, ne, ne)), sigma=corr_cells, mode="wrap")
+    g = (g - g.mean()) / g.std()
+    kappa = np.exp(g).reshape(-1)
+    h = 1.0 / ne
+    gp = np.array([0.5 - np.sqrt(3) / 6, 0.5 + np.sqrt(3) / 6])
+    axis = (np.arange(ne)[:, None] + gp[None, :]) * h  # (NE, 2) Gauss coordinates
+    amps = rng.uniform(-1.0, 1.0, 4)
+    centres = rng.uniform(0.0, 1.0, (4, 3))
+    w = 3.0 * h
+    Y = np.zeros((ne, ne, ne, 2, 2, 2))  # (k2, k1, k0, qz, qy, qx)
+    for a, c in zip(amps, centres):
+        f = [np.exp(-((axis - c[d]) ** 2) / (2 * w * w)) for d in range(3)]
+        Y += a * (f[2][:, None, None, :, None, None] * f[1][None, :, None, None, :, None] *
+                  f[0][None, None, :, None, None, :])
+    nn = ne + 1
+    q = np.zeros(nn ** 3)
+    q[(nn - 1) * nn * nn:] = 1.0
+    return {"kappa": kappa, "Y": Y.reshape(-1), "q": q, "ne": ne, "seed": seed,
+            "amps": amps.tolist(), "centres": centres.tolist()}
+
+
+# ----------------------------------------------------------------------------------------------
+# clocks during the timed region
+# ----------------------------------------------------------------------------------------------
+
+class ClockSampler:
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id: str | None):
+        self.gpu_id = gpu_id
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200"]
+        if self.gpu_id:
+            cmd += ["-i", self.gpu_id]
+        try:
+            self.proc = subprocess.Popen(cmd, stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 8:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[0]) for r in rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows for n, v in zip(names, r[4:8]) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ----------------------------------------------------------------------------------------------
+# CPU baseline: the reference's own assembler + paso solver (oracle/_ref), else the oracle port
+# ----------------------------------------------------------------------------------------------
+
+def cpu_reference_sample(inp, n_iter_full: int | None, threads: int):
+    """Times, on the host cores, the reference's assembly of the full input, the constraint,
+    and paso's solve for 10 and for 40 iterations; the time-to-solution is extrapolated as
+    assemble + constrain + setup + n_iter * (time per iteration).  Returns a dict."""
+    from oracle import oracle as O
+    ne = inp["ne"]
+    nel = ne ** 3
+    kind = "reference" if O.have_ref() else "port"
+    use_ref = kind == "reference"
+    if use_ref:
+        O.set_threads(threads)
+    else:
+        os.environ["OMP_NUM_THREADS"] = str(threads)
+    A = np.zeros((nel, 8, 3, 3))
+    for i in range(3):
+        A[:, :, i, i] = inp["kappa"][:, None]
+    A = A.reshape(-1)
+    pat = O.pattern(3, (ne, ne, ne))
+    t0 = time.perf_counter()
+    val, rhs = O.assemble(3, (ne, ne, ne), [1.0 / ne] * 3, pat, A=(O.EXPANDED, A),
+                          Y=(O.EXPANDED, inp["Y"]), use_ref=use_ref)
+    t1 = time.perf_counter()
+    O.insert_constraint(pat, val, rhs, inp["q"])
+    t2 = time.perf_counter()
+    times = {}
+    for its in (10, 40):
+        v = val.copy()
+        s0 = time.perf_counter()
+        r = O.solve_paso(pat, v, rhs, tol=RTOL, iter_max=its, use_ref=use_ref)
+        times[its] = (time.perf_counter() - s0, r.num_iter)
+    (ta, ia), (tb, ib) = times[10], times[40]
+    per_iter = (tb - ta) / max(ib - ia, 1)
+    setup = ta - ia * per_iter
+    out = {"assemble_s": t1 - t0, "constraint_s": t2 - t1, "setup_s": setup, "per_iter_s": per_iter,
+           "kind": kind, "cores": threads}
+    if n_iter_full:
+        out["time_to_solution_s"] = (t1 - t0) + (t2 - t1) + setup + n_iter_full * per_iter
+    return out
+
+
+def cpu_full_reference_iterations(inp, threads):
+    """One complete paso solve with the reference code (gives paso's iteration count)."""
+    from oracle import oracle as O
+    ne = inp["ne"]
+    nel = ne ** 3
+    use_ref = O.have_ref()
+    if use_ref:
+        O.set_threads(threads)
+    A = np.zeros((nel, 8, 3, 3))
+    for i in range(3):
+        A[:, :, i, i] = inp["kappa"][:, None]
+    pat = O.pattern(3, (ne, ne, ne))
+    val, rhs = O.assemble(3, (ne, ne, ne), [1.0 / ne] * 3, pat, A=(O.EXPANDED, A.reshape(-1)),
+                          Y=(O.EXPANDED, inp["Y"]), use_ref=use_ref)
+    O.insert_constraint(pat, val, rhs, inp["q"])
+    t0 = time.perf_counter()
+    r = O.solve_paso(pat, val, rhs, tol=RTOL, use_ref=use_ref)
+    return r.num_iter, time.perf_counter() - t0
+
+
+# ----------------------------------------------------------------------------------------------
+# our arm
+# ----------------------------------------------------------------------------------------------
+
+# algorithmic bytes per launch of the dominant kernel, per DOF (n): the FP32 band SpMV reads
+# 27 band values (4 B each, padded bands count) + z and p_old, and writes p_new and q
+F32_SPMV_BYTES_PER_ROW = 27 * 4 + 4 * 4
+
+
+def run_ours(args):
+    import ctypes as C
+    import torch
+    from esys_b200 import _lib as L
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    lib = L.lib()
+    ne = args.ne
+    inp = make_inputs(ne, args.seed + rank, 8.0 * ne / 128.0)
+    nel = ne ** 3
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream()
+    L.set_stream_from_torch()
+
+    # device-resident inputs: A per element (kappa*I, 9 values), Y at the Gauss points, q
+    A_pe = np.zeros((nel, 3, 3))
+    for i in range(3):
+        A_pe[:, i, i] = inp["kappa"]
+    A_host = torch.from_numpy(A_pe.reshape(-1)).pin_memory()
+    Y_host = torch.from_numpy(inp["Y"]).pin_memory()
+    q_host = torch.from_numpy(inp["q"]).pin_memory()
+    A_d = A_host.to(dev)
+    Y_d = Y_host.to(dev)
+    q_d = q_host.to(dev)
+
+    dom = C.c_void_p()
+    ne3 = (C.c_int64 * 3)(ne, ne, ne)
+    L.check(lib.rg_domain_create(3, ne3, (C.c_double * 3)(0, 0, 0), (C.c_double * 3)(1, 1, 1), C.byref(dom)))
+    n, nnz = C.c_int64(), C.c_int64()
+    L.check(lib.rg_domain_info(dom, C.byref(n), C.byref(nnz), None, None, None))
+    n, nnz = n.value, nnz.value
+    mat = C.c_void_p()
+    L.check(lib.rg_matrix_create(dom, C.byref(mat)))
+    rhs = torch.zeros(n, dtype=torch.float64, device=dev)
+    x = torch.zeros(n, dtype=torch.float64, device=dev)
+
+    def opts(mode, precision, tol=RTOL):
+        o = L.rg_solver_opts()
+        lib.rg_solver_opts_default(C.byref(o))
+        o.tolerance = tol
+        o.mode = mode
+        o.precision = precision
+        o.layout = L.RG_LAYOUT_BAND if precision == L.RG_PREC_FP32_REFINE else L.RG_LAYOUT_CSR
+        return o
+
+    fast = opts(L.RG_MODE_STANDARD, L.RG_PREC_FP32_REFINE)
+    plain = opts(L.RG_MODE_PASO, L.RG_PREC_FP64)
+    empty = L.rg_coef(None, 0)
+    cA = L.rg_coef(A_d.data_ptr(), L.RG_COEF_PER_ELEMENT)
+    cY = L.rg_coef(Y_d.data_ptr(), L.RG_COEF_EXPANDED)
+
+    def step(o, A_dev=None, Y_dev=None, q_dev=None):
+        ca = cA if A_dev is None else L.rg_coef(A_dev.data_ptr(), L.RG_COEF_PER_ELEMENT)
+        cy = cY if Y_dev is None else L.rg_coef(Y_dev.data_ptr(), L.RG_COEF_EXPANDED)
+        qq = q_d if q_dev is None else q_dev
+        L.check(lib.rg_matrix_reset(mat))
+        rhs.zero_()
+        L.check(lib.rg_assemble_single(mat, C.c_void_p(rhs.data_ptr()), C.byref(ca), C.byref(empty),
+                                       C.byref(empty), C.byref(empty), C.byref(empty), C.byref(cy)))
+        L.check(lib.rg_insert_constraint(mat, C.c_void_p(rhs.data_ptr()), C.c_void_p(qq.data_ptr()), None, 0))
+        d = L.rg_diag()
+        L.check(lib.rg_solve(mat, C.c_void_p(rhs.data_ptr()), C.c_void_p(x.data_ptr()), C.byref(o), C.byref(d)))
+        return d
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(v):
+        if dist is None:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # --- FP64 reference solution for the error statement (paso algorithm, rtol 1e-10)
+    step(opts(L.RG_MODE_PASO, L.RG_PREC_FP64, 1e-10))
+    x_fp64 = x.clone()
+
+    # --- plain FP64 paso PCG (the reference algorithm) on the same input
+    d_plain = step(plain)
+    plain_iters = int(d_plain.num_iter)
+    barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    n_plain = max(2, min(args.steps, 3))
+    ev0.record(stream)
+    for _ in range(n_plain):
+        d_plain = step(plain)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    plain_ms = max_over_ranks(ev0.elapsed_time(ev1) / n_plain)
+
+    # --- warm-up of the timed path
+    for _ in range(args.warmup):
+        step(fast)
+    barrier()
+
+    # --- timed region: K steps of the fast path, timers on
+    gpu_id = None
+    try:
+        import torch.cuda as tc
+        gpu_id = "GPU-" + str(tc.get_device_properties(local).uuid)
+    except Exception:
+        gpu_id = None
+    clocks = ClockSampler(gpu_id)
+    lib.rg_timers_reset()
+    lib.rg_timers_enable(1)
+    clocks.start()
+    barrier()
+    ev0.record(stream)
+    for _ in range(args.steps):
+        d_fast = step(fast)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    lib.rg_timers_enable(0)
+    ms = max_over_ranks(ev0.elapsed_time(ev1) / args.steps)
+    tm = L.timers()
+    launches = int(sum(v[0] for v in tm.values()))
+    x_fast = x.clone()
+    err = float((x_fast - x_fp64).norm() / x_fp64.norm())
+
+    # dominant kernel: FP32 band SpMV (+ dot); average launch time from the live events
+    spmv_n, spmv_t, spmv_ms = tm["f32_spmv"]
+    avg_s = spmv_ms / max(spmv_t, 1) / 1e3
+    algo_bytes = F32_SPMV_BYTES_PER_ROW * n
+    peaks = {}
+    pk_path = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(pk_path):
+        peaks = json.load(open(pk_path))
+    hbm = peaks.get("hbm_gbs")
+    peak_note = "of measured" if hbm else "of fallback"
+    hbm = hbm or 6650.0
+    achieved = algo_bytes / avg_s / 1e9 if avg_s > 0 else 0.0
+    traffic = None
+    tr_path = os.path.join(REPO, "profiles", "traffic.json")
+    if os.path.exists(tr_path):
+        tr = json.load(open(tr_path)).get("f32_spmv")
+        if tr and tr.get("ne") == ne:
+            traffic = tr.get("bytes_per_launch")
+    roofline = {"bound": "hbm", "kernel": "k_f32_spmv<27> (FP32 27-band SpMV + p update + p.q)",
+                "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
+                "frac": round(achieved / hbm, 4), "peak_source": peak_note,
+                "algorithmic_bytes_per_launch": algo_bytes, "avg_launch_us": round(avg_s * 1e6, 2),
+                "traffic": traffic}
+
+    # --- end to end through the C-ABI with host buffers (pinned), copies inside the timed region
+    bi = A_host.numel() * 8 + Y_host.numel() * 8 + q_host.numel() * 8
+    bo = n * 8
+    x_host = torch.empty(n, dtype=torch.float64).pin_memory()
+    A_e = torch.empty_like(A_d)
+    Y_e = torch.empty_like(Y_d)
+    q_e = torch.empty_like(q_d)
+    barrier()
+    ev0.record(stream)
+    for _ in range(args.steps):
+        A_e.copy_(A_host, non_blocking=True)
+        Y_e.copy_(Y_host, non_blocking=True)
+        q_e.copy_(q_host, non_blocking=True)
+        step(fast, A_e, Y_e, q_e)
+        x_host.copy_(x, non_blocking=True)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(ev0.elapsed_time(ev1) / args.steps)
+
+    # --- CPU baseline (rank 0, one GPU): the reference's own code on a bounded sample
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        threads = os.cpu_count() or 1
+        s = cpu_reference_sample(inp, plain_iters, threads)
+        cpu = {"value": round(s["time_to_solution_s"] * 1e3, 1), "unit": "ms", "cores": threads,
+               "kind": s["kind"],
+               "sample": (f"reference DefaultAssembler3D + insertConstraint on the full {ne}^3 input, "
+                          f"paso Solver/PCG run for 10 and 40 iterations; time-to-solution = "
+                          f"assemble + constrain + setup + {plain_iters} (GPU paso iteration count) "
+                          f"x {s['per_iter_s'] * 1e3:.2f} ms/iteration"),
+               "assemble_s": round(s["assemble_s"], 3), "per_iter_ms": round(s["per_iter_s"] * 1e3, 3)}
+
+    kernels = {k: {"launches": v[0], "ms": round(v[2], 3)} for k, v in tm.items() if v[0]}
+    out = {
+        "metric": METRIC, "value": round(ms, 3), "unit": "ms", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 inner / f64 refine",
+        "data": "synthetic, seeded: kappa=exp(GRF corr 8 cells, std 1), 4 Gaussian blobs",
+        "config": {"workload": f"Brick {ne}^3 variable-coefficient Poisson, u=0 on top face, "
+                               f"PCG+Jacobi rtol {RTOL:g} (assemble+constrain+solve per step)",
+                   "ne": [ne, ne, ne], "n_dof": n, "nnz": nnz, "seed": args.seed,
+                   "path": "FP32 27-band inner PCG, FP64 CSR outer residual/update (no learned guess yet)",
+                   "l2": "inputs larger than L2 (FP64 CSR values 456 MB, band copy 232 MB per step)",
+                   "parallelism": f"{world} independent replicas" if world > 1 else "1 GPU"},
+        "iterations": int(d_fast.num_iter), "outer_steps": int(d_fast.num_outer),
+        "rel_residual": float(d_fast.residual_norm / d_fast.rhs_norm),
+        "error_vs_fp64": err,
+        "plain_fp64": {"ms": round(plain_ms, 3), "iterations": plain_iters,
+                       "algorithm": "paso PCG with residual smoothing, balanced CSR FP64"},
+        "speedup_vs_plain_fp64": round(plain_ms / ms, 3),
+        "roofline": roofline, "cpu_baseline": cpu,
+        "e2e": {"value": round(e2e_ms, 3), "unit": "ms", "h2d_bytes_per_step": bi, "d2h_bytes_per_step": bo},
+        "gpu_launches": launches, "clocks": clk, "kernels": kernels,
+    }
+    lib.rg_matrix_destroy(mat)
+    lib.rg_domain_destroy(dom)
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+# ----------------------------------------------------------------------------------------------
+# reference arm: the reference's own CPU implementation of the path on the host cores
+# ----------------------------------------------------------------------------------------------
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    threads = os.cpu_count() or 1
+    inp = make_inputs(args.ne, args.seed, 8.0 * args.ne / 128.0)
+    # warm-up 1: one complete solve gives paso's iteration count for the extrapolation
+    n_iter, full_s = cpu_full_reference_iterations(inp, threads)
+    for _ in range(max(args.warmup - 1, 0)):
+        cpu_reference_sample(inp, n_iter, threads)
+    vals = []
+    for _ in range(args.steps):
+        s = cpu_reference_sample(inp, n_iter, threads)
+        vals.append(s["time_to_solution_s"] * 1e3)
+    v = statistics.mean(vals)
+    kind = "reference" if O.have_ref() else "port"
+    out = {
+        "impl": "reference", "metric": METRIC, "value": round(v, 1), "unit": "ms", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(v, 1), "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic, seeded: kappa=exp(GRF corr 8 cells, std 1), 4 Gaussian blobs",
+        "config": {"workload": f"Brick {args.ne}^3 variable-coefficient Poisson, u=0 on top face, "
+                               f"PCG+Jacobi rtol {RTOL:g} (assemble+constrain+solve per step)",
+                   "ne": [args.ne] * 3, "seed": args.seed, "full_solve_s": round(full_s, 2),
+                   "iterations": n_iter},
+        "cpu_baseline": {"value": round(v, 1), "unit": "ms", "cores": threads, "kind": kind,
+                         "sample": ("reference DefaultAssembler3D + insertConstraint on the full input, "
+                                    f"paso Solver/PCG for 10 and 40 iterations, extrapolated to the "
+                                    f"{n_iter} iterations of one full reference solve (warm-up)")},
+        "e2e": {"value": round(v, 1), "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--ne", type=int, default=128, help="elements per axis (128 = the named workload)")
+    ap.add_argument("--seed", type=int, default=2026)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,185 @@
+/*
+ * ripley_gpu — B200 (sm_100a) implementation of the ripley Q1 assembly and
+ * paso PCG/Jacobi solve path of esys-escript, behind a plain C ABI.
+ *
+ * Every entry point returns an int status (RG_OK on success) and never throws.
+ * rg_last_error() returns the message of the last failure on the calling thread.
+ * Pointers are DEVICE pointers unless the name says _host.  Work is ordered on
+ * the stream set by rg_set_stream (default: the legacy default stream); calls
+ * are not thread-safe per handle.
+ *
+ * The reference interfaces replaced (paths relative to the esys-escript tree):
+ *   ripley::Brick / ripley::Rectangle construction     ripley/src/ripleycpp.cpp:151-238, 521-546
+ *   RipleyDomain::getPasoMatrixPattern / Pattern       ripley/src/Brick.cpp:2546-2747, 3000-3061
+ *   RipleyDomain::newSystemMatrix (paso SystemMatrix)   ripley/src/RipleyDomain.cpp:950-1022
+ *   AbstractAssembler::assemblePDESingle               ripley/src/AbstractAssembler.h:33-63
+ *   DefaultAssembler{2,3}D::assemblePDESingle          ripley/src/DefaultAssembler3D.cpp:152-2226
+ *   DefaultAssembler{2,3}D::assemblePDEBoundarySingle  ripley/src/DefaultAssembler3D.cpp:2232-2888
+ *   LinearPDE.insertConstraint                         escriptcore/py_src/linearPDEs.py:2084-2112
+ *   AbstractSystemMatrix::nullifyRowsAndCols           paso/src/SystemMatrix.h:544-605
+ *   AbstractSystemMatrix::ypAx                         paso/src/SystemMatrix.h:643-666
+ *   AbstractSystemMatrix::setToSolution -> paso solve  paso/src/SystemMatrix.h:614-641,
+ *                                                      paso/src/Solver.cpp:46-330, PCG.cpp:62-367
+ *   AbstractSystemMatrix::saveMM                       paso/src/SystemMatrix.h:70-80
+ *   Brick::interpolateNodesOnElements                  ripley/src/Brick.cpp:3315-3398
+ */
+#ifndef RIPLEY_GPU_H
+#define RIPLEY_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes (paso SolverResult + PasoException classes, paso/src/solve.cpp:119-142) */
+#define RG_OK 0
+#define RG_INVALID_ARG 1   /* ValueError / PasoException on bad input                       */
+#define RG_CUDA_ERROR 2    /* a CUDA runtime call failed                                    */
+#define RG_MAXITER 3       /* "maximum number of iteration steps reached"                   */
+#define RG_BREAKDOWN 4     /* "fatal break down in iterative solver"                        */
+#define RG_NAN 5           /* "Matrix or right hand side contains undefined values"        */
+#define RG_TIMEOUT 6       /* a bounded device wait gave up (persistent kernels)            */
+#define RG_DIVERGENCE 7    /* "No improvement during iteration. Iterative solver gives up." */
+#define RG_NOT_SUPPORTED 8 /* option combination this library does not implement            */
+
+typedef struct rg_domain rg_domain;
+typedef struct rg_matrix rg_matrix;
+
+/* ---- library ------------------------------------------------------------------------- */
+int rg_version(void);
+/* copies the last error message (NUL-terminated, truncated to len) */
+int rg_last_error(char* buf, size_t len);
+/* cudaStream_t used for all following calls from this thread (NULL = default stream) */
+int rg_set_stream(void* stream);
+
+/* ---- domain: ripley::Rectangle (dim 2) / ripley::Brick (dim 3), one rank -------------- */
+/* ne: elements per axis; x0/x1: coordinate range per axis (Brick(n0,n1,n2,l0,l1,l2) with
+   l = (x0, x1) tuples).  The CSR pattern is built on the device at creation. */
+int rg_domain_create(int dim, const int64_t ne[3], const double x0[3], const double x1[3],
+                     rg_domain** out);
+int rg_domain_destroy(rg_domain* dom);
+/* n: DOF count (= nodes); nnz: pattern entries; nn/ne: nodes/elements per axis; dx: spacing */
+int rg_domain_info(const rg_domain* dom, int64_t* n, int64_t* nnz, int64_t nn[3],
+                   int64_t ne[3], double dx[3]);
+/* device CSR pattern (int32, offset 0, rows sorted): Brick::getConnections +
+   paso::Pattern.  Pointers stay owned by the domain. */
+int rg_pattern(const rg_domain* dom, const int32_t** ptr, const int32_t** idx, int64_t* n,
+               int64_t* nnz);
+/* host copy of the pattern; ptr_host has n+1 entries, idx_host nnz */
+int rg_pattern_to_host(const rg_domain* dom, int32_t* ptr_host, int32_t* idx_host);
+
+/* ---- coefficients (escript::Data on Function / FunctionOnBoundary) -------------------- */
+#define RG_COEF_EMPTY 0       /* coefficient not set                                      */
+#define RG_COEF_CONSTANT 1    /* one data point for every element (DataConstant)          */
+#define RG_COEF_EXPANDED 2    /* one data point per quadrature point (DataExpanded)       */
+#define RG_COEF_PER_ELEMENT 3 /* one data point per element, same at its quadrature points */
+typedef struct {
+    const double* ptr; /* device pointer; layout as escript: A[i + d*j + d*d*q + d*d*Q*e],
+                          B/C/X[i + d*q + d*Q*e], D/Y[q + Q*e] (Q = 2^dim quadrature
+                          points, q x-fastest); PER_ELEMENT drops the q index          */
+    int kind;
+} rg_coef;
+
+/* ---- system matrix: paso::SystemMatrix<double>, block size 1 -------------------------- */
+int rg_matrix_create(rg_domain* dom, rg_matrix** out); /* values zeroed */
+int rg_matrix_destroy(rg_matrix* mat);
+/* AbstractSystemMatrix::resetValues: zero the values, drop balancing and solver data */
+int rg_matrix_reset(rg_matrix* mat);
+/* device pointer to the nnz CSR values (FP64), in the domain's pattern order */
+int rg_matrix_values(rg_matrix* mat, double** val);
+/* 1 when the values have been balanced in place by a solve (paso keeps them so) */
+int rg_matrix_is_balanced(const rg_matrix* mat, int* balanced);
+/* device pointer to the balance vector (n entries); valid when balanced */
+int rg_matrix_balance_vector(rg_matrix* mat, const double** bv);
+
+/* assemblePDESingle: adds the interior terms of
+     -(A_ij u_,j + B_i u)_,i + C_j u_,j + D u = -X_i,i + Y
+   into mat (may be NULL) and rhs (n doubles, may be NULL).  Any coefficient may be NULL
+   or RG_COEF_EMPTY. */
+int rg_assemble_single(rg_matrix* mat, double* rhs, const rg_coef* A, const rg_coef* B,
+                       const rg_coef* C, const rg_coef* D, const rg_coef* X, const rg_coef* Y);
+/* assemblePDEBoundarySingle: adds the face terms d (matrix) and y (rhs).  d/y are on
+   FunctionOnBoundary: faces left,right,bottom,top(,front,back), face elements lower
+   in-face axis fastest, 2^(dim-1) Gauss points per face element. */
+int rg_assemble_boundary(rg_matrix* mat, double* rhs, const rg_coef* d, const rg_coef* y);
+
+/* LinearPDE.insertConstraint(rhs_only=0): rhs -= A*u with u = r on q>0 else 0; rows and
+   columns with q>0 nullified with 1 on the diagonal; rhs[q>0] = r.  r may be NULL (= 0).
+   With rhs_only=1 only rhs[q>0] = r is applied, as the reference does. */
+int rg_insert_constraint(rg_matrix* mat, double* rhs, const double* q, const double* r,
+                         int rhs_only);
+/* SystemMatrix::nullifyRowsAndCols(mask_row, mask_col, main_diagonal_value) */
+int rg_nullify_rows_and_cols(rg_matrix* mat, const double* mask_row, const double* mask_col,
+                             double main_diagonal_value);
+/* ypAx / MatrixVector: y = alpha*A*x + beta*y on the unbalanced matrix (paso throws for a
+   balanced matrix: RG_INVALID_ARG here) */
+int rg_spmv(rg_matrix* mat, double alpha, const double* x, double beta, double* y);
+/* Brick/Rectangle::interpolateNodesOnElements: nodal (n x ncomp) -> Function
+   (NE x Q x ncomp), or ReducedFunction (element mean) when reduced != 0 */
+int rg_interpolate_nodes(const rg_domain* dom, const double* nodal, int ncomp, double* out,
+                         int reduced);
+/* MatrixMarket coordinate real general, 1-based (SystemMatrix::saveMM) */
+int rg_save_mm(rg_matrix* mat, const char* path);
+
+/* ---- solver: SolverBuddy subset + paso Options (escriptcore/src/SolverOptions.cpp:40-70) */
+#define RG_METHOD_PCG 10          /* SolverOptions.PCG                                       */
+#define RG_PRECOND_JACOBI 20      /* SolverOptions.JACOBI                                    */
+#define RG_MODE_PASO 0            /* paso Solver(): balance, Jacobi initial guess, smoothed
+                                     residual PCG, dual-norm outer test (Solver.cpp:186-322)*/
+#define RG_MODE_STANDARD 1        /* textbook Jacobi-PCG on the balanced system, same outer
+                                     dual-norm test, optional initial guess               */
+#define RG_PREC_FP64 0            /* all FP64                                                */
+#define RG_PREC_FP32_REFINE 1     /* FP32 inner PCG, FP64 residual/update/stop test         */
+#define RG_LAYOUT_CSR 0           /* inner SpMV on the paso CSR values                       */
+#define RG_LAYOUT_BAND 1          /* inner SpMV on a 27-band (9 in 2D) structured copy       */
+
+typedef struct {
+    int method;                 /* RG_METHOD_PCG                                            */
+    int preconditioner;         /* RG_PRECOND_JACOBI                                        */
+    double tolerance;           /* relative tolerance, default 1e-8                         */
+    int64_t iter_max;           /* default 100000                                           */
+    int sweeps;                 /* Jacobi sweeps, default 1 (only 1 supported on the GPU)   */
+    int verbose;                /* print per-step residuals like paso                       */
+    int accept_convergence_failure;
+    int mode;                   /* RG_MODE_*                                                */
+    int precision;              /* RG_PREC_*                                                */
+    int layout;                 /* RG_LAYOUT_*                                              */
+    double inner_tolerance;     /* FP32_REFINE: relative reduction per inner solve (1e-5)   */
+    const double* initial_guess;/* STANDARD mode only: device x0 (unbalanced units) or NULL */
+} rg_solver_opts;
+
+typedef struct {
+    int64_t num_iter;           /* total inner iterations (SolverBuddy num_iter)            */
+    int64_t num_outer;          /* outer residual steps                                     */
+    double residual_norm;       /* last l2 norm of the balanced true residual               */
+    double residual_max;        /* last max norm of the balanced true residual              */
+    double rhs_norm;            /* l2 norm of the balanced right hand side                  */
+    int converged;
+    double time;                /* seconds, whole solve (SolverBuddy time)                  */
+    double set_up_time;         /* balancing + preconditioner                               */
+    double net_time;            /* iterations                                               */
+} rg_diag;
+
+void rg_solver_opts_default(rg_solver_opts* opts);
+/* setToSolution: x (n doubles) = A^-1 rhs.  rhs is not modified.  The matrix is
+   balanced in place on the first solve, as paso does; later solves reuse it. */
+int rg_solve(rg_matrix* mat, const double* rhs, double* x, const rg_solver_opts* opts,
+             rg_diag* diag);
+
+
+/* ---- instrumentation ------------------------------------------------------------------ */
+/* Every kernel launch of the library is counted per kind; with timers enabled each launch
+   is also bracketed by CUDA events on its stream.  rg_timers_read folds finished events
+   into the totals (it waits for them).  Kinds are 0..rg_timers_count()-1. */
+int rg_timers_enable(int on);
+int rg_timers_reset(void);
+int rg_timers_count(void);
+const char* rg_timer_name(int kind);
+int rg_timers_read(int kind, int64_t* launches, int64_t* timed, double* total_ms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RIPLEY_GPU_H */

@@ -1,0 +1,124 @@
+"""Generate golden vectors from the reference's own hot-path sources.
+
+Runs the reference's DefaultAssembler2D/3D.cpp and paso Solver.cpp/PCG.cpp/
+SparseMatrix_MatrixVector.cpp, compiled in place by ``make -C oracle ref`` into
+oracle/_ref/libripley_ref.so, on small seeded inputs and stores inputs and outputs in
+tests/golden/golden.npz.  The reference tree is needed only to run this script; the
+tests read the committed .npz.
+
+    python tests/golden/make_golden.py
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, REPO)
+
+from oracle import oracle as O  # noqa: E402
+
+
+def coef_set(rng, dim, nel, kind):
+    nq = 1 << dim
+    out = {}
+    for name, size in (("A", dim * dim), ("B", dim), ("C", dim), ("D", 1), ("X", dim), ("Y", 1)):
+        n = size if kind == O.CONSTANT else size * nq * nel
+        out[name] = rng.standard_normal(n)
+    return out
+
+
+def top_mask(dim, ne):
+    nn = [e + 1 for e in ne]
+    n = int(np.prod(nn))
+    layer = int(np.prod(nn[: dim - 1]))
+    q = np.zeros(n)
+    q[(np.arange(n) // layer) == nn[dim - 1] - 1] = 1.0
+    return q
+
+
+def kappa_problem(rng, dim, ne):
+    nel = int(np.prod(ne))
+    nq = 1 << dim
+    kappa = np.exp(rng.standard_normal(nel))
+    A = np.zeros((nel, nq, dim, dim))
+    for i in range(dim):
+        A[:, :, i, i] = kappa[:, None]
+    A = A.transpose(0, 1, 3, 2).reshape(-1)  # escript order A[i + d*j]
+    Y = rng.standard_normal(nel * nq)
+    return A, Y
+
+
+def main():
+    if not O.have_ref():
+        O.build(reference=True)
+    rng = np.random.default_rng(20261203)
+    g = {}
+    for dim, ne in ((2, (5, 7)), (3, (3, 4, 5))):
+        dx = tuple(0.3 + 0.2 * k for k in range(dim))
+        tag = f"{dim}d"
+        pat = O.pattern(dim, ne)
+        g[f"pat{tag}_ptr"], g[f"pat{tag}_idx"] = pat.ptr, pat.idx
+        nel = int(np.prod(ne))
+        for kname, kind in (("const", O.CONSTANT), ("exp", O.EXPANDED)):
+            cs = coef_set(rng, dim, nel, kind)
+            val, rhs = O.assemble(dim, ne, dx, pat, use_ref=True,
+                                  **{("C_" if k == "C" else k): (kind, v) for k, v in cs.items()})
+            for k, v in cs.items():
+                g[f"asm{tag}_{kname}_{k}"] = v
+            g[f"asm{tag}_{kname}_val"] = val
+            g[f"asm{tag}_{kname}_rhs"] = rhs
+            nf = (2 * ne[1] + 2 * ne[0]) if dim == 2 else 2 * (ne[1] * ne[2] + ne[0] * ne[2] + ne[0] * ne[1])
+            nqf = 1 << (dim - 1)
+            d = rng.standard_normal(1 if kind == O.CONSTANT else nf * nqf)
+            y = rng.standard_normal(1 if kind == O.CONSTANT else nf * nqf)
+            bval = np.zeros(pat.nnz)
+            brhs = np.zeros(pat.n)
+            O.assemble_boundary(dim, ne, dx, pat, bval, brhs, d=(kind, d), y=(kind, y), use_ref=True)
+            g[f"bnd{tag}_{kname}_d"], g[f"bnd{tag}_{kname}_y"] = d, y
+            g[f"bnd{tag}_{kname}_val"], g[f"bnd{tag}_{kname}_rhs"] = bval, brhs
+        g[f"asm{tag}_dx"] = np.array(dx)
+        g[f"asm{tag}_ne"] = np.array(ne)
+
+    # solves: variable-coefficient Poisson with Dirichlet on the top face, tol 1e-10
+    for dim, ne in ((2, (24, 20)), (3, (10, 9, 8))):
+        tag = f"{dim}d"
+        pat = O.pattern(dim, ne)
+        A, Y = kappa_problem(rng, dim, ne)
+        dx = [1.0 / e for e in ne]
+        val, rhs = O.assemble(dim, ne, dx, pat, A=(O.EXPANDED, A), Y=(O.EXPANDED, Y), use_ref=True)
+        q = top_mask(dim, ne)
+        O.insert_constraint(pat, val, rhs, q)
+        sys_val = val.copy()
+        res = O.solve_paso(pat, val, rhs, tol=1e-10, use_ref=True)
+        g[f"solve{tag}_ne"] = np.array(ne)
+        g[f"solve{tag}_A"], g[f"solve{tag}_Y"], g[f"solve{tag}_q"] = A, Y, q
+        g[f"solve{tag}_val"], g[f"solve{tag}_rhs"] = sys_val, rhs
+        g[f"solve{tag}_x"] = res.x
+        g[f"solve{tag}_iter"] = np.array(res.num_iter)
+        g[f"solve{tag}_status"] = np.array(res.status)
+
+    # the reference's CPU-runnable configuration: Rectangle 200x200, A = I, Y = 1,
+    # u = 0 on y = 0, PCG + Jacobi rtol 1e-8
+    ne = (200, 200)
+    pat = O.pattern(2, ne)
+    val, rhs = O.assemble(2, ne, (1 / 200, 1 / 200), pat, A=(O.CONSTANT, np.eye(2).reshape(-1)),
+                          Y=(O.CONSTANT, np.ones(1)), use_ref=True)
+    nn = 201
+    q = np.zeros(nn * nn)
+    q[:nn] = 1.0  # y == 0 row
+    O.insert_constraint(pat, val, rhs, q)
+    res = O.solve_paso(pat, val, rhs, tol=1e-8, use_ref=True)
+    g["r200_x"] = res.x
+    g["r200_iter"] = np.array(res.num_iter)
+
+    out = os.path.join(HERE, "golden.npz")
+    np.savez_compressed(out, **g)
+    print(f"wrote {out}: {len(g)} arrays, {os.path.getsize(out) / 1024:.0f} KiB; "
+          f"iterations r200={int(g['r200_iter'])} solve2d={int(g['solve2d_iter'])} "
+          f"solve3d={int(g['solve3d_iter'])}")
+
+
+if __name__ == "__main__":
+    main()

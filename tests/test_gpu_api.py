@@ -1,0 +1,133 @@
+"""The reference test suite's known-answer problems, run through the escript-facing API
+(esys_b200.escript / esys_b200.ripley) on the GPU.  Each mirrors a reference test:
+  test_PCG_JACOBI         escriptcore/test/python/test_linearPDEs.py:1741-1748
+  Test_Poisson.test_solve escriptcore/test/python/test_linearPDEs.py:382-407
+  SimpleSolve test_single escriptcore/test/python/test_simplesolve.py:125-163,273-282
+"""
+import numpy as np
+import pytest
+
+from esys_b200.escript import (LinearPDE, Poisson, SolverOptions, Solution, ContinuousFunction,
+                               Function, Scalar, Data, kronecker, whereZero, Lsup, inner)
+from esys_b200 import ripley
+from esys_b200 import _lib as L
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-8
+
+
+def check(u, u_ex, tol=TOL):
+    return Lsup(u - u_ex) <= tol * Lsup(u_ex)
+
+
+@pytest.fixture(params=["rect", "brick"])
+def domain(request, cuda):
+    if request.param == "rect":
+        return ripley.Rectangle(12 * 2 - 1, 12 * 2 - 1)
+    return ripley.Brick(12 - 1, 12 - 1, 8 - 1)
+
+
+@pytest.mark.parametrize("precision", [SolverOptions.PRECISION_FP64, SolverOptions.PRECISION_FP32_REFINE])
+def test_pcg_jacobi(domain, precision):
+    pde = LinearPDE(domain)
+    pde.setValue(A=kronecker(domain), D=1.0, Y=1.0)
+    so = pde.getSolverOptions()
+    so.setSolverMethod(SolverOptions.PCG)
+    so.setPreconditioner(SolverOptions.JACOBI)
+    so.setPrecision(precision)
+    u = pde.getSolution()
+    assert check(u, 1.0), "solution is wrong."
+    assert so.getDiagnostics("converged")
+
+
+def test_poisson_quadratic(domain):
+    d = domain.getDim()
+    cf = ContinuousFunction(domain)
+    x = cf.getX()
+    u_ex = Scalar(1.0, cf)
+    for i in range(d):
+        u_ex *= x[i] * (2.0 - x[i])
+    msk = Scalar(0.0, cf)
+    for i in range(d):
+        msk += whereZero(x[i])
+    f = Scalar(0, cf)
+    for i in range(d):
+        f_p = Scalar(1, cf)
+        for j in range(d):
+            if i == j:
+                f_p *= 2.0
+            else:
+                f_p *= x[j] * (2 - x[j])
+        f += f_p
+    pde = Poisson(domain)
+    pde.setValue(f=f, q=msk)
+    u = pde.getSolution()
+    # Q1 on these meshes: discretisation error well below 1e-2
+    assert check(u, u_ex, 1e-2)
+
+
+def test_simple_solve_single(domain):
+    dim = domain.getDim()
+    x = Solution(domain).getX()
+    u_ex = 1.0 + 2.0 * x[0] + 3.0 * x[1] + (4.0 * x[2] if dim == 3 else 0.0)
+    g_ex = np.array([2.0, 3.0, 4.0][:dim])
+    pde = LinearPDE(domain, numEquations=1)
+    pde.setValue(r=u_ex, q=whereZero(x[0]), A=kronecker(dim), y=inner(g_ex, domain.getNormal()))
+    so = pde.getSolverOptions()
+    so.setSolverMethod(SolverOptions.PCG)
+    so.setTolerance(1e-8)
+    u = pde.getSolution()
+    assert Lsup(u - u_ex) < 1e-6 * Lsup(u_ex)
+
+
+def test_rhs_only_change_reuses_operator(cuda):
+    dom = ripley.Brick(10, 8, 6)
+    pde = LinearPDE(dom)
+    pde.setValue(A=kronecker(3), D=1.0, Y=1.0)
+    u1 = pde.getSolution()
+    op1 = pde.getOperator()
+    pde.setValue(Y=2.0)
+    u2 = pde.getSolution()
+    assert pde.getOperator() is op1
+    assert check(u1, 1.0) and check(u2, 2.0)
+
+
+def test_unsupported_features_raise(cuda):
+    dom = ripley.Rectangle(4, 4)
+    with pytest.raises(NotImplementedError):
+        LinearPDE(dom, numEquations=2)
+    pde = LinearPDE(dom)
+    with pytest.raises(NotImplementedError):
+        pde.setValue(A_reduced=kronecker(2))
+    with pytest.raises(ValueError):
+        pde.setValue(Z=1.0)
+    pde.setValue(A=kronecker(2), Y=1.0)
+    pde.getSolverOptions().setSolverMethod(SolverOptions.GMRES)
+    with pytest.raises(NotImplementedError):
+        pde.getSolution()
+
+
+def test_maxiter_raises_paso_exception(cuda):
+    dom = ripley.Rectangle(40, 40)
+    pde = LinearPDE(dom)
+    x = Solution(dom).getX()
+    pde.setValue(A=kronecker(2), Y=1.0, q=whereZero(x[1]))
+    pde.getSolverOptions().setIterMax(3)
+    with pytest.raises(L.PasoException) as e:
+        pde.getSolution()
+    assert e.value.status == L.RG_MAXITER
+
+
+def test_function_space_coordinates(cuda):
+    dom = ripley.Brick(3, 2, 2, l0=(1.0, 4.0))
+    xq = Function(dom).getX().toNumpy()
+    assert xq.shape == (12 * 8, 3)
+    g0 = 0.5 - np.sqrt(3) / 6
+    assert np.allclose(xq[0], [1.0 + g0, g0 / 2, g0 / 2])
+    assert np.allclose(xq[1], [1.0 + 1 - g0, g0 / 2, g0 / 2])
+    xn = Solution(dom).getX().toNumpy()
+    assert np.allclose(xn[1], [2.0, 0, 0]) and np.allclose(xn[4], [1.0, 0.5, 0])
+    # interpolation of a linear field to the Gauss points is exact
+    lin = Data(Solution(dom).getX()[0] * 2.0 + Solution(dom).getX()[2], Function(dom))
+    assert np.allclose(lin.toNumpy(), 2 * xq[:, 0] + xq[:, 2])

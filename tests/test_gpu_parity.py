@@ -1,0 +1,262 @@
+"""GPU parity tests through the C-ABI: the CUDA path against the oracle and against the
+reference's own outputs (golden vectors).
+
+Tolerances:
+  * pattern: bit-exact;
+  * assembled values: |gpu - ref| <= 1e-13 * max|row| per row (rhs: 1e-13 * max|rhs|);
+  * solutions: paso mode at tol 1e-10 within 1e-8 relative of the reference solution;
+    FP32-inner/FP64-refine within 1e-7 relative at tol 1e-10.
+"""
+import numpy as np
+import pytest
+import torch
+
+from oracle import oracle as O
+import rgcapi as R
+from esys_b200 import _lib as L
+
+pytestmark = pytest.mark.gpu
+
+ASM_TOL = 1e-13
+
+
+def row_scaled_err(ptr, a, b):
+    rows = np.repeat(np.arange(len(ptr) - 1), np.diff(ptr))
+    m = np.zeros(len(ptr) - 1)
+    np.maximum.at(m, rows, np.abs(b))
+    m = np.maximum(m, 1e-300)
+    return float((np.abs(a - b) / m[rows]).max())
+
+
+@pytest.mark.parametrize("dim,ne", [(2, (5, 7)), (3, (3, 4, 5)), (2, (200, 200)), (3, (1, 1, 1)),
+                                    (3, (64, 48, 33)), (3, (128, 128, 128))])
+def test_pattern_bit_exact(cuda, dim, ne):
+    d = R.Domain(dim, ne)
+    p, i = d.pattern()
+    ref = O.pattern(dim, ne)
+    assert np.array_equal(p, ref.ptr)
+    assert np.array_equal(i, ref.idx)
+
+
+def _golden_coefs(golden, tag, kname):
+    kind = R.KINDS[kname]
+    return {k: (golden[f"asm{tag}_{kname}_{k}"], kind) for k in "ABCDXY"}
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+@pytest.mark.parametrize("kname", ["const", "exp"])
+def test_assembly_matches_reference(cuda, golden, dim, kname):
+    tag = f"{dim}d"
+    ne = tuple(int(v) for v in golden[f"asm{tag}_ne"])
+    dx = golden[f"asm{tag}_dx"]
+    d = R.Domain(dim, ne, x1=[dx[k] * ne[k] for k in range(dim)])
+    m = R.Matrix(d)
+    rhs = torch.zeros(d.n, dtype=torch.float64, device="cuda")
+    keep = []
+    R.assemble(m, rhs, keep, **_golden_coefs(golden, tag, kname))
+    val = m.values()
+    p, _ = d.pattern()
+    assert row_scaled_err(p, val, golden[f"asm{tag}_{kname}_val"]) < ASM_TOL
+    ref_rhs = golden[f"asm{tag}_{kname}_rhs"]
+    assert np.abs(rhs.cpu().numpy() - ref_rhs).max() <= ASM_TOL * np.abs(ref_rhs).max()
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+@pytest.mark.parametrize("kname", ["const", "exp"])
+def test_boundary_assembly_matches_reference(cuda, golden, dim, kname):
+    tag = f"{dim}d"
+    ne = tuple(int(v) for v in golden[f"asm{tag}_ne"])
+    dx = golden[f"asm{tag}_dx"]
+    d = R.Domain(dim, ne, x1=[dx[k] * ne[k] for k in range(dim)])
+    m = R.Matrix(d)
+    rhs = torch.zeros(d.n, dtype=torch.float64, device="cuda")
+    keep = []
+    kind = R.KINDS[kname]
+    R.assemble_boundary(m, rhs, keep, d=(golden[f"bnd{tag}_{kname}_d"], kind),
+                        y=(golden[f"bnd{tag}_{kname}_y"], kind))
+    rv, rr = golden[f"bnd{tag}_{kname}_val"], golden[f"bnd{tag}_{kname}_rhs"]
+    assert np.abs(m.values() - rv).max() <= ASM_TOL * np.abs(rv).max()
+    assert np.abs(rhs.cpu().numpy() - rr).max() <= ASM_TOL * np.abs(rr).max()
+
+
+@pytest.mark.parametrize("dim,ne", [(2, (9, 6)), (3, (6, 5, 7))])
+def test_per_element_equals_expanded(cuda, dim, ne):
+    """A per-element coefficient is the expanded one with equal values at the Gauss points."""
+    rng = np.random.default_rng(5)
+    nel = int(np.prod(ne))
+    nq = 1 << dim
+    Ae = rng.standard_normal((nel, dim * dim))
+    De = rng.standard_normal(nel)
+    d = R.Domain(dim, ne)
+    m1, m2 = R.Matrix(d), R.Matrix(d)
+    r1 = torch.zeros(d.n, dtype=torch.float64, device="cuda")
+    r2 = torch.zeros_like(r1)
+    keep = []
+    R.assemble(m1, r1, keep, A=(Ae, R.KINDS["elem"]), D=(De, R.KINDS["elem"]), Y=(De, R.KINDS["elem"]))
+    R.assemble(m2, r2, keep, A=(np.repeat(Ae, nq, axis=0), R.KINDS["exp"]),
+               D=(np.repeat(De, nq), R.KINDS["exp"]), Y=(np.repeat(De, nq), R.KINDS["exp"]))
+    p, _ = d.pattern()
+    assert row_scaled_err(p, m1.values(), m2.values()) < ASM_TOL
+    assert torch.allclose(r1, r2, rtol=0, atol=ASM_TOL * float(r2.abs().max()))
+
+
+def test_large_brick_assembly_matches_oracle(cuda):
+    """Brick 48x40x32 with expanded isotropic kappa and expanded Y (the benchmark's
+    coefficient form) against the oracle."""
+    rng = np.random.default_rng(7)
+    ne = (48, 40, 32)
+    nel = int(np.prod(ne))
+    kappa = np.exp(rng.standard_normal(nel))
+    A = np.zeros((nel, 8, 3, 3))
+    for i in range(3):
+        A[:, :, i, i] = kappa[:, None]
+    A = A.reshape(-1)
+    Y = rng.standard_normal(nel * 8)
+    d = R.Domain(3, ne)
+    m = R.Matrix(d)
+    rhs = torch.zeros(d.n, dtype=torch.float64, device="cuda")
+    keep = []
+    R.assemble(m, rhs, keep, A=(A, R.KINDS["exp"]), Y=(Y, R.KINDS["exp"]))
+    pat = O.pattern(3, ne)
+    val, rr = O.assemble(3, ne, d.dx, pat, A=(O.EXPANDED, A), Y=(O.EXPANDED, Y))
+    assert row_scaled_err(pat.ptr, m.values(), val) < ASM_TOL
+    assert np.abs(rhs.cpu().numpy() - rr).max() <= ASM_TOL * np.abs(rr).max()
+
+
+def _system(golden, tag):
+    ne = tuple(int(v) for v in golden[f"solve{tag}_ne"])
+    dim = len(ne)
+    d = R.Domain(dim, ne)
+    m = R.Matrix(d)
+    rhs = torch.zeros(d.n, dtype=torch.float64, device="cuda")
+    keep = []
+    R.assemble(m, rhs, keep, A=(golden[f"solve{tag}_A"], R.KINDS["exp"]),
+               Y=(golden[f"solve{tag}_Y"], R.KINDS["exp"]))
+    q = R.dev(golden[f"solve{tag}_q"])
+    R.insert_constraint(m, rhs, q)
+    return d, m, rhs, keep
+
+
+@pytest.mark.parametrize("tag", ["2d", "3d"])
+def test_constraint_matches_reference(cuda, golden, tag):
+    d, m, rhs, _ = _system(golden, tag)
+    p, _ = d.pattern()
+    assert row_scaled_err(p, m.values(), golden[f"solve{tag}_val"]) < ASM_TOL
+    ref = golden[f"solve{tag}_rhs"]
+    assert np.abs(rhs.cpu().numpy() - ref).max() <= ASM_TOL * np.abs(ref).max()
+
+
+def test_constraint_with_values_and_spmv(cuda):
+    """rhs -= A u_r with nonzero r, then y = A x on the unbalanced matrix (ypAx)."""
+    rng = np.random.default_rng(9)
+    ne = (7, 6, 5)
+    d = R.Domain(3, ne)
+    m = R.Matrix(d)
+    nel = int(np.prod(ne))
+    A = rng.standard_normal(nel * 8 * 9)
+    Y = rng.standard_normal(nel * 8)
+    rhs = torch.zeros(d.n, dtype=torch.float64, device="cuda")
+    keep = []
+    R.assemble(m, rhs, keep, A=(A, R.KINDS["exp"]), Y=(Y, R.KINDS["exp"]))
+    q = (rng.random(d.n) < 0.2).astype(float)
+    r = rng.standard_normal(d.n)
+    R.insert_constraint(m, rhs, R.dev(q), R.dev(r))
+    pat = O.pattern(3, ne)
+    val, rr = O.assemble(3, ne, d.dx, pat, A=(O.EXPANDED, A), Y=(O.EXPANDED, Y))
+    O.insert_constraint(pat, val, rr, q, r)
+    gv = m.values()
+    assert row_scaled_err(pat.ptr, gv, val) < ASM_TOL
+    assert np.abs(rhs.cpu().numpy() - rr).max() <= 1e-12 * np.abs(rr).max()
+    x = rng.standard_normal(d.n)
+    y0 = rng.standard_normal(d.n)
+    y = R.dev(y0)
+    L.check(R.lib().rg_spmv(m.h, 2.0, R.ptr(R.dev(x)), -0.5, R.ptr(y)))
+    ref = O.spmv(pat, val, x, alpha=2.0, beta=-0.5, y=y0)
+    assert np.abs(y.cpu().numpy() - ref).max() <= 1e-12 * np.abs(ref).max()
+
+
+@pytest.mark.parametrize("tag", ["2d", "3d"])
+def test_paso_solve_matches_reference(cuda, golden, tag):
+    d, m, rhs, _ = _system(golden, tag)
+    x = torch.zeros(d.n, dtype=torch.float64, device="cuda")
+    st, dg = R.solve(m, rhs, x, R.opts(tolerance=1e-10))
+    assert st == 0 and dg.converged
+    ref = golden[f"solve{tag}_x"]
+    err = np.linalg.norm(x.cpu().numpy() - ref) / np.linalg.norm(ref)
+    assert err < 1e-8
+    assert abs(int(dg.num_iter) - int(golden[f"solve{tag}_iter"])) <= 1
+
+
+@pytest.mark.parametrize("tag", ["2d", "3d"])
+@pytest.mark.parametrize("mode,precision", [(L.RG_MODE_STANDARD, L.RG_PREC_FP64),
+                                            (L.RG_MODE_STANDARD, L.RG_PREC_FP32_REFINE)])
+def test_fast_modes_match_reference(cuda, golden, tag, mode, precision):
+    d, m, rhs, _ = _system(golden, tag)
+    x = torch.zeros(d.n, dtype=torch.float64, device="cuda")
+    st, dg = R.solve(m, rhs, x, R.opts(tolerance=1e-10, mode=mode, precision=precision))
+    assert st == 0 and dg.converged
+    ref = golden[f"solve{tag}_x"]
+    err = np.linalg.norm(x.cpu().numpy() - ref) / np.linalg.norm(ref)
+    assert err < (1e-8 if precision == L.RG_PREC_FP64 else 1e-7)
+    # the stopping test is the paso dual-norm test on the FP64 true residual
+    assert dg.residual_norm <= 1e-10 * dg.rhs_norm * (1 + 1e-12)
+
+
+def test_rectangle_200_configuration(cuda, golden):
+    """The reference's CPU-runnable case (Rectangle 200x200, Y = 1, u = 0 on y = 0)."""
+    d = R.Domain(2, (200, 200))
+    m = R.Matrix(d)
+    rhs = torch.zeros(d.n, dtype=torch.float64, device="cuda")
+    keep = []
+    R.assemble(m, rhs, keep, A=(np.eye(2).reshape(-1), R.KINDS["const"]), Y=(np.ones(1), R.KINDS["const"]))
+    q = np.zeros(d.n)
+    q[:201] = 1.0
+    R.insert_constraint(m, rhs, R.dev(q))
+    x = torch.zeros(d.n, dtype=torch.float64, device="cuda")
+    st, dg = R.solve(m, rhs, x, R.opts(tolerance=1e-8))
+    assert st == 0
+    ref = golden["r200_x"]
+    assert np.linalg.norm(x.cpu().numpy() - ref) / np.linalg.norm(ref) < 1e-8
+    assert abs(int(dg.num_iter) - int(golden["r200_iter"])) <= 1
+
+
+def test_second_solve_reuses_balanced_matrix(cuda, golden):
+    d, m, rhs, _ = _system(golden, "3d")
+    x1 = torch.zeros(d.n, dtype=torch.float64, device="cuda")
+    x2 = torch.zeros_like(x1)
+    assert R.solve(m, rhs, x1, R.opts(tolerance=1e-10))[0] == 0
+    b = C_int()
+    L.check(R.lib().rg_matrix_is_balanced(m.h, R.C.byref(b)))
+    assert b.value == 1
+    assert R.solve(m, rhs, x2, R.opts(tolerance=1e-10))[0] == 0
+    assert torch.equal(x1, x2)
+    # values can no longer be changed without a reset (paso balances in place)
+    keep = []
+    with pytest.raises(ValueError):
+        R.assemble(m, None, keep, D=(np.ones(1), R.KINDS["const"]))
+    with pytest.raises(ValueError):
+        L.check(R.lib().rg_spmv(m.h, 1.0, R.ptr(x1), 0.0, R.ptr(x2)))
+
+
+def C_int():
+    import ctypes
+    return ctypes.c_int()
+
+
+def test_solver_errors_are_reported(cuda, golden):
+    d, m, rhs, _ = _system(golden, "2d")
+    x = torch.zeros(d.n, dtype=torch.float64, device="cuda")
+    st, _ = R.solve(m, rhs, x, R.opts(tolerance=1e-20))
+    assert st == L.RG_INVALID_ARG and "Tolerance" in L.last_error()
+    st, _ = R.solve(m, rhs, x, R.opts(iter_max=2))
+    assert st == L.RG_MAXITER
+    st, dg = R.solve(m, rhs, x, R.opts(iter_max=2, accept_convergence_failure=1))
+    assert st == 0 and not dg.converged
+    bad = rhs.clone()
+    bad[5] = float("nan")
+    st, _ = R.solve(m, bad, x, R.opts())
+    assert st == L.RG_NAN
+    st, dg = R.solve(m, torch.zeros_like(rhs), x, R.opts())
+    assert st == 0 and dg.converged and not bool(x.any())
+    st, _ = R.solve(m, rhs, x, R.opts(sweeps=2))
+    assert st == L.RG_NOT_SUPPORTED

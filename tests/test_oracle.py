@@ -1,0 +1,233 @@
+"""CPU tests: the oracle restatement against the reference's own outputs (golden vectors
+made by tests/golden/make_golden.py from the reference sources) and against the
+known-answer problems of the reference's test suite."""
+import math
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+# assembled values are compared relative to the largest entry of their row, because
+# entries that vanish analytically carry only rounding noise
+ASM_TOL = 1e-13
+
+
+def row_scaled_err(pat, a, b):
+    err = 0.0
+    for i in range(pat.n):
+        s = slice(pat.ptr[i], pat.ptr[i + 1])
+        m = max(np.abs(b[s]).max(), 1e-300)
+        err = max(err, np.abs(a[s] - b[s]).max() / m)
+    return err
+
+
+def coefs_from(golden, tag, kname, kind):
+    out = {}
+    for k in "ABCDXY":
+        out["C_" if k == "C" else k] = (kind, golden[f"asm{tag}_{kname}_{k}"])
+    return out
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_pattern_matches_reference_numbering(golden, dim):
+    ne = tuple(golden[f"asm{dim}d_ne"])
+    pat = O.pattern(dim, ne)
+    assert np.array_equal(pat.ptr, golden[f"pat{dim}d_ptr"])
+    assert np.array_equal(pat.idx, golden[f"pat{dim}d_idx"])
+    nn = [e + 1 for e in ne]
+    assert pat.nnz == int(np.prod([3 * v - 2 for v in nn]))
+    # rows sorted, diagonal present
+    for i in range(pat.n):
+        row = pat.idx[pat.ptr[i]:pat.ptr[i + 1]]
+        assert np.all(np.diff(row) > 0) and i in row
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+@pytest.mark.parametrize("kname,kind", [("const", O.CONSTANT), ("exp", O.EXPANDED)])
+def test_assembly_matches_reference(golden, dim, kname, kind):
+    tag = f"{dim}d"
+    ne = tuple(golden[f"asm{tag}_ne"])
+    dx = tuple(golden[f"asm{tag}_dx"])
+    pat = O.pattern(dim, ne)
+    val, rhs = O.assemble(dim, ne, dx, pat, **coefs_from(golden, tag, kname, kind))
+    assert row_scaled_err(pat, val, golden[f"asm{tag}_{kname}_val"]) < ASM_TOL
+    ref_rhs = golden[f"asm{tag}_{kname}_rhs"]
+    assert np.abs(rhs - ref_rhs).max() <= ASM_TOL * np.abs(ref_rhs).max()
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+@pytest.mark.parametrize("kname,kind", [("const", O.CONSTANT), ("exp", O.EXPANDED)])
+def test_boundary_assembly_matches_reference(golden, dim, kname, kind):
+    tag = f"{dim}d"
+    ne = tuple(golden[f"asm{tag}_ne"])
+    dx = tuple(golden[f"asm{tag}_dx"])
+    pat = O.pattern(dim, ne)
+    val = np.zeros(pat.nnz)
+    rhs = np.zeros(pat.n)
+    O.assemble_boundary(dim, ne, dx, pat, val, rhs, d=(kind, golden[f"bnd{tag}_{kname}_d"]),
+                        y=(kind, golden[f"bnd{tag}_{kname}_y"]))
+    rv, rr = golden[f"bnd{tag}_{kname}_val"], golden[f"bnd{tag}_{kname}_rhs"]
+    assert np.abs(val - rv).max() <= ASM_TOL * np.abs(rv).max()
+    assert np.abs(rhs - rr).max() <= ASM_TOL * np.abs(rr).max()
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_paso_solver_matches_reference(golden, dim):
+    tag = f"{dim}d"
+    ne = tuple(golden[f"solve{tag}_ne"])
+    pat = O.pattern(dim, ne)
+    val = golden[f"solve{tag}_val"].copy()
+    res = O.solve_paso(pat, val, golden[f"solve{tag}_rhs"], tol=1e-10)
+    assert res.status == int(golden[f"solve{tag}_status"]) == 0
+    assert res.num_iter == int(golden[f"solve{tag}_iter"])
+    ref = golden[f"solve{tag}_x"]
+    assert np.linalg.norm(res.x - ref) / np.linalg.norm(ref) < 1e-12
+
+
+def test_rectangle_200_configuration_matches_reference(golden):
+    ne = (200, 200)
+    pat = O.pattern(2, ne)
+    val, rhs = O.assemble(2, ne, (1 / 200, 1 / 200), pat, A=(O.CONSTANT, np.eye(2).reshape(-1)),
+                          Y=(O.CONSTANT, np.ones(1)))
+    q = np.zeros(pat.n)
+    q[:201] = 1.0
+    O.insert_constraint(pat, val, rhs, q)
+    res = O.solve_paso(pat, val, rhs, tol=1e-8)
+    assert res.num_iter == int(golden["r200_iter"])
+    assert np.linalg.norm(res.x - golden["r200_x"]) / np.linalg.norm(golden["r200_x"]) < 1e-12
+
+
+# ---- analytic known answers -------------------------------------------------------------
+
+def test_unit_cube_laplacian_element():
+    """Q1 stiffness of the unit cube: diagonal 1/3, edge neighbours 0, face and body
+    diagonals -1/12."""
+    pat = O.pattern(3, (1, 1, 1))
+    val, _ = O.assemble(3, (1, 1, 1), (1.0, 1.0, 1.0), pat, A=(O.CONSTANT, np.eye(3).reshape(-1)))
+    K = np.zeros((8, 8))
+    for i in range(8):
+        for k in range(pat.ptr[i], pat.ptr[i + 1]):
+            K[i, pat.idx[k]] = val[k]
+    for i in range(8):
+        for j in range(8):
+            hd = bin(i ^ j).count("1")
+            expect = {0: 1 / 3, 1: 0.0, 2: -1 / 12, 3: -1 / 12}[hd]
+            assert abs(K[i, j] - expect) < 1e-15
+
+
+@pytest.mark.parametrize("dim,ne", [(2, (7, 5)), (3, (4, 3, 5))])
+def test_row_sums_and_rhs_integral(dim, ne):
+    rng = np.random.default_rng(3)
+    pat = O.pattern(dim, ne)
+    nel = int(np.prod(ne))
+    nq = 1 << dim
+    dx = [0.1 * (k + 1) for k in range(dim)]
+    A = rng.standard_normal(nel * nq * dim * dim)
+    Y = rng.standard_normal(nel * nq)
+    val, rhs = O.assemble(dim, ne, dx, pat, A=(O.EXPANDED, A), Y=(O.EXPANDED, Y))
+    rows = np.add.reduceat(val, pat.ptr[:-1])
+    assert np.abs(rows).max() < 1e-12 * np.abs(val).max()
+    # sum of rhs = integral of Y = sum_q W Y_q
+    W = np.prod(dx) / nq
+    assert abs(rhs.sum() - W * Y.sum()) < 1e-12 * np.abs(Y).sum() * W
+
+
+def _nodes(dim, ne):
+    nn = [e + 1 for e in ne]
+    axes = [np.arange(v) / e for v, e in zip(nn, ne)]
+    grids = np.meshgrid(*reversed(axes), indexing="ij")
+    return np.stack([g.reshape(-1) for g in reversed(grids)], 1)
+
+
+@pytest.mark.parametrize("dim,ne", [(2, (8, 8)), (3, (8, 8, 8))])
+def test_pcg_jacobi_known_answer(dim, ne):
+    """test_linearPDEs.test_PCG_JACOBI: A = I, D = 1, Y = 1 gives u = 1."""
+    pat = O.pattern(dim, ne)
+    dx = [1.0 / e for e in ne]
+    val, rhs = O.assemble(dim, ne, dx, pat, A=(O.CONSTANT, np.eye(dim).reshape(-1)),
+                          D=(O.CONSTANT, np.ones(1)), Y=(O.CONSTANT, np.ones(1)))
+    res = O.solve_paso(pat, val, rhs, tol=1e-8)
+    assert res.converged and np.abs(res.x - 1.0).max() < 1e-7
+
+
+@pytest.mark.parametrize("dim,ne", [(2, (8, 8)), (3, (8, 8, 8))])
+def test_poisson_known_answer(dim, ne):
+    """Test_Poisson.test_solve: u = prod x_i (2 - x_i), u = 0 on x_i = 0 faces, within 10*TOL
+    relative (Q1 is not exact for this quadratic; the reference uses 10*TOL = 1e-7... on
+    a scale set by its own mesh; here the discretisation error at h = 1/8 is checked)."""
+    pat = O.pattern(dim, ne)
+    dx = [1.0 / e for e in ne]
+    X = _nodes(dim, ne)
+    u_ex = np.prod(X * (2 - X), axis=1)
+    f = np.zeros(len(X))
+    for i in range(dim):
+        fp = np.ones(len(X))
+        for j in range(dim):
+            fp *= 2.0 if i == j else X[:, j] * (2 - X[:, j])
+        f += fp
+    fq = O.interpolate_nodes(dim, ne, f)
+    val, rhs = O.assemble(dim, ne, dx, pat, A=(O.CONSTANT, np.eye(dim).reshape(-1)), Y=(O.EXPANDED, fq))
+    q = np.zeros(len(X))
+    for i in range(dim):
+        q += (np.abs(X[:, i]) < 1e-12)
+    O.insert_constraint(pat, val, rhs, q)
+    res = O.solve_paso(pat, val, rhs, tol=1e-8)
+    err = np.abs(res.x - u_ex).max() / np.abs(u_ex).max()
+    assert res.converged and err < 2e-2
+
+
+@pytest.mark.parametrize("dim,ne", [(2, (11, 11)), (3, (11, 11, 7))])
+def test_simple_solve_known_answer(dim, ne):
+    """SimpleSolveTestCase.test_single: u = 1 + 2x + 3y (+ 4z), A = I, u = u_ex on x = 0,
+    Neumann y = grad(u).n; Q1 reproduces the linear field (REL_TOL 1e-6)."""
+    pat = O.pattern(dim, ne)
+    dx = [1.0 / e for e in ne]
+    X = _nodes(dim, ne)
+    g = np.array([2.0, 3.0, 4.0][:dim])
+    u_ex = 1.0 + X @ g
+    val, rhs = O.assemble(dim, ne, dx, pat, A=(O.CONSTANT, np.eye(dim).reshape(-1)))
+    # y = g.n per face, faces left,right,bottom,top(,front,back)
+    nf_counts = ([ne[1]] * 2 + [ne[0]] * 2) if dim == 2 else \
+        [ne[1] * ne[2]] * 2 + [ne[0] * ne[2]] * 2 + [ne[0] * ne[1]] * 2
+    nqf = 1 << (dim - 1)
+    y = np.concatenate([np.full(c * nqf, (1 if f % 2 else -1) * g[f // 2]) for f, c in enumerate(nf_counts)])
+    O.assemble_boundary(dim, ne, dx, pat, val, rhs, y=(O.EXPANDED, y))
+    q = (np.abs(X[:, 0]) < 1e-12).astype(float)
+    O.insert_constraint(pat, val, rhs, q, u_ex)
+    res = O.solve_paso(pat, val, rhs, tol=1e-8)
+    assert res.converged
+    assert np.abs(res.x - u_ex).max() < 1e-6 * np.abs(u_ex).max()
+
+
+def test_solver_input_errors():
+    pat = O.pattern(2, (4, 4))
+    val, rhs = O.assemble(2, (4, 4), (0.25, 0.25), pat, A=(O.CONSTANT, np.eye(2).reshape(-1)),
+                          D=(O.CONSTANT, np.ones(1)), Y=(O.CONSTANT, np.ones(1)))
+    assert O.solve_paso(pat, val.copy(), rhs, tol=1e-20).status == 1  # tolerance too small
+    bad = rhs.copy()
+    bad[3] = math.nan
+    assert O.solve_paso(pat, val.copy(), bad).status == 5               # undefined values
+    assert O.solve_paso(pat, val.copy(), rhs, iter_max=1).status == 3  # max iterations
+    z = O.solve_paso(pat, val.copy(), np.zeros(pat.n))
+    assert z.status == 0 and not z.x.any()                              # zero rhs -> x = 0
+
+
+def test_oracle_equals_reference_build_when_available():
+    """Where the reference sources were compiled (oracle/_ref), compare directly on
+    fresh random inputs."""
+    if not O.have_ref():
+        pytest.skip("reference sources not compiled here")
+    rng = np.random.default_rng(11)
+    for dim, ne in ((2, (6, 9)), (3, (5, 4, 3))):
+        pat = O.pattern(dim, ne)
+        nel = int(np.prod(ne))
+        nq = 1 << dim
+        cs = {"A": (O.EXPANDED, rng.standard_normal(nel * nq * dim * dim)),
+              "C_": (O.CONSTANT, rng.standard_normal(dim)),
+              "D": (O.EXPANDED, rng.standard_normal(nel * nq)),
+              "Y": (O.EXPANDED, rng.standard_normal(nel * nq))}
+        v1, r1 = O.assemble(dim, ne, [0.5] * dim, pat, **cs)
+        v2, r2 = O.assemble(dim, ne, [0.5] * dim, pat, use_ref=True, **cs)
+        assert row_scaled_err(pat, v1, v2) < ASM_TOL
+        assert np.abs(r1 - r2).max() <= ASM_TOL * np.abs(r2).max()
