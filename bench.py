@@ -276,6 +276,19 @@ def run_ours(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
+    if args.only == "plain":
+        for _ in range(args.warmup + args.steps):
+            step(plain)
+        torch.cuda.synchronize()
+        print(json.dumps({"only": "plain", "iterations": int(step(plain).num_iter)}), flush=True)
+        return
+    if args.only == "fast":
+        for _ in range(args.warmup + args.steps):
+            d = step(fast)
+        torch.cuda.synchronize()
+        print(json.dumps({"only": "fast", "iterations": int(d.num_iter)}), flush=True)
+        return
+
     # --- FP64 reference solution for the error statement (paso algorithm, rtol 1e-10)
     step(opts(L.RG_MODE_PASO, L.RG_PREC_FP64, 1e-10))
     x_fp64 = x.clone()
@@ -459,6 +472,8 @@ def main():
     ap.add_argument("--ne", type=int, default=128, help="elements per axis (128 = the named workload)")
     ap.add_argument("--seed", type=int, default=2026)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--only", choices=["all", "fast", "plain"], default="all",
+                    help="profiling runs: only the fast path, or only the plain FP64 paso solve")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

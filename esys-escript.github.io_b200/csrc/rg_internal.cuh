@@ -58,6 +58,7 @@ struct Domain {
     int32_t* ptr = nullptr;  // device CSR pattern
     int32_t* idx = nullptr;
     int nbands;              // 27 (3D) or 9 (2D)
+    int64_t npad;            // band stride: n rounded up to a multiple of 32
     int64_t band_off[27];    // column offset of band b: dx + NN0*dy + NN0*NN1*dz
     Q1Tables q1;
 };
@@ -72,7 +73,7 @@ struct Matrix {
     // solver data derived from the balanced values (paso's preconditioner data)
     bool solver_ready = false;
     double* dinv = nullptr;    // 1 / balanced diagonal
-    float* band32 = nullptr;   // [nbands][n] FP32 copy of the balanced matrix
+    float* band32 = nullptr;   // [nbands][npad] FP32 copy of the balanced matrix
     float* dinv32 = nullptr;
     Workspace* ws = nullptr;
 };

@@ -5,14 +5,21 @@
 //    minimal-residual smoothing sequence (rs, x2, gamma_1/2) stopping on the smoothed
 //    residual, and the outer loop's dual l2/lmax test on the true residual.
 //  * RG_MODE_STANDARD: the same outer loop around textbook Jacobi-PCG (no smoothing).
-//  * RG_PREC_FP32_REFINE: the outer loop stays FP64 (true residual on the FP64 CSR
-//    values, solution update, norms), the inner Jacobi-PCG runs on the FP32 band copy
-//    with FP32 vectors and FP64 dot products.
+//  * RG_PREC_FP32_REFINE: FP32 Jacobi-PCG on the band copy of the balanced matrix with
+//    FP64 residual replacement: the solution is accumulated in FP64, and every time the
+//    recursive FP32 residual has dropped by `inner_tolerance` the true residual is
+//    recomputed in FP64 on the CSR values, tested with paso's dual-norm criterion and
+//    written back into the FP32 recurrence (the Krylov direction is kept, no restart).
 //
-// One PCG iteration is two or three kernels.  Scalars (alpha, beta, tau, ...) live in
-// device memory: every reduction is finished by the last CTA of its kernel, which
-// also sets the next step's scalars and a `done` flag, so the host only polls `done`
-// once per chunk of iterations and kernels queued after convergence return at once.
+// One PCG iteration is three kernels: a pure SpMV of the search direction with its
+// p.q reduction, an elementwise update with the iteration's reductions, and an
+// elementwise kernel that forms the next search direction (in paso mode it also does
+// the smoothing step).  Scalars (alpha, beta, tau, ...) live in device memory: the last
+// CTA of each reduction kernel finishes the sum in a fixed order, sets the next step's
+// scalars and a `done` flag, so the host polls `done` once per chunk of iterations and
+// kernels queued after convergence return at once.  Elementwise kernels use 16-byte
+// vector accesses; matrix data is loaded with streaming (evict-first) hints so that the
+// solver vectors stay resident in the 126 MB L2.
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -24,18 +31,18 @@ namespace rg {
 
 namespace {
 
-constexpr int kLpr = 8;     // lanes per CSR row
+constexpr int kLpr = 8;  // lanes per CSR row
 constexpr int kThreads = 256;
 
 struct Scal {
-    double tau, tau_next, tau_old;  // paso: tau = v.r
+    double tau, tau_next;      // paso: tau = v.r of this and of the next iteration
     double delta, alpha, beta;
     double gamma1, gamma2;
-    double norm, tol;               // stopping norm and its limit
-    double rho, rho_next;           // textbook PCG
-    double n2, nm;                  // norms from norm kernels
+    double norm, tol;          // stopping norm and its limit
+    double rho;                // textbook PCG: r.z
+    double n2, nm;             // norms from norm kernels
     long long iter, maxit;
-    int done, status, pidx, pad;
+    int done, status, pad0, pad1;
 };
 
 enum { ST_RUN = 0, ST_CONV = 1, ST_MAXIT = 3, ST_BREAK = 4 };
@@ -45,16 +52,16 @@ enum { ST_RUN = 0, ST_CONV = 1, ST_MAXIT = 3, ST_BREAK = 4 };
 struct Workspace {
     int64_t n = 0;
     double *r = nullptr, *x = nullptr, *rs = nullptr, *x2 = nullptr, *q = nullptr, *z = nullptr;
-    double* p[2] = {nullptr, nullptr};
-    double *bb = nullptr;  // balanced rhs
-    float *r32 = nullptr, *d32 = nullptr, *q32 = nullptr, *z32 = nullptr;
-    float* p32[2] = {nullptr, nullptr};
+    double* p = nullptr;
+    double* bb = nullptr;  // balanced rhs
+    float *r32 = nullptr, *d32 = nullptr, *q32 = nullptr, *z32 = nullptr, *p32 = nullptr;
     double* partials = nullptr;
     unsigned* counter = nullptr;
-    Scal* s = nullptr;        // device scalars
-    Scal* hs = nullptr;       // pinned host copy
+    Scal* s = nullptr;   // device scalars
+    Scal* hs = nullptr;  // pinned host copy
     int* bad = nullptr;
-    int grid = 0;
+    int grid_rows = 0;   // CSR row-group kernels
+    int grid_vec = 0;    // elementwise kernels
 };
 
 namespace {
@@ -73,11 +80,12 @@ int ensure_workspace(Matrix* m, bool fp32)
         Workspace* w = new Workspace();
         m->ws = w;
         w->n = n;
-        w->grid = grid_for(n, kThreads / kLpr, 8);
+        w->grid_rows = grid_for(n, kThreads / kLpr, 8);
+        w->grid_vec = grid_for((n + 3) / 4, kThreads, 8);
         int rc;
         if ((rc = dalloc(&w->r, n)) || (rc = dalloc(&w->x, n)) || (rc = dalloc(&w->rs, n)) ||
             (rc = dalloc(&w->x2, n)) || (rc = dalloc(&w->q, n)) || (rc = dalloc(&w->z, n)) ||
-            (rc = dalloc(&w->p[0], n)) || (rc = dalloc(&w->p[1], n)) || (rc = dalloc(&w->bb, n)) ||
+            (rc = dalloc(&w->p, n)) || (rc = dalloc(&w->bb, n)) ||
             (rc = dalloc(&w->partials, (size_t)4 * kNumSMs * 64)) || (rc = dalloc(&w->counter, 1)) ||
             (rc = dalloc(&w->s, 1)) || (rc = dalloc(&w->bad, 1)))
             return rc;
@@ -88,15 +96,23 @@ int ensure_workspace(Matrix* m, bool fp32)
     if (fp32 && !w->r32) {
         int rc;
         if ((rc = dalloc(&w->r32, n)) || (rc = dalloc(&w->d32, n)) || (rc = dalloc(&w->q32, n)) ||
-            (rc = dalloc(&w->z32, n)) || (rc = dalloc(&w->p32[0], n)) || (rc = dalloc(&w->p32[1], n)))
+            (rc = dalloc(&w->z32, n)) || (rc = dalloc(&w->p32, n)))
             return rc;
     }
     return RG_OK;
 }
 
-// ------------------------------------------------------------------ common kernels
-// row-group iteration helper: each group of kLpr lanes owns one row per trip; the trip
-// count is uniform over a warp so shuffles stay converged.
+// ------------------------------------------------------------------ access helpers
+__device__ __forceinline__ int64_t gtid() { return (int64_t)blockIdx.x * blockDim.x + threadIdx.x; }
+__device__ __forceinline__ int64_t gstride() { return (int64_t)gridDim.x * blockDim.x; }
+
+__device__ __forceinline__ double2 ld2(const double* p, int64_t v) { return reinterpret_cast<const double2*>(p)[v]; }
+__device__ __forceinline__ void st2(double* p, int64_t v, double2 a) { reinterpret_cast<double2*>(p)[v] = a; }
+__device__ __forceinline__ float4 ld4(const float* p, int64_t v) { return reinterpret_cast<const float4*>(p)[v]; }
+__device__ __forceinline__ void st4(float* p, int64_t v, float4 a) { reinterpret_cast<float4*>(p)[v] = a; }
+
+// CSR row-group loop: each group of kLpr lanes owns one row per trip; the trip count is
+// uniform over a warp so the shuffles stay converged.
 #define RG_ROW_LOOP(n)                                                                  \
     const int lane = threadIdx.x & (kLpr - 1);                                          \
     const int64_t groups_ = (int64_t)gridDim.x * blockDim.x / kLpr;                     \
@@ -112,14 +128,42 @@ __device__ __forceinline__ double group_sum(double s)
     return s;
 }
 
-// out = a .* b (out may be b), returns ||out||_2^2 and ||out||_inf in s->n2, s->nm
+// sum_k val[k]*x[idx[k]] over this lane's entries of CSR row `row`; all loads of a
+// 32-entry chunk are issued before the multiply-adds.  Matrix data streams (evict-first).
+__device__ __forceinline__ double csr_row_dot(const int32_t* __restrict__ ptr, const int32_t* __restrict__ idx,
+                                              const double* __restrict__ val, const double* __restrict__ x,
+                                              int64_t row, int lane)
+{
+    const int32_t k0 = __ldg(ptr + row), k1 = __ldg(ptr + row + 1);
+    double acc = 0.0;
+    for (int32_t kb = k0 + lane; kb < k1; kb += 4 * kLpr) {
+        int32_t j[4];
+        double a[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int32_t k = kb + u * kLpr;
+            const bool ok = k < k1;
+            j[u] = ok ? __ldcs(idx + k) : (int32_t)row;
+            a[u] = ok ? __ldcs(val + k) : 0.0;
+        }
+        double xv[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) xv[u] = __ldg(x + j[u]);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) acc = fma(a[u], xv[u], acc);
+    }
+    return acc;
+}
+
+// ------------------------------------------------------------------ common kernels
+// out = a .* b, with ||out||_2^2 and ||out||_inf into s->n2, s->nm.  b is the caller's
+// right hand side, whose alignment is unknown, so the accesses are scalar.
 __global__ void __launch_bounds__(kThreads) k_scale_norms(int64_t n, const double* __restrict__ a,
-                                                          const double* b, double* out, ReduceBuf rb,
-                                                          Scal* s)
+                                                          const double* __restrict__ b,
+                                                          double* __restrict__ out, ReduceBuf rb, Scal* s)
 {
     double v[2] = {0.0, 0.0};
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-         i += (int64_t)gridDim.x * blockDim.x) {
+    for (int64_t i = gtid(); i < n; i += gstride()) {
         const double o = a[i] * b[i];
         out[i] = o;
         v[0] += o * o;
@@ -132,7 +176,7 @@ __global__ void __launch_bounds__(kThreads) k_scale_norms(int64_t n, const doubl
     }
 }
 
-// r = bb - A x (bb the balanced rhs) with the l2^2 / max norms of r
+// r = bb - A x (paso MatrixVector_CSR_OFFSET0(-1, x, 1, r)) with l2^2 / max norms of r
 __global__ void __launch_bounds__(kThreads) k_residual(int64_t n, const int32_t* __restrict__ ptr,
                                                        const int32_t* __restrict__ idx,
                                                        const double* __restrict__ val,
@@ -143,9 +187,7 @@ __global__ void __launch_bounds__(kThreads) k_residual(int64_t n, const int32_t*
     double v[2] = {0.0, 0.0};
     RG_ROW_LOOP(n)
     {
-        double acc = 0.0;
-        if (row < n)
-            for (int32_t k = ptr[row] + lane; k < ptr[row + 1]; k += kLpr) acc = fma(val[k], x[idx[k]], acc);
+        double acc = row < n ? csr_row_dot(ptr, idx, val, x, row, lane) : 0.0;
         acc = group_sum(acc);
         if (row < n && lane == 0) {
             const double o = bb[row] + (-1.0) * acc;
@@ -161,96 +203,72 @@ __global__ void __launch_bounds__(kThreads) k_residual(int64_t n, const int32_t*
     }
 }
 
-__global__ void k_mul(int64_t n, const double* __restrict__ a, const double* b, double* out)
+__global__ void k_mul(int64_t n, const double* __restrict__ a, const double* __restrict__ b,
+                      double* __restrict__ out)
 {
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-         i += (int64_t)gridDim.x * blockDim.x)
-        out[i] = a[i] * b[i];
+    for (int64_t i = gtid(); i < n; i += gstride()) out[i] = a[i] * b[i];
 }
 
-__global__ void k_div(int64_t n, const double* a, const double* __restrict__ b, double* out)
+__global__ void k_div(int64_t n, const double* __restrict__ a, const double* __restrict__ b,
+                      double* __restrict__ out)
 {
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-         i += (int64_t)gridDim.x * blockDim.x)
-        out[i] = a[i] / b[i];
+    for (int64_t i = gtid(); i < n; i += gstride()) out[i] = a[i] / b[i];
 }
 
 // ------------------------------------------------------------------ paso PCG (FP64, CSR)
-// PCG.cpp:102-131 initialisation + the first v = prec(r), tau = v.r
+// PCG.cpp:102-131 initialisation, the first v = prec(r), tau = v.r and p = v
 __global__ void __launch_bounds__(kThreads) k_paso_init(int64_t n, const double* __restrict__ r,
                                                         const double* __restrict__ x,
                                                         const double* __restrict__ dinv,
-                                                        double* rs, double* x2, double* p0,
-                                                        double* z, ReduceBuf rb, Scal* s,
-                                                        double tol, long long maxit)
+                                                        double* __restrict__ rs, double* __restrict__ x2,
+                                                        double* __restrict__ p, double* __restrict__ z,
+                                                        ReduceBuf rb, Scal* s, double tol, long long maxit)
 {
     double v[1] = {0.0};
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-         i += (int64_t)gridDim.x * blockDim.x) {
+    for (int64_t i = gtid(); i < n; i += gstride()) {
         const double ri = r[i];
         rs[i] = ri;
         x2[i] = x[i];
-        p0[i] = 0.0;
         const double zi = ri * dinv[i];
         z[i] = zi;
+        p[i] = zi;
         v[0] += zi * ri;
     }
     double t[1];
     if (grid_reduce<1>(v, rb, t) && threadIdx.x == 0) {
-        s->tau = 0.0;
-        s->tau_next = t[0];
+        s->tau = t[0];
         s->iter = 0;
         s->maxit = maxit;
         s->tol = tol;
         s->done = 0;
         s->status = ST_RUN;
-        s->pidx = 0;
         s->norm = 0.0;
     }
 }
 
-// p = v + beta*p (PCG.cpp:193-218) evaluated per column on the fly, v = A*p (223),
-// delta = p.v (228-260), alpha = tau/delta, breakdown on delta == 0
+// v = A*p (PCG.cpp:223), delta = p.v, alpha = tau/delta; breakdown on delta == 0 (228-262)
 __global__ void __launch_bounds__(kThreads) k_paso_spmv(int64_t n, const int32_t* __restrict__ ptr,
                                                         const int32_t* __restrict__ idx,
                                                         const double* __restrict__ val,
-                                                        const double* __restrict__ z,
-                                                        double* pa, double* pb, double* __restrict__ q,
-                                                        ReduceBuf rb, Scal* s)
+                                                        const double* __restrict__ p,
+                                                        double* __restrict__ q, ReduceBuf rb, Scal* s)
 {
     if (s->done) return;
-    const double tau = s->tau_next;
-    const bool first = s->iter == 0;
-    const double beta = first ? 0.0 : tau / s->tau;
-    const double* __restrict__ pold = s->pidx ? pb : pa;
-    double* __restrict__ pnew = s->pidx ? pa : pb;
     double v[1] = {0.0};
     RG_ROW_LOOP(n)
     {
-        double acc = 0.0;
-        if (row < n) {
-            for (int32_t k = ptr[row] + lane; k < ptr[row + 1]; k += kLpr) {
-                const int32_t j = idx[k];
-                const double pj = first ? z[j] : z[j] + beta * pold[j];
-                acc = fma(val[k], pj, acc);
-            }
-        }
+        double acc = row < n ? csr_row_dot(ptr, idx, val, p, row, lane) : 0.0;
         acc = group_sum(acc);
         if (row < n && lane == 0) {
-            const double pi = first ? z[row] : z[row] + beta * pold[row];
-            pnew[row] = pi;
             q[row] = acc;
-            v[0] += acc * pi;
+            v[0] += acc * p[row];
         }
     }
     double t[1];
     if (grid_reduce<1>(v, rb, t) && threadIdx.x == 0) {
-        s->tau_old = s->tau;
-        s->tau = tau;
-        s->beta = beta;
         s->delta = t[0];
-        s->alpha = tau / t[0];
-        if (fabs(t[0]) <= 0.0) {  // breakFlag (PCG.cpp:262)
+        s->alpha = s->tau / t[0];
+        if (fabs(t[0]) <= 0.0) {  // breakFlag
             s->iter += 1;
             s->status = ST_BREAK;
             s->done = 1;
@@ -258,30 +276,42 @@ __global__ void __launch_bounds__(kThreads) k_paso_spmv(int64_t n, const int32_t
     }
 }
 
-// r -= alpha*v; d = r - rs; sum d^2, d.rs (PCG.cpp:263-306); x2 += alpha*p; and the next
-// iteration's v = prec(r), tau = v.r
+// r -= alpha*v; d = r - rs; sum d^2 and d.rs (PCG.cpp:263-306); x2 += alpha*p; the next
+// iteration's v = prec(r) and tau = v.r, so that beta = tau_next/tau is known before
+// the smoothing kernel
 __global__ void __launch_bounds__(kThreads) k_paso_update1(int64_t n, double* __restrict__ r,
                                                            const double* __restrict__ q,
                                                            const double* __restrict__ rs,
                                                            double* __restrict__ x2,
-                                                           const double* pa, const double* pb,
+                                                           const double* __restrict__ p,
                                                            const double* __restrict__ dinv,
-                                                           double* __restrict__ z, ReduceBuf rb,
-                                                           Scal* s)
+                                                           double* __restrict__ z, ReduceBuf rb, Scal* s)
 {
     if (s->done) return;
     const double alpha = s->alpha;
-    const double* __restrict__ pnew = s->pidx ? pa : pb;
     double v[3] = {0.0, 0.0, 0.0};
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-         i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t nv = n >> 1;
+    for (int64_t k = gtid(); k < nv; k += gstride()) {
+        const double2 r0 = ld2(r, k), q0 = ld2(q, k), rs0 = ld2(rs, k), x20 = ld2(x2, k);
+        const double2 p0 = ld2(p, k), di = ld2(dinv, k);
+        const double ra = r0.x - alpha * q0.x, rb2 = r0.y - alpha * q0.y;
+        st2(r, k, make_double2(ra, rb2));
+        const double da = ra - rs0.x, db = rb2 - rs0.y;
+        v[0] += da * da + db * db;
+        v[1] += da * rs0.x + db * rs0.y;
+        st2(x2, k, make_double2(x20.x + alpha * p0.x, x20.y + alpha * p0.y));
+        const double za = ra * di.x, zb = rb2 * di.y;
+        st2(z, k, make_double2(za, zb));
+        v[2] += za * ra + zb * rb2;
+    }
+    if ((n & 1) && gtid() == 0) {
+        const int64_t i = n - 1;
         const double ri = r[i] - alpha * q[i];
         r[i] = ri;
-        const double rsi = rs[i];
-        const double d = ri - rsi;
+        const double d = ri - rs[i];
         v[0] += d * d;
-        v[1] += d * rsi;
-        x2[i] += alpha * pnew[i];
+        v[1] += d * rs[i];
+        x2[i] += alpha * p[i];
         const double zi = ri * dinv[i];
         z[i] = zi;
         v[2] += zi * ri;
@@ -292,25 +322,39 @@ __global__ void __launch_bounds__(kThreads) k_paso_update1(int64_t n, double* __
         s->gamma1 = g1;
         s->gamma2 = 1.0 - g1;
         s->tau_next = t[2];
+        s->beta = t[2] / s->tau;
     }
 }
 
-// rs = g2 rs + g1 r; x = g2 x + g1 x2; sum rs^2; stopping tests (PCG.cpp:307-347)
+// rs = g2 rs + g1 r; x = g2 x + g1 x2; sum rs^2; stopping tests (PCG.cpp:307-347); then
+// the next search direction p = v + beta p (PCG.cpp:193-218)
 __global__ void __launch_bounds__(kThreads) k_paso_update2(int64_t n, double* __restrict__ rs,
                                                            const double* __restrict__ r,
                                                            double* __restrict__ x,
                                                            const double* __restrict__ x2,
-                                                           ReduceBuf rb, Scal* s)
+                                                           const double* __restrict__ z,
+                                                           double* __restrict__ p, ReduceBuf rb, Scal* s)
 {
     if (s->done) return;
-    const double g1 = s->gamma1, g2 = s->gamma2;
+    const double g1 = s->gamma1, g2 = s->gamma2, beta = s->beta;
     double v[1] = {0.0};
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-         i += (int64_t)gridDim.x * blockDim.x) {
-        const double rsi = g2 * rs[i] + g1 * r[i];
-        rs[i] = rsi;
+    const int64_t nv = n >> 1;
+    for (int64_t k = gtid(); k < nv; k += gstride()) {
+        const double2 rs0 = ld2(rs, k), r0 = ld2(r, k), x0 = ld2(x, k), x20 = ld2(x2, k);
+        const double2 z0 = ld2(z, k), p0 = ld2(p, k);
+        const double a = g2 * rs0.x + g1 * r0.x, b = g2 * rs0.y + g1 * r0.y;
+        st2(rs, k, make_double2(a, b));
+        st2(x, k, make_double2(g2 * x0.x + g1 * x20.x, g2 * x0.y + g1 * x20.y));
+        st2(p, k, make_double2(z0.x + beta * p0.x, z0.y + beta * p0.y));
+        v[0] += a * a + b * b;
+    }
+    if ((n & 1) && gtid() == 0) {
+        const int64_t i = n - 1;
+        const double a = g2 * rs[i] + g1 * r[i];
+        rs[i] = a;
         x[i] = g2 * x[i] + g1 * x2[i];
-        v[0] += rsi * rsi;
+        p[i] = z[i] + beta * p[i];
+        v[0] += a * a;
     }
     double t[1];
     if (grid_reduce<1>(v, rb, t) && threadIdx.x == 0) {
@@ -321,7 +365,6 @@ __global__ void __launch_bounds__(kThreads) k_paso_update2(int64_t n, double* __
         const bool conv = norm <= s->tol;
         const bool maxf = it > s->maxit;
         const bool brk = fabs(s->tau) <= 0.0;
-        s->pidx ^= 1;
         if (maxf) {
             s->status = ST_MAXIT;
             s->done = 1;
@@ -332,34 +375,32 @@ __global__ void __launch_bounds__(kThreads) k_paso_update2(int64_t n, double* __
             s->status = ST_CONV;
             s->done = 1;
         }
+        s->tau = s->tau_next;
     }
 }
 
 // ------------------------------------------------------------------ textbook PCG, FP64 CSR
 __global__ void __launch_bounds__(kThreads) k_std_init(int64_t n, const double* __restrict__ r,
                                                        const double* __restrict__ dinv,
-                                                       double* z, double* p0, ReduceBuf rb,
-                                                       Scal* s, double tol, long long maxit)
+                                                       double* __restrict__ z, double* __restrict__ p,
+                                                       ReduceBuf rb, Scal* s, double tol, long long maxit)
 {
     double v[2] = {0.0, 0.0};
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-         i += (int64_t)gridDim.x * blockDim.x) {
+    for (int64_t i = gtid(); i < n; i += gstride()) {
         const double ri = r[i];
         const double zi = ri * dinv[i];
         z[i] = zi;
-        p0[i] = 0.0;
+        p[i] = zi;
         v[0] += zi * ri;
         v[1] += ri * ri;
     }
     double t[2];
     if (grid_reduce<2>(v, rb, t) && threadIdx.x == 0) {
-        s->rho = 0.0;
-        s->rho_next = t[0];
+        s->rho = t[0];
         s->norm = sqrt(t[1]);
         s->iter = 0;
         s->maxit = maxit;
         s->tol = tol;
-        s->pidx = 0;
         s->status = ST_RUN;
         s->done = (s->norm <= tol) ? 1 : 0;
         if (s->done) s->status = ST_CONV;
@@ -369,38 +410,24 @@ __global__ void __launch_bounds__(kThreads) k_std_init(int64_t n, const double* 
 __global__ void __launch_bounds__(kThreads) k_std_spmv(int64_t n, const int32_t* __restrict__ ptr,
                                                        const int32_t* __restrict__ idx,
                                                        const double* __restrict__ val,
-                                                       const double* __restrict__ z, double* pa,
-                                                       double* pb, double* __restrict__ q,
-                                                       ReduceBuf rb, Scal* s)
+                                                       const double* __restrict__ p,
+                                                       double* __restrict__ q, ReduceBuf rb, Scal* s)
 {
     if (s->done) return;
-    const double rho = s->rho_next;
-    const bool first = s->iter == 0;
-    const double beta = first ? 0.0 : rho / s->rho;
-    const double* __restrict__ pold = s->pidx ? pb : pa;
-    double* __restrict__ pnew = s->pidx ? pa : pb;
     double v[1] = {0.0};
     RG_ROW_LOOP(n)
     {
-        double acc = 0.0;
-        if (row < n)
-            for (int32_t k = ptr[row] + lane; k < ptr[row + 1]; k += kLpr) {
-                const int32_t j = idx[k];
-                acc = fma(val[k], first ? z[j] : z[j] + beta * pold[j], acc);
-            }
+        double acc = row < n ? csr_row_dot(ptr, idx, val, p, row, lane) : 0.0;
         acc = group_sum(acc);
         if (row < n && lane == 0) {
-            const double pi = first ? z[row] : z[row] + beta * pold[row];
-            pnew[row] = pi;
             q[row] = acc;
-            v[0] += acc * pi;
+            v[0] += acc * p[row];
         }
     }
     double t[1];
     if (grid_reduce<1>(v, rb, t) && threadIdx.x == 0) {
-        s->rho = rho;
         s->delta = t[0];
-        s->alpha = rho / t[0];
+        s->alpha = s->rho / t[0];
         if (!(fabs(t[0]) > 0.0)) {
             s->iter += 1;
             s->status = ST_BREAK;
@@ -409,21 +436,31 @@ __global__ void __launch_bounds__(kThreads) k_std_spmv(int64_t n, const int32_t*
     }
 }
 
+// x += alpha p; r -= alpha q; z = dinv r; rho_next = r.z, ||r||^2; stopping tests; beta
 __global__ void __launch_bounds__(kThreads) k_std_update(int64_t n, double* __restrict__ x,
                                                          double* __restrict__ r,
                                                          const double* __restrict__ q,
-                                                         const double* pa, const double* pb,
+                                                         const double* __restrict__ p,
                                                          const double* __restrict__ dinv,
-                                                         double* __restrict__ z, ReduceBuf rb,
-                                                         Scal* s)
+                                                         double* __restrict__ z, ReduceBuf rb, Scal* s)
 {
     if (s->done) return;
     const double alpha = s->alpha;
-    const double* __restrict__ pnew = s->pidx ? pa : pb;
     double v[2] = {0.0, 0.0};
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-         i += (int64_t)gridDim.x * blockDim.x) {
-        x[i] += alpha * pnew[i];
+    const int64_t nv = n >> 1;
+    for (int64_t k = gtid(); k < nv; k += gstride()) {
+        const double2 x0 = ld2(x, k), r0 = ld2(r, k), q0 = ld2(q, k), p0 = ld2(p, k), di = ld2(dinv, k);
+        st2(x, k, make_double2(x0.x + alpha * p0.x, x0.y + alpha * p0.y));
+        const double ra = r0.x - alpha * q0.x, rb2 = r0.y - alpha * q0.y;
+        st2(r, k, make_double2(ra, rb2));
+        const double za = ra * di.x, zb = rb2 * di.y;
+        st2(z, k, make_double2(za, zb));
+        v[0] += za * ra + zb * rb2;
+        v[1] += ra * ra + rb2 * rb2;
+    }
+    if ((n & 1) && gtid() == 0) {
+        const int64_t i = n - 1;
+        x[i] += alpha * p[i];
         const double ri = r[i] - alpha * q[i];
         r[i] = ri;
         const double zi = ri * dinv[i];
@@ -435,98 +472,126 @@ __global__ void __launch_bounds__(kThreads) k_std_update(int64_t n, double* __re
     if (grid_reduce<2>(v, rb, t) && threadIdx.x == 0) {
         const long long it = s->iter + 1;
         s->iter = it;
-        s->rho_next = t[0];
         const double norm = sqrt(t[1]);
         s->norm = norm;
-        s->pidx ^= 1;
+        s->beta = t[0] / s->rho;
+        const bool brk = !(fabs(t[0]) > 0.0);
+        s->rho = t[0];
         if (norm <= s->tol) {
             s->status = ST_CONV;
             s->done = 1;
         } else if (it >= s->maxit) {
             s->status = ST_MAXIT;
             s->done = 1;
-        } else if (!(fabs(t[0]) > 0.0)) {
+        } else if (brk) {
             s->status = ST_BREAK;
             s->done = 1;
         }
     }
 }
 
-// ------------------------------------------------------------------ textbook PCG, FP32 band
-// The band copy stores row i's coefficient to neighbour i+off_b at band[b*n + i] (0 where
-// the neighbour does not exist), so a thread per row reads every band coalesced; column
-// indices are clamped into range, where the matching band value is 0.
-struct BandOffsets {
+__global__ void __launch_bounds__(kThreads) k_std_pupdate(int64_t n, const double* __restrict__ z,
+                                                          double* __restrict__ p, const Scal* s)
+{
+    if (s->done) return;
+    const double beta = s->beta;
+    const int64_t nv = n >> 1;
+    for (int64_t k = gtid(); k < nv; k += gstride()) {
+        const double2 z0 = ld2(z, k), p0 = ld2(p, k);
+        st2(p, k, make_double2(z0.x + beta * p0.x, z0.y + beta * p0.y));
+    }
+    if ((n & 1) && gtid() == 0) p[n - 1] = z[n - 1] + beta * p[n - 1];
+}
+
+// ------------------------------------------------------------------ FP32 PCG on the band copy
+// band[b*npad + i] holds row i's coefficient to neighbour i + off_b (0 where there is
+// none; padding rows are 0).  A thread owns 4 consecutive rows: one 16-byte streaming
+// load per band, four neighbour values of p per band (L1/L2 hits).  Near the two ends of
+// the vector the neighbour indices are clamped into range, where the band value is 0.
+struct BandArgs {
     int off[27];
+    int64_t halo;  // max |off|
 };
 
+// r32 = r64 * inv_scale, z = dinv r, rho = r.z, ||r||; d = 0 when reset_d.
+// fresh != 0: p = z (first direction).  fresh == 0 (residual replacement): the search
+// direction continues, p = z + beta p with the beta of the last recursive update.
 __global__ void __launch_bounds__(kThreads) k_f32_init(int64_t n, const double* __restrict__ r64,
                                                        const float* __restrict__ dinv32,
-                                                       float* r32, float* z32, float* d32,
-                                                       float* p0, ReduceBuf rb, Scal* s,
-                                                       double inv_scale, double rel_tol,
-                                                       long long maxit)
+                                                       float* __restrict__ r32, float* __restrict__ z32,
+                                                       float* __restrict__ p32, float* __restrict__ d32,
+                                                       int reset_d, int fresh, ReduceBuf rb, Scal* s,
+                                                       double inv_scale)
 {
+    const float beta = fresh ? 0.f : (float)s->beta;
     double v[2] = {0.0, 0.0};
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-         i += (int64_t)gridDim.x * blockDim.x) {
+    for (int64_t i = gtid(); i < n; i += gstride()) {
         const float ri = (float)(r64[i] * inv_scale);
         r32[i] = ri;
         const float zi = ri * dinv32[i];
         z32[i] = zi;
-        d32[i] = 0.f;
-        p0[i] = 0.f;
+        p32[i] = fresh ? zi : fmaf(beta, p32[i], zi);
+        if (reset_d) d32[i] = 0.f;
         v[0] += (double)zi * (double)ri;
         v[1] += (double)ri * (double)ri;
     }
     double t[2];
     if (grid_reduce<2>(v, rb, t) && threadIdx.x == 0) {
-        s->rho = 0.0;
-        s->rho_next = t[0];
+        s->rho = t[0];
         s->norm = sqrt(t[1]);
-        s->tol = rel_tol * sqrt(t[1]);
-        s->iter = 0;
-        s->maxit = maxit;
-        s->pidx = 0;
-        s->status = ST_RUN;
-        s->done = 0;
     }
 }
 
 template <int NB>
-__global__ void __launch_bounds__(kThreads) k_f32_spmv(int64_t n, const float* __restrict__ band,
-                                                       const __grid_constant__ BandOffsets bo,
-                                                       const float* __restrict__ z, float* pa,
-                                                       float* pb, float* __restrict__ q,
+__global__ void __launch_bounds__(kThreads) k_f32_spmv(int64_t n, int64_t npad, const float* __restrict__ band,
+                                                       const __grid_constant__ BandArgs ba,
+                                                       const float* __restrict__ p, float* __restrict__ q,
                                                        ReduceBuf rb, Scal* s)
 {
     if (s->done) return;
-    const double rho = s->rho_next;
-    const bool first = s->iter == 0;
-    const float beta = first ? 0.f : (float)(rho / s->rho);
-    const float* __restrict__ pold = s->pidx ? pb : pa;
-    float* __restrict__ pnew = s->pidx ? pa : pb;
     double v[1] = {0.0};
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-         i += (int64_t)gridDim.x * blockDim.x) {
-        float acc = 0.f;
+    const int64_t ng = (n + 3) >> 2;
+    for (int64_t g = gtid(); g < ng; g += gstride()) {
+        const int64_t i0 = g << 2;
+        float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
+        const bool inner = i0 >= ba.halo && i0 + 3 + ba.halo < n;
 #pragma unroll
         for (int b = 0; b < NB; ++b) {
-            int64_t j = i + bo.off[b];
-            j = j < 0 ? 0 : (j >= n ? n - 1 : j);
-            const float pj = first ? z[j] : fmaf(beta, pold[j], z[j]);
-            acc = fmaf(band[(size_t)b * n + i], pj, acc);
+            const float4 c = __ldcs(reinterpret_cast<const float4*>(band + (size_t)b * npad + i0));
+            const int64_t j = i0 + ba.off[b];
+            float p0, p1, p2, p3;
+            if (inner) {
+                p0 = __ldg(p + j);
+                p1 = __ldg(p + j + 1);
+                p2 = __ldg(p + j + 2);
+                p3 = __ldg(p + j + 3);
+            } else {
+                p0 = __ldg(p + min(max(j, (int64_t)0), n - 1));
+                p1 = __ldg(p + min(max(j + 1, (int64_t)0), n - 1));
+                p2 = __ldg(p + min(max(j + 2, (int64_t)0), n - 1));
+                p3 = __ldg(p + min(max(j + 3, (int64_t)0), n - 1));
+            }
+            a0 = fmaf(c.x, p0, a0);
+            a1 = fmaf(c.y, p1, a1);
+            a2 = fmaf(c.z, p2, a2);
+            a3 = fmaf(c.w, p3, a3);
         }
-        const float pi = first ? z[i] : fmaf(beta, pold[i], z[i]);
-        pnew[i] = pi;
-        q[i] = acc;
-        v[0] += (double)acc * (double)pi;
+        if (i0 + 3 < n) {
+            st4(q, g, make_float4(a0, a1, a2, a3));
+            const float4 pp = ld4(p, g);
+            v[0] += (double)a0 * pp.x + (double)a1 * pp.y + (double)a2 * pp.z + (double)a3 * pp.w;
+        } else {
+            const float a[4] = {a0, a1, a2, a3};
+            for (int k = 0; k < 4 && i0 + k < n; ++k) {
+                q[i0 + k] = a[k];
+                v[0] += (double)a[k] * p[i0 + k];
+            }
+        }
     }
     double t[1];
     if (grid_reduce<1>(v, rb, t) && threadIdx.x == 0) {
-        s->rho = rho;
         s->delta = t[0];
-        s->alpha = rho / t[0];
+        s->alpha = s->rho / t[0];
         if (!(fabs(t[0]) > 0.0)) {
             s->iter += 1;
             s->status = ST_BREAK;
@@ -535,56 +600,86 @@ __global__ void __launch_bounds__(kThreads) k_f32_spmv(int64_t n, const float* _
     }
 }
 
+// d += alpha p; r -= alpha q; z = dinv r; rho_next = r.z and ||r||^2 in FP64; tests; beta
 __global__ void __launch_bounds__(kThreads) k_f32_update(int64_t n, float* __restrict__ d,
                                                          float* __restrict__ r,
                                                          const float* __restrict__ q,
-                                                         const float* pa, const float* pb,
+                                                         const float* __restrict__ p,
                                                          const float* __restrict__ dinv,
-                                                         float* __restrict__ z, ReduceBuf rb,
-                                                         Scal* s)
+                                                         float* __restrict__ z, ReduceBuf rb, Scal* s)
 {
     if (s->done) return;
     const float alpha = (float)s->alpha;
-    const float* __restrict__ pnew = s->pidx ? pa : pb;
     double v[2] = {0.0, 0.0};
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-         i += (int64_t)gridDim.x * blockDim.x) {
-        d[i] = fmaf(alpha, pnew[i], d[i]);
+    const int64_t nv = n >> 2;
+    for (int64_t k = gtid(); k < nv; k += gstride()) {
+        const float4 d0 = ld4(d, k), r0 = ld4(r, k), q0 = ld4(q, k), p0 = ld4(p, k), di = ld4(dinv, k);
+        st4(d, k, make_float4(fmaf(alpha, p0.x, d0.x), fmaf(alpha, p0.y, d0.y), fmaf(alpha, p0.z, d0.z),
+                              fmaf(alpha, p0.w, d0.w)));
+        const float4 rn = make_float4(fmaf(-alpha, q0.x, r0.x), fmaf(-alpha, q0.y, r0.y),
+                                      fmaf(-alpha, q0.z, r0.z), fmaf(-alpha, q0.w, r0.w));
+        st4(r, k, rn);
+        const float4 zn = make_float4(rn.x * di.x, rn.y * di.y, rn.z * di.z, rn.w * di.w);
+        st4(z, k, zn);
+        v[0] += (double)zn.x * rn.x + (double)zn.y * rn.y + (double)zn.z * rn.z + (double)zn.w * rn.w;
+        v[1] += (double)rn.x * rn.x + (double)rn.y * rn.y + (double)rn.z * rn.z + (double)rn.w * rn.w;
+    }
+    if (gtid() < (n & 3)) {
+        const int64_t i = (nv << 2) + gtid();
+        d[i] = fmaf(alpha, p[i], d[i]);
         const float ri = fmaf(-alpha, q[i], r[i]);
         r[i] = ri;
         const float zi = ri * dinv[i];
         z[i] = zi;
-        v[0] += (double)zi * (double)ri;
-        v[1] += (double)ri * (double)ri;
+        v[0] += (double)zi * ri;
+        v[1] += (double)ri * ri;
     }
     double t[2];
     if (grid_reduce<2>(v, rb, t) && threadIdx.x == 0) {
         const long long it = s->iter + 1;
         s->iter = it;
-        s->rho_next = t[0];
         const double norm = sqrt(t[1]);
         s->norm = norm;
-        s->pidx ^= 1;
+        s->beta = t[0] / s->rho;
+        const bool brk = !(fabs(t[0]) > 0.0);
+        s->rho = t[0];
         if (norm <= s->tol) {
             s->status = ST_CONV;
             s->done = 1;
         } else if (it >= s->maxit) {
             s->status = ST_MAXIT;
             s->done = 1;
-        } else if (!(fabs(t[0]) > 0.0)) {
+        } else if (brk) {
             s->status = ST_BREAK;
             s->done = 1;
         }
     }
 }
 
-// x64 += scale * d32
-__global__ void k_add_correction(int64_t n, double* __restrict__ x, const float* __restrict__ d,
-                                 double scale)
+__global__ void __launch_bounds__(kThreads) k_f32_pupdate(int64_t n, const float* __restrict__ z,
+                                                          float* __restrict__ p, const Scal* s)
 {
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-         i += (int64_t)gridDim.x * blockDim.x)
+    if (s->done) return;
+    const float beta = (float)s->beta;
+    const int64_t nv = n >> 2;
+    for (int64_t k = gtid(); k < nv; k += gstride()) {
+        const float4 z0 = ld4(z, k), p0 = ld4(p, k);
+        st4(p, k, make_float4(fmaf(beta, p0.x, z0.x), fmaf(beta, p0.y, z0.y), fmaf(beta, p0.z, z0.z),
+                              fmaf(beta, p0.w, z0.w)));
+    }
+    if (gtid() < (n & 3)) {
+        const int64_t i = (nv << 2) + gtid();
+        p[i] = fmaf(beta, p[i], z[i]);
+    }
+}
+
+// x64 += scale * d32; d32 = 0
+__global__ void k_add_correction(int64_t n, double* __restrict__ x, float* __restrict__ d, double scale)
+{
+    for (int64_t i = gtid(); i < n; i += gstride()) {
         x[i] += scale * (double)d[i];
+        d[i] = 0.f;
+    }
 }
 
 // ------------------------------------------------------------------ host helpers
@@ -601,25 +696,40 @@ int read_scal(Workspace* w)
     return RG_OK;
 }
 
+// set device scalars from the host (stream-ordered)
+int write_scal_fields(Workspace* w, double tol, long long maxit, long long iter0)
+{
+    Scal h = *w->hs;
+    h.tol = tol;
+    h.maxit = maxit;
+    h.iter = iter0;
+    h.done = 0;
+    h.status = ST_RUN;
+    *w->hs = h;
+    RG_CHECK_CUDA(cudaMemcpyAsync(w->s, w->hs, sizeof(Scal), cudaMemcpyHostToDevice, stream()));
+    return RG_OK;
+}
+
 ReduceBuf rbuf(Workspace* w) { return ReduceBuf{w->partials, w->counter}; }
 
 // iterations per host poll: about 1 ms of device work, at least 4
 int chunk_for(int64_t n, int64_t bytes_per_row)
 {
-    const double iter_s = (double)n * bytes_per_row / 5.0e12 + 6e-6;
+    const double iter_s = (double)n * bytes_per_row / 5.0e12 + 8e-6;
     int c = (int)(1e-3 / iter_s);
     return c < 4 ? 4 : (c > 256 ? 256 : c);
 }
 
-// runs PCG iterations until the device flags done; returns iterations and status
-using IterFn = int (*)(Matrix*, int);
+using IterFn = int (*)(Matrix*);
+
+// runs PCG iterations until the device flags done
 int run_until_done(Matrix* m, IterFn step, int chunk, long long cap, long long* iters, int* status)
 {
     Workspace* w = m->ws;
     long long launched = 0;
     for (;;) {
         for (int c = 0; c < chunk; ++c) {
-            int rc = step(m, c);
+            int rc = step(m);
             if (rc) return rc;
         }
         launched += chunk;
@@ -636,46 +746,54 @@ int run_until_done(Matrix* m, IterFn step, int chunk, long long cap, long long* 
     return RG_OK;
 }
 
-int paso_step(Matrix* m, int)
+int paso_step(Matrix* m)
 {
     Workspace* w = m->ws;
     const Domain* d = m->dom;
-    RG_TIMED(T_PASO_SPMV, (k_paso_spmv<<<w->grid, kThreads, 0, stream()>>>(d->n, d->ptr, d->idx, m->val, w->z, w->p[0], w->p[1],
-                                                   w->q, rbuf(w), w->s)));
-    RG_TIMED(T_PASO_UPDATE1, (k_paso_update1<<<w->grid, kThreads, 0, stream()>>>(d->n, w->r, w->q, w->rs, w->x2, w->p[0], w->p[1],
-                                                      m->dinv, w->z, rbuf(w), w->s)));
-    RG_TIMED(T_PASO_UPDATE2, (k_paso_update2<<<w->grid, kThreads, 0, stream()>>>(d->n, w->rs, w->r, w->x, w->x2, rbuf(w), w->s)));
+    RG_TIMED(T_PASO_SPMV, (k_paso_spmv<<<w->grid_rows, kThreads, 0, stream()>>>(
+                              d->n, d->ptr, d->idx, m->val, w->p, w->q, rbuf(w), w->s)));
+    RG_TIMED(T_PASO_UPDATE1, (k_paso_update1<<<w->grid_vec, kThreads, 0, stream()>>>(
+                                 d->n, w->r, w->q, w->rs, w->x2, w->p, m->dinv, w->z, rbuf(w), w->s)));
+    RG_TIMED(T_PASO_UPDATE2, (k_paso_update2<<<w->grid_vec, kThreads, 0, stream()>>>(
+                                 d->n, w->rs, w->r, w->x, w->x2, w->z, w->p, rbuf(w), w->s)));
     RG_CHECK_LAUNCH();
     return RG_OK;
 }
 
-int std_step(Matrix* m, int)
+int std_step(Matrix* m)
 {
     Workspace* w = m->ws;
     const Domain* d = m->dom;
-    RG_TIMED(T_STD_SPMV, (k_std_spmv<<<w->grid, kThreads, 0, stream()>>>(d->n, d->ptr, d->idx, m->val, w->z, w->p[0], w->p[1],
-                                                  w->q, rbuf(w), w->s)));
-    RG_TIMED(T_STD_UPDATE, (k_std_update<<<w->grid, kThreads, 0, stream()>>>(d->n, w->x, w->r, w->q, w->p[0], w->p[1], m->dinv,
-                                                    w->z, rbuf(w), w->s)));
+    RG_TIMED(T_STD_SPMV, (k_std_spmv<<<w->grid_rows, kThreads, 0, stream()>>>(d->n, d->ptr, d->idx, m->val, w->p,
+                                                                              w->q, rbuf(w), w->s)));
+    RG_TIMED(T_STD_UPDATE, (k_std_update<<<w->grid_vec, kThreads, 0, stream()>>>(d->n, w->x, w->r, w->q, w->p,
+                                                                                 m->dinv, w->z, rbuf(w), w->s)));
+    RG_TIMED(T_VECTOR, (k_std_pupdate<<<w->grid_vec, kThreads, 0, stream()>>>(d->n, w->z, w->p, w->s)));
     RG_CHECK_LAUNCH();
     return RG_OK;
 }
 
-int f32_step(Matrix* m, int)
+int f32_step(Matrix* m)
 {
     Workspace* w = m->ws;
     const Domain* d = m->dom;
-    const int grid = grid_for(d->n, kThreads, 8);
-    BandOffsets bo;
-    for (int b = 0; b < d->nbands; ++b) bo.off[b] = (int)d->band_off[b];
+    BandArgs ba;
+    int64_t h = 0;
+    for (int b = 0; b < d->nbands; ++b) {
+        ba.off[b] = (int)d->band_off[b];
+        h = std::max<int64_t>(h, std::abs(d->band_off[b]));
+    }
+    ba.halo = h;
+    const int gs = grid_for((d->n + 3) / 4, kThreads, 8);
     if (d->nbands == 27)
-        RG_TIMED(T_F32_SPMV, (k_f32_spmv<27><<<grid, kThreads, 0, stream()>>>(d->n, m->band32, bo, w->z32, w->p32[0], w->p32[1],
-                                                       w->q32, rbuf(w), w->s)));
+        RG_TIMED(T_F32_SPMV, (k_f32_spmv<27><<<gs, kThreads, 0, stream()>>>(d->n, d->npad, m->band32, ba, w->p32,
+                                                                            w->q32, rbuf(w), w->s)));
     else
-        RG_TIMED(T_F32_SPMV, (k_f32_spmv<9><<<grid, kThreads, 0, stream()>>>(d->n, m->band32, bo, w->z32, w->p32[0], w->p32[1],
-                                                      w->q32, rbuf(w), w->s)));
-    RG_TIMED(T_F32_UPDATE, (k_f32_update<<<grid, kThreads, 0, stream()>>>(d->n, w->d32, w->r32, w->q32, w->p32[0], w->p32[1],
-                                                 m->dinv32, w->z32, rbuf(w), w->s)));
+        RG_TIMED(T_F32_SPMV, (k_f32_spmv<9><<<gs, kThreads, 0, stream()>>>(d->n, d->npad, m->band32, ba, w->p32,
+                                                                           w->q32, rbuf(w), w->s)));
+    RG_TIMED(T_F32_UPDATE, (k_f32_update<<<w->grid_vec, kThreads, 0, stream()>>>(
+                               d->n, w->d32, w->r32, w->q32, w->p32, m->dinv32, w->z32, rbuf(w), w->s)));
+    RG_TIMED(T_VECTOR, (k_f32_pupdate<<<w->grid_vec, kThreads, 0, stream()>>>(d->n, w->z32, w->p32, w->s)));
     RG_CHECK_LAUNCH();
     return RG_OK;
 }
@@ -687,7 +805,7 @@ int prepare(Matrix* m, bool want_band)
     Workspace* w = m->ws;
     const bool need_band = want_band && !m->band32;
     if (need_band) {
-        RG_CHECK_CUDA(cudaMalloc((void**)&m->band32, sizeof(float) * d->nbands * d->n));
+        RG_CHECK_CUDA(cudaMalloc((void**)&m->band32, sizeof(float) * d->nbands * d->npad));
         if (!m->dinv32) RG_CHECK_CUDA(cudaMalloc((void**)&m->dinv32, sizeof(float) * d->n));
         m->solver_ready = false;
     }
@@ -708,15 +826,171 @@ int prepare(Matrix* m, bool want_band)
     return RG_OK;
 }
 
+struct OuterState {
+    double n2b, nmb;
+    double last2, lastm;
+    long long totIter;
+};
+
+// r = B b - A x and the paso dual-norm test (Solver.cpp:190-248).  Returns RG_OK with
+// *conv set, or an error status (NaN, divergence).
+int outer_residual(Matrix* m, const rg_solver_opts* o, OuterState& st, rg_diag& dg, bool* conv,
+                   double* n2r, double* nmr, bool first)
+{
+    Workspace* w = m->ws;
+    const Domain* d = m->dom;
+    RG_TIMED(T_RESIDUAL, (k_residual<<<w->grid_rows, kThreads, 0, stream()>>>(d->n, d->ptr, d->idx, m->val, w->x,
+                                                                              w->bb, w->r, rbuf(w), w->s)));
+    RG_CHECK_LAUNCH();
+    int rc = read_scal(w);
+    if (rc) return rc;
+    *n2r = std::sqrt(w->hs->n2);
+    *nmr = w->hs->nm;
+    dg.residual_norm = *n2r;
+    dg.residual_max = *nmr;
+    dg.num_outer++;
+    if (o->verbose) printf("Solver: Step %lld: l2/lmax-norm of residual is %g/%g", st.totIter, *n2r, *nmr);
+    if (std::isnan(*n2r)) {
+        if (o->verbose) printf("\n");
+        set_error("Solver: Matrix or right hand side contains undefined values.");
+        return RG_NAN;
+    }
+    if (!first && *n2r >= st.last2 && *nmr >= st.lastm) {
+        if (o->verbose) printf(" divergence!\n");
+        set_error("Solver: No improvement during iteration. Iterative solver gives up.");
+        return RG_DIVERGENCE;
+    }
+    *conv = !(*n2r > o->tolerance * st.n2b || *nmr > o->tolerance * st.nmb);
+    if (*conv) {
+        if (o->verbose) printf(" convergence!\n");
+        dg.converged = 1;
+    }
+    return RG_OK;
+}
+
+int status_from(int st, long long it, const rg_solver_opts* o, long long totIter, bool* restart)
+{
+    *restart = false;
+    if (st == ST_CONV) {
+        *restart = true;
+        return RG_OK;
+    }
+    if (st == ST_MAXIT) {
+        if (o->verbose) printf("Solver: Maximum number of iterations reached.\n");
+        set_error("Solver: maximum number of iteration steps reached.\nReturned solution does not fulfil stopping criterion.");
+        return RG_MAXITER;
+    }
+    if (st == ST_BREAK) {
+        if (it <= 1) {
+            if (o->verbose) printf("Solver: Uncurable break down!\n");
+            set_error("Solver: fatal break down in iterative solver.");
+            return RG_BREAKDOWN;
+        }
+        if (o->verbose) printf("Solver: Breakdown at iter %lld. Restarting ...\n", totIter);
+        *restart = true;
+        return RG_OK;
+    }
+    return RG_OK;
+}
+
+// paso Solver() outer loop around the paso or the textbook FP64 PCG
+int solve_fp64(Matrix* m, const rg_solver_opts* o, bool paso, OuterState& st, rg_diag& dg)
+{
+    Workspace* w = m->ws;
+    const int64_t n = m->dom->n;
+    const int chunk = chunk_for(n, paso ? 12 * 27 + 160 : 12 * 27 + 112);
+    bool first = true;
+    for (;;) {
+        const long long cnt = o->iter_max - st.totIter;
+        bool conv = false;
+        double n2r = 0, nmr = 0;
+        int rc = outer_residual(m, o, st, dg, &conv, &n2r, &nmr, first);
+        first = false;
+        if (rc || conv) return rc;
+        const double tol = o->tolerance * std::fmin(st.n2b, 0.1 * n2r / nmr * st.nmb);
+        if (o->verbose) printf(" (new tolerance = %g).\n", tol);
+        st.last2 = n2r;
+        st.lastm = nmr;
+        long long it = 0;
+        int dst = ST_RUN;
+        if (paso) {
+            RG_TIMED(T_VECTOR, (k_paso_init<<<w->grid_rows, kThreads, 0, stream()>>>(
+                                   n, w->r, w->x, m->dinv, w->rs, w->x2, w->p, w->z, rbuf(w), w->s, tol, cnt)));
+            RG_CHECK_LAUNCH();
+            if ((rc = run_until_done(m, paso_step, chunk, cnt, &it, &dst))) return rc;
+        } else {
+            RG_TIMED(T_VECTOR, (k_std_init<<<w->grid_rows, kThreads, 0, stream()>>>(
+                                   n, w->r, m->dinv, w->z, w->p, rbuf(w), w->s, tol, cnt > 0 ? cnt : 1)));
+            RG_CHECK_LAUNCH();
+            if ((rc = run_until_done(m, std_step, chunk, cnt, &it, &dst))) return rc;
+        }
+        st.totIter += it;
+        bool restart = false;
+        rc = status_from(dst, it, o, st.totIter, &restart);
+        if (rc || !restart) return rc;
+    }
+}
+
+// FP32 PCG with FP64 residual replacement
+int solve_f32(Matrix* m, const rg_solver_opts* o, OuterState& st, rg_diag& dg)
+{
+    Workspace* w = m->ws;
+    const int64_t n = m->dom->n;
+    const int eg = grid_for(n, kThreads, 8);
+    const int chunk = chunk_for(n, 4 * 27 + 64);
+    const double seg = std::fmin(std::fmax(o->inner_tolerance > 0 ? o->inner_tolerance : 1e-3, 1e-6), 0.5);
+    const double scale = st.nmb;  // fixed FP32 scaling of the recurrence
+    bool conv = false;
+    double n2r = 0, nmr = 0;
+    int rc = outer_residual(m, o, st, dg, &conv, &n2r, &nmr, true);
+    if (rc || conv) return rc;
+    bool first = true;
+    long long done_iters = 0;
+    for (;;) {
+        // (re)seed the FP32 recurrence from the FP64 residual; keep p after the first time
+        RG_TIMED(T_VECTOR, (k_f32_init<<<eg, kThreads, 0, stream()>>>(n, w->r, m->dinv32, w->r32, w->z32, w->p32,
+                                                                      w->d32, first ? 1 : 0, first ? 1 : 0, rbuf(w),
+                                                                      w->s, 1.0 / scale)));
+        RG_CHECK_LAUNCH();
+        if ((rc = read_scal(w))) return rc;
+        const double norm0 = w->hs->norm;  // ||r32||
+        // stop this segment when the recursive residual has dropped by `seg`, or below
+        // what the dual-norm test needs (with a margin for the FP32 recurrence)
+        const double need = 0.5 * o->tolerance * std::fmin(st.n2b, 0.1 * n2r / nmr * st.nmb) / scale;
+        const double tol = std::fmax(need, seg * norm0);
+        const long long cap = o->iter_max - st.totIter;
+        if ((rc = write_scal_fields(w, tol, cap > 0 ? cap : 1, 0))) return rc;
+        long long it = 0;
+        int dst = ST_RUN;
+        if ((rc = run_until_done(m, f32_step, chunk, cap, &it, &dst))) return rc;
+        st.totIter += it;
+        done_iters += it;
+        // fold the FP32 correction into x and test the FP64 true residual
+        RG_TIMED(T_VECTOR, (k_add_correction<<<eg, kThreads, 0, stream()>>>(n, w->x, w->d32, scale)));
+        RG_CHECK_LAUNCH();
+        st.last2 = n2r;
+        st.lastm = nmr;
+        rc = outer_residual(m, o, st, dg, &conv, &n2r, &nmr, false);
+        if (rc || conv) return rc;
+        if (o->verbose) printf(" (FP32 segment of %lld iterations).\n", it);
+        bool restart = false;
+        rc = status_from(dst, it, o, st.totIter, &restart);
+        if (rc) return rc;
+        if (dst == ST_BREAK) first = true;  // restart the recurrence after a breakdown
+        else first = false;
+        (void)done_iters;
+    }
+}
+
 }  // namespace
 
 void free_workspace(Matrix* m)
 {
     Workspace* w = m->ws;
     if (!w) return;
-    double* dd[] = {w->r, w->x, w->rs, w->x2, w->q, w->z, w->p[0], w->p[1], w->bb, w->partials};
+    double* dd[] = {w->r, w->x, w->rs, w->x2, w->q, w->z, w->p, w->bb, w->partials};
     for (double* p : dd) cudaFree(p);
-    float* ff[] = {w->r32, w->d32, w->q32, w->z32, w->p32[0], w->p32[1]};
+    float* ff[] = {w->r32, w->d32, w->q32, w->z32, w->p32};
     for (float* p : ff) cudaFree(p);
     cudaFree(w->counter);
     cudaFree(w->s);
@@ -750,21 +1024,24 @@ int solve(Matrix* m, const double* rhs, double* x, const rg_solver_opts* o, rg_d
     if ((rc = prepare(m, fp32))) return rc;
     const double t_setup = now_s();
     dg.set_up_time = t_setup - t_start;
-    const int grid = w->grid;
-    const ReduceBuf rb = rbuf(w);
-    const double tolerance = o->tolerance;
 
     // r = B b and its norms (Solver.cpp:104-130)
-    RG_TIMED(T_NORMS, (k_scale_norms<<<grid, kThreads, 0, stream()>>>(n, m->bv, rhs, w->bb, rb, w->s)));
+    RG_TIMED(T_NORMS, (k_scale_norms<<<w->grid_vec, kThreads, 0, stream()>>>(n, m->bv, rhs, w->bb, rbuf(w), w->s)));
     RG_CHECK_LAUNCH();
     if ((rc = read_scal(w))) return rc;
-    const double n2b = std::sqrt(w->hs->n2), nmb = w->hs->nm;
-    dg.rhs_norm = n2b;
+    OuterState st;
+    st.n2b = std::sqrt(w->hs->n2);
+    st.nmb = w->hs->nm;
+    st.last2 = st.n2b;
+    st.lastm = st.nmb;
+    st.totIter = 1;
+    dg.rhs_norm = st.n2b;
     int status = RG_OK;
-    if (std::isnan(n2b) || std::isnan(nmb)) {
+    const int eg = grid_for(n, kThreads, 8);
+    if (std::isnan(st.n2b) || std::isnan(st.nmb)) {
         set_error("Solver: Matrix or right hand side contains undefined values.");
         status = RG_NAN;
-    } else if (n2b <= 0.) {
+    } else if (st.n2b <= 0.) {
         RG_CHECK_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * n, stream()));
         dg.converged = 1;
         if (o->verbose) printf("right hand side is identical to zero.\n");
@@ -773,9 +1050,8 @@ int solve(Matrix* m, const double* rhs, double* x, const rg_solver_opts* o, rg_d
             printf("Solver: l2/lmax-norm of right hand side is %g/%g.\n"
                    "Solver: l2/lmax-stopping criterion is %g/%g.\n"
                    "Solver: Iterative method is PCG.\n",
-                   n2b, nmb, n2b * tolerance, nmb * tolerance);
+                   st.n2b, st.nmb, st.n2b * o->tolerance, st.nmb * o->tolerance);
         // initial guess: Jacobi of B b in paso (Solver.cpp:181); x0 / B or 0 otherwise
-        const int eg = grid_for(n, kThreads, 8);
         if (paso) {
             RG_TIMED(T_VECTOR, (k_mul<<<eg, kThreads, 0, stream()>>>(n, m->dinv, w->bb, w->x)));
         } else if (o->initial_guess) {
@@ -785,97 +1061,14 @@ int solve(Matrix* m, const double* rhs, double* x, const rg_solver_opts* o, rg_d
         }
         RG_CHECK_LAUNCH();
         const double t_net = now_s();
-        long long totIter = 1;
-        double last2 = n2b, lastm = nmb;
-        bool fin = false;
-        const int chunk_paso = chunk_for(n, 12 * 27 + 152);
-        const int chunk_std = chunk_for(n, 12 * 27 + 96);
-        const int chunk_f32 = chunk_for(n, 4 * 27 + 48);
-        while (!fin) {
-            long long cnt = o->iter_max - totIter;
-            fin = true;
-            // r = B b - A x, norms (Solver.cpp:190-224)
-            RG_TIMED(T_RESIDUAL, (k_residual<<<grid, kThreads, 0, stream()>>>(n, d->ptr, d->idx, m->val, w->x, w->bb, w->r, rb, w->s)));
-            RG_CHECK_LAUNCH();
-            if ((rc = read_scal(w))) return rc;
-            const double n2r = std::sqrt(w->hs->n2), nmr = w->hs->nm;
-            dg.residual_norm = n2r;
-            dg.residual_max = nmr;
-            dg.num_outer++;
-            if (o->verbose) printf("Solver: Step %lld: l2/lmax-norm of residual is %g/%g", totIter, n2r, nmr);
-            if (std::isnan(n2r)) {
-                set_error("Solver: Matrix or right hand side contains undefined values.");
-                status = RG_NAN;
-                break;
-            }
-            if (totIter > 1 && n2r >= last2 && nmr >= lastm) {
-                if (o->verbose) printf(" divergence!\n");
-                set_error("Solver: No improvement during iteration. Iterative solver gives up.");
-                status = RG_DIVERGENCE;
-                break;
-            }
-            if (!(n2r > tolerance * n2b || nmr > tolerance * nmb)) {
-                if (o->verbose) printf(" convergence!\n");
-                dg.converged = 1;
-                break;
-            }
-            double tol = tolerance * std::fmin(n2b, 0.1 * n2r / nmr * nmb);
-            if (o->verbose) printf(" (new tolerance = %g).\n", tol);
-            last2 = n2r;
-            lastm = nmr;
-            long long it = 0;
-            int st = ST_RUN;
-            if (paso) {
-                RG_TIMED(T_VECTOR, (k_paso_init<<<grid, kThreads, 0, stream()>>>(n, w->r, w->x, m->dinv, w->rs, w->x2, w->p[0], w->z,
-                                                            rb, w->s, tol, cnt)));
-                RG_CHECK_LAUNCH();
-                if ((rc = run_until_done(m, paso_step, chunk_paso, cnt, &it, &st))) return rc;
-            } else if (!fp32) {
-                RG_TIMED(T_VECTOR, (k_std_init<<<grid, kThreads, 0, stream()>>>(n, w->r, m->dinv, w->z, w->p[0], rb, w->s, tol,
-                                                           cnt > 0 ? cnt : 1)));
-                RG_CHECK_LAUNCH();
-                if ((rc = run_until_done(m, std_step, chunk_std, cnt, &it, &st))) return rc;
-            } else {
-                // FP32 inner solve of A d = r / s, relative reduction eta
-                const double need = tol / n2r;
-                const double eta = std::fmax(need, o->inner_tolerance > 0 ? o->inner_tolerance : 1e-5);
-                const double scale = nmr;
-                RG_TIMED(T_VECTOR, (k_f32_init<<<grid_for(n, kThreads, 8), kThreads, 0, stream()>>>(
-                    n, w->r, m->dinv32, w->r32, w->z32, w->d32, w->p32[0], rb, w->s, 1.0 / scale, eta,
-                    cnt > 0 ? cnt : 1)));
-                RG_CHECK_LAUNCH();
-                if ((rc = run_until_done(m, f32_step, chunk_f32, cnt, &it, &st))) return rc;
-                RG_TIMED(T_VECTOR, (k_add_correction<<<grid_for(n, kThreads, 8), kThreads, 0, stream()>>>(n, w->x, w->d32, scale)));
-                RG_CHECK_LAUNCH();
-                if (st == ST_CONV || st == ST_MAXIT) {
-                    // a converged or exhausted inner solve still improves x; the outer
-                    // residual decides
-                }
-            }
-            totIter += it;
-            if (st == ST_CONV) {
-                fin = false;
-            } else if (st == ST_MAXIT) {
-                if (o->verbose) printf("Solver: Maximum number of iterations reached.\n");
-                set_error("Solver: maximum number of iteration steps reached.\nReturned solution does not fulfil stopping criterion.");
-                status = RG_MAXITER;
-                break;
-            } else if (st == ST_BREAK) {
-                if (it <= 1) {
-                    if (o->verbose) printf("Solver: Uncurable break down!\n");
-                    set_error("Solver: fatal break down in iterative solver.");
-                    status = RG_BREAKDOWN;
-                    break;
-                }
-                if (o->verbose) printf("Solver: Breakdown at iter %lld. Restarting ...\n", totIter);
-                fin = false;
-            }
-        }
+        status = fp32 ? solve_f32(m, o, st, dg) : solve_fp64(m, o, paso, st, dg);
         dg.net_time = now_s() - t_net;
-        dg.num_iter = totIter;
-        // x = B x (Solver.cpp:326)
-        RG_TIMED(T_VECTOR, (k_mul<<<eg, kThreads, 0, stream()>>>(n, m->bv, w->x, x)));
-        RG_CHECK_LAUNCH();
+        dg.num_iter = st.totIter;
+        if (status == RG_OK || status == RG_MAXITER) {
+            // x = B x (Solver.cpp:326)
+            RG_TIMED(T_VECTOR, (k_mul<<<eg, kThreads, 0, stream()>>>(n, m->bv, w->x, x)));
+            RG_CHECK_LAUNCH();
+        }
     }
     RG_CHECK_CUDA(cudaStreamSynchronize(stream()));
     dg.time = now_s() - t_start;

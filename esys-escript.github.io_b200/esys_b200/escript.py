@@ -629,12 +629,15 @@ class SolverBuddy:
 
     # diagnostics (SolverBuddy::getDiagnostics)
     def resetDiagnostics(self, all=False):
+        """SolverBuddy::resetDiagnostics: the cumulative items survive unless all=True."""
+        cum = {k: v for k, v in getattr(self, "_SolverBuddy__diag", {}).items() if k.startswith("cum_")}
         self.__diag = {"num_iter": 0, "num_level": 0, "num_inner_iter": 0, "time": 0.0,
                        "set_up_time": 0.0, "net_time": 0.0, "residual_norm": 0.0,
                        "converged": False, "num_outer": 0}
-        if all:
-            self.__diag.update({"cum_num_iter": 0, "cum_time": 0.0, "cum_set_up_time": 0.0,
-                                "cum_net_time": 0.0, "cum_num_inner_iter": 0})
+        if all or not cum:
+            cum = {"cum_num_iter": 0, "cum_time": 0.0, "cum_set_up_time": 0.0,
+                   "cum_net_time": 0.0, "cum_num_inner_iter": 0}
+        self.__diag.update(cum)
 
     def _updateDiagnostics(self, d: "L.rg_diag"):
         self.__diag.update(num_iter=int(d.num_iter), num_outer=int(d.num_outer),
