@@ -136,7 +136,7 @@ int rg_domain_create(int dim, const int64_t ne[3], const double x0[3], const dou
     }
     d.n = n;
     d.nnz = nnz;
-    d.npad = (n + 31) / 32 * 32;
+    d.npad = (n + 255) / 256 * 256;  // whole 256-row tiles of the band SpMV
     d.nbands = dim == 3 ? 27 : 9;
     for (int b = 0; b < d.nbands; ++b) {
         const int bx = b % 3 - 1, by = (b / 3) % 3 - 1, bz = dim == 3 ? b / 9 - 1 : 0;

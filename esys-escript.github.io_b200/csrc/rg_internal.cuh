@@ -12,6 +12,7 @@ namespace rg {
 
 // ---------------------------------------------------------------- error plumbing
 void set_error(const std::string& msg);
+void set_stream(cudaStream_t s);
 const std::string& last_error();
 cudaStream_t stream();
 
@@ -58,7 +59,7 @@ struct Domain {
     int32_t* ptr = nullptr;  // device CSR pattern
     int32_t* idx = nullptr;
     int nbands;              // 27 (3D) or 9 (2D)
-    int64_t npad;            // band stride: n rounded up to a multiple of 32
+    int64_t npad;            // band stride: n rounded up to a multiple of 256
     int64_t band_off[27];    // column offset of band b: dx + NN0*dy + NN0*NN1*dz
     Q1Tables q1;
 };
@@ -188,6 +189,9 @@ enum TimerKind {
 void timer_begin(int kind);
 void timer_end(int kind);
 void timers_collect();  // folds finished event pairs into the totals (syncs the events)
+bool timers_on();
+void timers_snapshot(long long out[T_COUNT]);  // launch counters
+void timers_add(const long long delta[T_COUNT], long long times);
 
 #define RG_TIMED(kind, launch) \
     do {                       \

@@ -62,6 +62,15 @@ struct Workspace {
     int* bad = nullptr;
     int grid_rows = 0;   // CSR row-group kernels
     int grid_vec = 0;    // elementwise kernels
+    // solves run on a private stream (ordered after and before the caller's stream) so
+    // that chunks of iterations can be captured and replayed as CUDA graphs
+    cudaStream_t priv = nullptr;
+    cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+    cudaEvent_t poll_ev[2] = {nullptr, nullptr};
+    Scal* hpoll = nullptr;                   // 2 pinned slots for pipelined polling
+    cudaGraphExec_t graph[3] = {nullptr, nullptr, nullptr};
+    int graph_chunk[3] = {0, 0, 0};
+    long long graph_launches[3][T_COUNT] = {};
 };
 
 namespace {
@@ -90,6 +99,12 @@ int ensure_workspace(Matrix* m, bool fp32)
             (rc = dalloc(&w->s, 1)) || (rc = dalloc(&w->bad, 1)))
             return rc;
         RG_CHECK_CUDA(cudaMallocHost((void**)&w->hs, sizeof(Scal)));
+        RG_CHECK_CUDA(cudaMallocHost((void**)&w->hpoll, 2 * sizeof(Scal)));
+        RG_CHECK_CUDA(cudaStreamCreateWithFlags(&w->priv, cudaStreamNonBlocking));
+        RG_CHECK_CUDA(cudaEventCreateWithFlags(&w->ev_in, cudaEventDisableTiming));
+        RG_CHECK_CUDA(cudaEventCreateWithFlags(&w->ev_out, cudaEventDisableTiming));
+        RG_CHECK_CUDA(cudaEventCreateWithFlags(&w->poll_ev[0], cudaEventDisableTiming));
+        RG_CHECK_CUDA(cudaEventCreateWithFlags(&w->poll_ev[1], cudaEventDisableTiming));
         RG_CHECK_CUDA(cudaMemsetAsync(w->counter, 0, sizeof(unsigned), stream()));
     }
     Workspace* w = m->ws;
@@ -600,6 +615,182 @@ __global__ void __launch_bounds__(kThreads) k_f32_spmv(int64_t n, int64_t npad, 
     }
 }
 
+// ---- TMA-pipelined band SpMV ---------------------------------------------------------------
+// Persistent, one CTA per SM.  A tile is kTile consecutive rows; for each tile one thread
+// issues bulk copies (cp.async.bulk, completion counted on an mbarrier) of the 27 band
+// segments band[b*npad + i0 .. +kTile) and, for interior tiles, of the 9 windows of p that
+// the tile's neighbours span (one per (dy,dz) column of the stencil, kTile+8 values from a
+// 16-byte aligned start) into a kStages-deep ring of shared-memory stages.  Threads compute
+// their row from shared memory while later tiles are in flight.  Tiles whose p windows would
+// leave [0, n) read p with clamped loads instead.  Every wait is bounded: on timeout the
+// kernel records ST_TIMEOUT in the scalars and returns.
+constexpr int kTile = 256;
+constexpr int kStages = 4;
+constexpr int kPWin = kTile + 8;
+enum { ST_TIMEOUT = 6 };
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p)
+{
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar)
+{
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+
+struct TmaBandArgs {
+    int off[27];     // column offset of band b
+    int goff[9];     // column offset of group g = (dy,dz) at dx = -1
+    int64_t n, npad;
+    int64_t halo;    // largest |offset|
+};
+
+template <int NB>
+__global__ void __launch_bounds__(kTile, 1) k_f32_spmv_tma(const float* __restrict__ band,
+                                                           const __grid_constant__ TmaBandArgs ta,
+                                                           const float* __restrict__ p,
+                                                           float* __restrict__ q, ReduceBuf rb, Scal* s)
+{
+    constexpr int NG = NB / 3;  // stencil columns (dy,dz)
+    constexpr int kStageFloats = NB * kTile + NG * kPWin;
+    extern __shared__ __align__(128) float smem[];
+    __shared__ __align__(8) uint64_t bars[kStages];
+    __shared__ int bad;
+    if (s->done) return;
+    const int t = threadIdx.x;
+    const int64_t n = ta.n;
+    const int64_t ntiles = (n + kTile - 1) / kTile;
+    // tiles of this CTA: blockIdx.x, blockIdx.x + gridDim.x, ...
+    const int64_t my_tiles = blockIdx.x < ntiles ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+    if (t == 0) {
+        for (int k = 0; k < kStages; ++k) mbar_init(&bars[k], 1);
+        bad = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+
+    auto interior = [&](int64_t i0) { return i0 - ta.halo - 8 >= 0 && i0 + kTile + ta.halo + 8 <= n; };
+    auto issue = [&](int64_t k) {  // tile number k of this CTA into stage k % kStages
+        const int st = (int)(k % kStages);
+        const int64_t i0 = (blockIdx.x + k * gridDim.x) * (int64_t)kTile;
+        float* dst = smem + (size_t)st * kStageFloats;
+        const bool in = interior(i0);
+        const uint32_t bytes = NB * kTile * 4 + (in ? NG * kPWin * 4 : 0);
+        mbar_expect_tx(&bars[st], bytes);
+        for (int b = 0; b < NB; ++b) bulk_g2s(dst + b * kTile, band + (size_t)b * ta.npad + i0, kTile * 4, &bars[st]);
+        if (in)
+            for (int g = 0; g < NG; ++g) {
+                const int64_t a = (i0 + ta.goff[g]) & ~(int64_t)3;
+                bulk_g2s(dst + NB * kTile + g * kPWin, p + a, kPWin * 4, &bars[st]);
+            }
+    };
+
+    if (t == 0)
+        for (int64_t k = 0; k < kStages - 1 && k < my_tiles; ++k) issue(k);
+
+    double v[1] = {0.0};
+    for (int64_t k = 0; k < my_tiles; ++k) {
+        const int st = (int)(k % kStages);
+        if (t == 0 && k + kStages - 1 < my_tiles) {
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            issue(k + kStages - 1);
+        }
+        // bounded wait for this tile's copies
+        const uint32_t parity = (uint32_t)((k / kStages) & 1);
+        int tries = 0;
+        while (!mbar_try_wait(&bars[st], parity)) {
+            if (++tries > (1 << 22)) {
+                bad = 1;
+                break;
+            }
+        }
+        const float* bs = smem + (size_t)st * kStageFloats;
+        const int64_t i0 = (blockIdx.x + k * gridDim.x) * (int64_t)kTile;
+        const int64_t i = i0 + t;
+        float acc = 0.f, pi = 0.f;
+        if (interior(i0)) {
+            const float* pw = bs + NB * kTile;
+#pragma unroll
+            for (int g = 0; g < NG; ++g) {
+                const int base = (int)((i0 + ta.goff[g]) - ((i0 + ta.goff[g]) & ~(int64_t)3)) + t;
+                const float* w = pw + g * kPWin + base;
+                acc = fmaf(bs[(3 * g + 0) * kTile + t], w[0], acc);
+                acc = fmaf(bs[(3 * g + 1) * kTile + t], w[1], acc);
+                acc = fmaf(bs[(3 * g + 2) * kTile + t], w[2], acc);
+                if (3 * g + 1 == NB / 2) pi = w[1];
+            }
+        } else {
+#pragma unroll
+            for (int b = 0; b < NB; ++b) {
+                const int64_t j = min(max(i + ta.off[b], (int64_t)0), n - 1);
+                const float pj = __ldg(p + j);
+                acc = fmaf(bs[b * kTile + t], pj, acc);
+                if (b == NB / 2) pi = pj;
+            }
+        }
+        if (i < n) {
+            q[i] = acc;
+            v[0] += (double)acc * (double)pi;
+        }
+        __syncthreads();  // stage st is free for the copy issued in a later iteration
+        if (bad) {
+            // give the copies already issued for later tiles a bounded chance to land
+            // before the CTA's shared memory is released
+            if (t == 0)
+                for (int64_t kk = k + 1; kk < my_tiles && kk < k + kStages; ++kk) {
+                    const uint32_t par = (uint32_t)((kk / kStages) & 1);
+                    for (int tries = 0; tries < (1 << 20) && !mbar_try_wait(&bars[kk % kStages], par); ++tries) {
+                    }
+                }
+            break;
+        }
+    }
+    if (bad) {
+        if (t == 0) {
+            s->status = ST_TIMEOUT;
+            s->done = 1;
+        }
+        return;
+    }
+    double tt[1];
+    if (grid_reduce<1>(v, rb, tt) && threadIdx.x == 0) {
+        s->delta = tt[0];
+        s->alpha = s->rho / tt[0];
+        if (!(fabs(tt[0]) > 0.0)) {
+            s->iter += 1;
+            s->status = ST_BREAK;
+            s->done = 1;
+        }
+    }
+}
+
 // d += alpha p; r -= alpha q; z = dinv r; rho_next = r.z and ||r||^2 in FP64; tests; beta
 __global__ void __launch_bounds__(kThreads) k_f32_update(int64_t n, float* __restrict__ d,
                                                          float* __restrict__ r,
@@ -722,27 +913,101 @@ int chunk_for(int64_t n, int64_t bytes_per_row)
 
 using IterFn = int (*)(Matrix*);
 
-// runs PCG iterations until the device flags done
-int run_until_done(Matrix* m, IterFn step, int chunk, long long cap, long long* iters, int* status)
+bool graphs_enabled()
+{
+    static int on = -1;
+    if (on < 0) {
+        const char* e = getenv("RG_GRAPHS");
+        on = (e && e[0] == '0') ? 0 : 1;
+    }
+    return on == 1 && !timers_on();
+}
+
+// runs PCG iterations until the device flags done.  Chunks of `chunk` iterations are
+// captured once per (matrix, kind) as a CUDA graph and replayed; the done flag of chunk
+// k is read while chunk k+1 is already queued, so the device never waits for the host.
+// Kernels of a chunk that follow convergence return at once.  With kernel timers on the
+// steps are launched directly (events cannot be timed inside a replayed graph).
+int run_until_done(Matrix* m, int kind, IterFn step, int chunk, long long cap, long long* iters,
+                   int* status)
 {
     Workspace* w = m->ws;
     long long launched = 0;
-    for (;;) {
-        for (int c = 0; c < chunk; ++c) {
-            int rc = step(m);
+    if (!graphs_enabled()) {
+        for (;;) {
+            for (int c = 0; c < chunk; ++c) {
+                int rc = step(m);
+                if (rc) return rc;
+            }
+            launched += chunk;
+            int rc = read_scal(w);
             if (rc) return rc;
+            if (w->hs->done) break;
+            if (launched > cap + 2 * chunk + 8) {
+                set_error("PCG iteration loop did not terminate");
+                return RG_TIMEOUT;
+            }
         }
-        launched += chunk;
-        int rc = read_scal(w);
+        *iters = w->hs->iter;
+        *status = w->hs->status;
+        return RG_OK;
+    }
+    if (!w->graph[kind] || w->graph_chunk[kind] != chunk) {
+        if (w->graph[kind]) cudaGraphExecDestroy(w->graph[kind]);
+        w->graph[kind] = nullptr;
+        long long before[T_COUNT], after[T_COUNT];
+        timers_snapshot(before);
+        RG_CHECK_CUDA(cudaStreamBeginCapture(stream(), cudaStreamCaptureModeThreadLocal));
+        int rc = RG_OK;
+        for (int c = 0; c < chunk && rc == RG_OK; ++c) rc = step(m);
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamEndCapture(stream(), &g);
         if (rc) return rc;
-        if (w->hs->done) break;
-        if (launched > cap + 2 * chunk + 8) {
+        if (e != cudaSuccess) {
+            set_error(std::string("graph capture: ") + cudaGetErrorString(e));
+            return RG_CUDA_ERROR;
+        }
+        e = cudaGraphInstantiate(&w->graph[kind], g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) {
+            set_error(std::string("graph instantiate: ") + cudaGetErrorString(e));
+            return RG_CUDA_ERROR;
+        }
+        w->graph_chunk[kind] = chunk;
+        timers_snapshot(after);
+        long long undo[T_COUNT];
+        for (int k = 0; k < T_COUNT; ++k) {
+            w->graph_launches[kind][k] = after[k] - before[k];
+            undo[k] = before[k] - after[k];
+        }
+        timers_add(undo, 1);  // captured launches are counted when replayed
+    }
+    int k = 0;
+    const Scal* last = nullptr;
+    for (;;) {
+        RG_CHECK_CUDA(cudaGraphLaunch(w->graph[kind], stream()));
+        timers_add(w->graph_launches[kind], 1);
+        RG_CHECK_CUDA(cudaMemcpyAsync(&w->hpoll[k & 1], w->s, sizeof(Scal), cudaMemcpyDeviceToHost, stream()));
+        RG_CHECK_CUDA(cudaEventRecord(w->poll_ev[k & 1], stream()));
+        launched += chunk;
+        if (k >= 1) {
+            RG_CHECK_CUDA(cudaEventSynchronize(w->poll_ev[(k - 1) & 1]));
+            if (w->hpoll[(k - 1) & 1].done) {
+                last = &w->hpoll[k & 1];
+                break;
+            }
+        }
+        if (launched > cap + 3 * chunk + 8) {
+            RG_CHECK_CUDA(cudaStreamSynchronize(stream()));
             set_error("PCG iteration loop did not terminate");
             return RG_TIMEOUT;
         }
+        ++k;
     }
-    *iters = w->hs->iter;
-    *status = w->hs->status;
+    RG_CHECK_CUDA(cudaEventSynchronize(w->poll_ev[k & 1]));
+    *w->hs = *last;
+    *iters = last->iter;
+    *status = last->status;
     return RG_OK;
 }
 
@@ -773,24 +1038,62 @@ int std_step(Matrix* m)
     return RG_OK;
 }
 
+int sm_count()
+{
+    static int count = 0;
+    if (!count) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&count, cudaDevAttrMultiProcessorCount, dev);
+        if (count <= 0) count = kNumSMs;
+    }
+    return count;
+}
+
+template <int NB>
+int launch_f32_spmv_tma(Matrix* m)
+{
+    Workspace* w = m->ws;
+    const Domain* d = m->dom;
+    constexpr int NG = NB / 3;
+    const size_t smem = sizeof(float) * kStages * (NB * kTile + NG * kPWin);
+    TmaBandArgs ta;
+    int64_t h = 0;
+    for (int b = 0; b < NB; ++b) {
+        ta.off[b] = (int)d->band_off[b];
+        h = std::max<int64_t>(h, std::abs(d->band_off[b]));
+    }
+    for (int g = 0; g < NG; ++g) ta.goff[g] = (int)d->band_off[3 * g];  // dx = -1 member
+    ta.n = d->n;
+    ta.npad = d->npad;
+    ta.halo = h;
+    const int64_t ntiles = (d->n + kTile - 1) / kTile;
+    const int grid = (int)std::min<int64_t>(ntiles, sm_count());
+    RG_TIMED(T_F32_SPMV, (k_f32_spmv_tma<NB><<<grid, kTile, smem, stream()>>>(m->band32, ta, w->p32, w->q32,
+                                                                             rbuf(w), w->s)));
+    RG_CHECK_LAUNCH();
+    return RG_OK;
+}
+
+int tma_attributes()
+{
+    static bool done = false;
+    if (!done) {
+        RG_CHECK_CUDA(cudaFuncSetAttribute(k_f32_spmv_tma<27>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)(sizeof(float) * kStages * (27 * kTile + 9 * kPWin))));
+        RG_CHECK_CUDA(cudaFuncSetAttribute(k_f32_spmv_tma<9>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)(sizeof(float) * kStages * (9 * kTile + 3 * kPWin))));
+        done = true;
+    }
+    return RG_OK;
+}
+
 int f32_step(Matrix* m)
 {
     Workspace* w = m->ws;
     const Domain* d = m->dom;
-    BandArgs ba;
-    int64_t h = 0;
-    for (int b = 0; b < d->nbands; ++b) {
-        ba.off[b] = (int)d->band_off[b];
-        h = std::max<int64_t>(h, std::abs(d->band_off[b]));
-    }
-    ba.halo = h;
-    const int gs = grid_for((d->n + 3) / 4, kThreads, 8);
-    if (d->nbands == 27)
-        RG_TIMED(T_F32_SPMV, (k_f32_spmv<27><<<gs, kThreads, 0, stream()>>>(d->n, d->npad, m->band32, ba, w->p32,
-                                                                            w->q32, rbuf(w), w->s)));
-    else
-        RG_TIMED(T_F32_SPMV, (k_f32_spmv<9><<<gs, kThreads, 0, stream()>>>(d->n, d->npad, m->band32, ba, w->p32,
-                                                                           w->q32, rbuf(w), w->s)));
+    int rc = d->nbands == 27 ? launch_f32_spmv_tma<27>(m) : launch_f32_spmv_tma<9>(m);
+    if (rc) return rc;
     RG_TIMED(T_F32_UPDATE, (k_f32_update<<<w->grid_vec, kThreads, 0, stream()>>>(
                                d->n, w->d32, w->r32, w->q32, w->p32, m->dinv32, w->z32, rbuf(w), w->s)));
     RG_TIMED(T_VECTOR, (k_f32_pupdate<<<w->grid_vec, kThreads, 0, stream()>>>(d->n, w->z32, w->p32, w->s)));
@@ -808,6 +1111,10 @@ int prepare(Matrix* m, bool want_band)
         RG_CHECK_CUDA(cudaMalloc((void**)&m->band32, sizeof(float) * d->nbands * d->npad));
         if (!m->dinv32) RG_CHECK_CUDA(cudaMalloc((void**)&m->dinv32, sizeof(float) * d->n));
         m->solver_ready = false;
+    }
+    if (want_band) {
+        int rc = tma_attributes();
+        if (rc) return rc;
     }
     if (m->balanced && m->solver_ready) return RG_OK;
     if (!m->dinv) RG_CHECK_CUDA(cudaMalloc((void**)&m->dinv, sizeof(double) * d->n));
@@ -917,12 +1224,12 @@ int solve_fp64(Matrix* m, const rg_solver_opts* o, bool paso, OuterState& st, rg
             RG_TIMED(T_VECTOR, (k_paso_init<<<w->grid_rows, kThreads, 0, stream()>>>(
                                    n, w->r, w->x, m->dinv, w->rs, w->x2, w->p, w->z, rbuf(w), w->s, tol, cnt)));
             RG_CHECK_LAUNCH();
-            if ((rc = run_until_done(m, paso_step, chunk, cnt, &it, &dst))) return rc;
+            if ((rc = run_until_done(m, 0, paso_step, chunk, cnt, &it, &dst))) return rc;
         } else {
             RG_TIMED(T_VECTOR, (k_std_init<<<w->grid_rows, kThreads, 0, stream()>>>(
                                    n, w->r, m->dinv, w->z, w->p, rbuf(w), w->s, tol, cnt > 0 ? cnt : 1)));
             RG_CHECK_LAUNCH();
-            if ((rc = run_until_done(m, std_step, chunk, cnt, &it, &dst))) return rc;
+            if ((rc = run_until_done(m, 1, std_step, chunk, cnt, &it, &dst))) return rc;
         }
         st.totIter += it;
         bool restart = false;
@@ -962,7 +1269,7 @@ int solve_f32(Matrix* m, const rg_solver_opts* o, OuterState& st, rg_diag& dg)
         if ((rc = write_scal_fields(w, tol, cap > 0 ? cap : 1, 0))) return rc;
         long long it = 0;
         int dst = ST_RUN;
-        if ((rc = run_until_done(m, f32_step, chunk, cap, &it, &dst))) return rc;
+        if ((rc = run_until_done(m, 2, f32_step, chunk, cap, &it, &dst))) return rc;
         st.totIter += it;
         done_iters += it;
         // fold the FP32 correction into x and test the FP64 true residual
@@ -996,13 +1303,63 @@ void free_workspace(Matrix* m)
     cudaFree(w->s);
     cudaFree(w->bad);
     cudaFreeHost(w->hs);
+    cudaFreeHost(w->hpoll);
+    for (int k = 0; k < 3; ++k)
+        if (w->graph[k]) cudaGraphExecDestroy(w->graph[k]);
+    if (w->ev_in) cudaEventDestroy(w->ev_in);
+    if (w->ev_out) cudaEventDestroy(w->ev_out);
+    for (int k = 0; k < 2; ++k)
+        if (w->poll_ev[k]) cudaEventDestroy(w->poll_ev[k]);
+    if (w->priv) cudaStreamDestroy(w->priv);
     delete w;
     m->ws = nullptr;
 }
 
+namespace {
+int solve_impl(Matrix* m, const double* rhs, double* x, const rg_solver_opts* o, rg_diag* diag,
+               double t_start);
+
+// runs the solve on the workspace's private stream, ordered after the caller's pending
+// work and before the caller's later work
+struct PrivateStream {
+    cudaStream_t caller;
+    Workspace* w;
+    bool ok = false;
+    PrivateStream(Workspace* ws) : caller(stream()), w(ws)
+    {
+        if (cudaEventRecord(w->ev_in, caller) != cudaSuccess) return;
+        if (cudaStreamWaitEvent(w->priv, w->ev_in, 0) != cudaSuccess) return;
+        set_stream(w->priv);
+        ok = true;
+    }
+    ~PrivateStream()
+    {
+        if (!ok) return;
+        cudaEventRecord(w->ev_out, w->priv);
+        cudaStreamWaitEvent(caller, w->ev_out, 0);
+        set_stream(caller);
+    }
+};
+}  // namespace
+
 int solve(Matrix* m, const double* rhs, double* x, const rg_solver_opts* o, rg_diag* diag)
 {
     const double t_start = now_s();
+    const bool fp32 = o->precision == RG_PREC_FP32_REFINE;
+    int rc = ensure_workspace(m, fp32);
+    if (rc) return rc;
+    PrivateStream ps(m->ws);
+    if (!ps.ok) {
+        set_error("solver: cannot order the private stream after the caller's stream");
+        return RG_CUDA_ERROR;
+    }
+    return solve_impl(m, rhs, x, o, diag, t_start);
+}
+
+namespace {
+int solve_impl(Matrix* m, const double* rhs, double* x, const rg_solver_opts* o, rg_diag* diag,
+               double t_start)
+{
     rg_diag dg{};
     Domain* d = m->dom;
     const int64_t n = d->n;
@@ -1079,5 +1436,7 @@ int solve(Matrix* m, const double* rhs, double* x, const rg_solver_opts* o, rg_d
     }
     return status;
 }
+
+}  // namespace
 
 }  // namespace rg

@@ -91,6 +91,24 @@ void timers_collect()
     g_pending.clear();
 }
 
+bool timers_on()
+{
+    std::lock_guard<std::mutex> lk(g_mu);
+    return g_on;
+}
+
+void timers_snapshot(long long out[T_COUNT])
+{
+    std::lock_guard<std::mutex> lk(g_mu);
+    for (int k = 0; k < T_COUNT; ++k) out[k] = g_launches[k];
+}
+
+void timers_add(const long long delta[T_COUNT], long long times)
+{
+    std::lock_guard<std::mutex> lk(g_mu);
+    for (int k = 0; k < T_COUNT; ++k) g_launches[k] += delta[k] * times;
+}
+
 }  // namespace rg
 
 extern "C" {
