@@ -127,8 +127,9 @@ __global__ void __launch_bounds__(256) k_row_balance(int64_t n, const int32_t* _
 // a_ij *= bv_i*bv_j, followed by the Jacobi data of the balanced matrix
 // (SparseMatrix::invMain, paso/src/SparseMatrix.cpp:387-435): dinv_i = 1/a~_ii; a zero or
 // missing diagonal sets *bad.  With band != null the balanced row is also copied into the
-// FP32 band layout band[b*npad + i], b = (dx+1) + 3(dy+1) (+ 9(dz+1)).
-__global__ void __launch_bounds__(256) k_apply_balance(int64_t n, int64_t npad, int dim, int64_t NN0, int64_t NN1,
+// tile-major FP32 band layout: band[((i/256)*nbands + b)*256 + i%256],
+// b = (dx+1) + 3(dy+1) (+ 9(dz+1)).
+__global__ void __launch_bounds__(256) k_apply_balance(int64_t n, int nbands, int dim, int64_t NN0, int64_t NN1,
                                                        const int32_t* __restrict__ ptr,
                                                        const int32_t* __restrict__ idx,
                                                        double* __restrict__ val,
@@ -164,7 +165,7 @@ __global__ void __launch_bounds__(256) k_apply_balance(int64_t n, int64_t npad, 
                     const int64_t xj = j % NN0, yj = (j / NN0) % NN1, zj = j / plane;
                     int b = (int)(xj - xi + 1) + 3 * (int)(yj - yi + 1);
                     if (dim == 3) b += 9 * (int)(zj - zi + 1);
-                    band[(size_t)b * npad + row] = (float)a;
+                    band[((size_t)(row >> 8) * nbands + b) * 256 + (row & 255)] = (float)a;
                 }
             }
         }
@@ -223,7 +224,7 @@ int launch_balance(Matrix* m, int scale, int* d_bad, bool want_band)
         RG_CHECK_LAUNCH();
     }
     if (want_band) RG_CHECK_CUDA(cudaMemsetAsync(m->band32, 0, sizeof(float) * d->nbands * d->npad, stream()));
-    RG_TIMED(T_BALANCE, (k_apply_balance<<<grid, 256, 0, stream()>>>(d->n, d->npad, d->dim, d->nn[0], d->nn[1], d->ptr, d->idx, m->val,
+    RG_TIMED(T_BALANCE, (k_apply_balance<<<grid, 256, 0, stream()>>>(d->n, d->nbands, d->dim, d->nn[0], d->nn[1], d->ptr, d->idx, m->val,
                                                 m->bv, scale, m->dinv, m->dinv32,
                                                 want_band ? m->band32 : nullptr, d_bad)));
     RG_CHECK_LAUNCH();

@@ -42,6 +42,7 @@ struct Scal {
     double rho;                // textbook PCG: r.z
     double n2, nm;             // norms from norm kernels
     long long iter, maxit;
+    long long pk;              // FP32 path: parity counter of the two search-direction buffers
     int done, status, pad0, pad1;
 };
 
@@ -54,7 +55,8 @@ struct Workspace {
     double *r = nullptr, *x = nullptr, *rs = nullptr, *x2 = nullptr, *q = nullptr, *z = nullptr;
     double* p = nullptr;
     double* bb = nullptr;  // balanced rhs
-    float *r32 = nullptr, *d32 = nullptr, *q32 = nullptr, *z32 = nullptr, *p32 = nullptr;
+    float *r32 = nullptr, *d32 = nullptr, *q32 = nullptr, *z32 = nullptr;
+    float* p32[2] = {nullptr, nullptr};
     double* partials = nullptr;
     unsigned* counter = nullptr;
     Scal* s = nullptr;   // device scalars
@@ -111,7 +113,7 @@ int ensure_workspace(Matrix* m, bool fp32)
     if (fp32 && !w->r32) {
         int rc;
         if ((rc = dalloc(&w->r32, n)) || (rc = dalloc(&w->d32, n)) || (rc = dalloc(&w->q32, n)) ||
-            (rc = dalloc(&w->z32, n)) || (rc = dalloc(&w->p32, n)))
+            (rc = dalloc(&w->z32, n)) || (rc = dalloc(&w->p32[0], n)) || (rc = dalloc(&w->p32[1], n)))
             return rc;
     }
     return RG_OK;
@@ -519,114 +521,20 @@ __global__ void __launch_bounds__(kThreads) k_std_pupdate(int64_t n, const doubl
 }
 
 // ------------------------------------------------------------------ FP32 PCG on the band copy
-// band[b*npad + i] holds row i's coefficient to neighbour i + off_b (0 where there is
-// none; padding rows are 0).  A thread owns 4 consecutive rows: one 16-byte streaming
-// load per band, four neighbour values of p per band (L1/L2 hits).  Near the two ends of
-// the vector the neighbour indices are clamped into range, where the band value is 0.
-struct BandArgs {
-    int off[27];
-    int64_t halo;  // max |off|
-};
-
-// r32 = r64 * inv_scale, z = dinv r, rho = r.z, ||r||; d = 0 when reset_d.
-// fresh != 0: p = z (first direction).  fresh == 0 (residual replacement): the search
-// direction continues, p = z + beta p with the beta of the last recursive update.
-__global__ void __launch_bounds__(kThreads) k_f32_init(int64_t n, const double* __restrict__ r64,
-                                                       const float* __restrict__ dinv32,
-                                                       float* __restrict__ r32, float* __restrict__ z32,
-                                                       float* __restrict__ p32, float* __restrict__ d32,
-                                                       int reset_d, int fresh, ReduceBuf rb, Scal* s,
-                                                       double inv_scale)
-{
-    const float beta = fresh ? 0.f : (float)s->beta;
-    double v[2] = {0.0, 0.0};
-    for (int64_t i = gtid(); i < n; i += gstride()) {
-        const float ri = (float)(r64[i] * inv_scale);
-        r32[i] = ri;
-        const float zi = ri * dinv32[i];
-        z32[i] = zi;
-        p32[i] = fresh ? zi : fmaf(beta, p32[i], zi);
-        if (reset_d) d32[i] = 0.f;
-        v[0] += (double)zi * (double)ri;
-        v[1] += (double)ri * (double)ri;
-    }
-    double t[2];
-    if (grid_reduce<2>(v, rb, t) && threadIdx.x == 0) {
-        s->rho = t[0];
-        s->norm = sqrt(t[1]);
-    }
-}
-
-template <int NB>
-__global__ void __launch_bounds__(kThreads) k_f32_spmv(int64_t n, int64_t npad, const float* __restrict__ band,
-                                                       const __grid_constant__ BandArgs ba,
-                                                       const float* __restrict__ p, float* __restrict__ q,
-                                                       ReduceBuf rb, Scal* s)
-{
-    if (s->done) return;
-    double v[1] = {0.0};
-    const int64_t ng = (n + 3) >> 2;
-    for (int64_t g = gtid(); g < ng; g += gstride()) {
-        const int64_t i0 = g << 2;
-        float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
-        const bool inner = i0 >= ba.halo && i0 + 3 + ba.halo < n;
-#pragma unroll
-        for (int b = 0; b < NB; ++b) {
-            const float4 c = __ldcs(reinterpret_cast<const float4*>(band + (size_t)b * npad + i0));
-            const int64_t j = i0 + ba.off[b];
-            float p0, p1, p2, p3;
-            if (inner) {
-                p0 = __ldg(p + j);
-                p1 = __ldg(p + j + 1);
-                p2 = __ldg(p + j + 2);
-                p3 = __ldg(p + j + 3);
-            } else {
-                p0 = __ldg(p + min(max(j, (int64_t)0), n - 1));
-                p1 = __ldg(p + min(max(j + 1, (int64_t)0), n - 1));
-                p2 = __ldg(p + min(max(j + 2, (int64_t)0), n - 1));
-                p3 = __ldg(p + min(max(j + 3, (int64_t)0), n - 1));
-            }
-            a0 = fmaf(c.x, p0, a0);
-            a1 = fmaf(c.y, p1, a1);
-            a2 = fmaf(c.z, p2, a2);
-            a3 = fmaf(c.w, p3, a3);
-        }
-        if (i0 + 3 < n) {
-            st4(q, g, make_float4(a0, a1, a2, a3));
-            const float4 pp = ld4(p, g);
-            v[0] += (double)a0 * pp.x + (double)a1 * pp.y + (double)a2 * pp.z + (double)a3 * pp.w;
-        } else {
-            const float a[4] = {a0, a1, a2, a3};
-            for (int k = 0; k < 4 && i0 + k < n; ++k) {
-                q[i0 + k] = a[k];
-                v[0] += (double)a[k] * p[i0 + k];
-            }
-        }
-    }
-    double t[1];
-    if (grid_reduce<1>(v, rb, t) && threadIdx.x == 0) {
-        s->delta = t[0];
-        s->alpha = s->rho / t[0];
-        if (!(fabs(t[0]) > 0.0)) {
-            s->iter += 1;
-            s->status = ST_BREAK;
-            s->done = 1;
-        }
-    }
-}
-
-// ---- TMA-pipelined band SpMV ---------------------------------------------------------------
-// Persistent, one CTA per SM.  A tile is kTile consecutive rows; for each tile one thread
-// issues bulk copies (cp.async.bulk, completion counted on an mbarrier) of the 27 band
-// segments band[b*npad + i0 .. +kTile) and, for interior tiles, of the 9 windows of p that
-// the tile's neighbours span (one per (dy,dz) column of the stencil, kTile+8 values from a
-// 16-byte aligned start) into a kStages-deep ring of shared-memory stages.  Threads compute
-// their row from shared memory while later tiles are in flight.  Tiles whose p windows would
-// leave [0, n) read p with clamped loads instead.  Every wait is bounded: on timeout the
-// kernel records ST_TIMEOUT in the scalars and returns.
+// Tile-major band layout: rows are grouped in tiles of kTile; tile T's coefficients are
+// band[(T*NB + b)*kTile + t] for row T*kTile + t and band b (neighbour i + off_b; 0 where
+// there is none, and in padding rows), so one tile's whole matrix slice is one contiguous
+// NB*kTile*4-byte block.
+//
+// Iteration (two kernels): the SpMV kernel forms the search direction p = z + beta p_old
+// (beta = 0 on a fresh start) from staged windows of z and p_old, writes p to the other
+// buffer, and computes q = A p and p.q; the update kernel does d += alpha p, r -= alpha q,
+// z = dinv r and the FP64 reductions r.z and r.r.  p alternates between two buffers by
+// the parity counter s->pk.
 constexpr int kTile = 256;
-constexpr int kStages = 4;
+constexpr int kStages = 3;
 constexpr int kPWin = kTile + 8;
+constexpr int kConsumerWarps = kTile / 32;
 enum { ST_TIMEOUT = 6 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p)
@@ -645,6 +553,11 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes)
                  : "memory");
 }
 
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
 {
     uint32_t ok;
@@ -656,6 +569,21 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
     return ok != 0;
 }
 
+// bounded wait; false when it gave up
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity)
+{
+    for (int tries = 0; tries < (1 << 22); ++tries)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+
+__device__ __forceinline__ uint64_t evict_first_policy()
+{
+    uint64_t pol;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
+
 __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar)
 {
     asm volatile(
@@ -665,114 +593,176 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
         : "memory");
 }
 
+__device__ __forceinline__ void bulk_g2s_hint(void* dst, const void* src, uint32_t bytes, uint64_t* bar,
+                                              uint64_t pol)
+{
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], "
+        "%4;" ::"r"(smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar)), "l"(pol)
+        : "memory");
+}
+
 struct TmaBandArgs {
-    int off[27];     // column offset of band b
-    int goff[9];     // column offset of group g = (dy,dz) at dx = -1
-    int64_t n, npad;
-    int64_t halo;    // largest |offset|
+    int off[27];   // column offset of band b
+    int goff[9];   // column offset of stencil column g = (dy,dz) at dx = -1
+    int64_t n;
+    int64_t halo;  // largest |offset|
 };
 
-template <int NB>
-__global__ void __launch_bounds__(kTile, 1) k_f32_spmv_tma(const float* __restrict__ band,
-                                                           const __grid_constant__ TmaBandArgs ta,
-                                                           const float* __restrict__ p,
-                                                           float* __restrict__ q, ReduceBuf rb, Scal* s)
+// r32 = r64 * inv_scale, z = dinv r, rho = r.z, ||r||.  fresh: d = 0, p_old = 0, beta = 0,
+// pk = 0 (a new recurrence).  Otherwise (residual replacement) the direction continues:
+// beta is rescaled to the replaced rho.
+__global__ void __launch_bounds__(kThreads) k_f32_init(int64_t n, const double* __restrict__ r64,
+                                                       const float* __restrict__ dinv32,
+                                                       float* __restrict__ r32, float* __restrict__ z32,
+                                                       float* __restrict__ p0, float* __restrict__ d32,
+                                                       int fresh, ReduceBuf rb, Scal* s, double inv_scale)
 {
-    constexpr int NG = NB / 3;  // stencil columns (dy,dz)
-    constexpr int kStageFloats = NB * kTile + NG * kPWin;
+    double v[2] = {0.0, 0.0};
+    for (int64_t i = gtid(); i < n; i += gstride()) {
+        const float ri = (float)(r64[i] * inv_scale);
+        r32[i] = ri;
+        const float zi = ri * dinv32[i];
+        z32[i] = zi;
+        if (fresh) {
+            p0[i] = 0.f;
+            d32[i] = 0.f;
+        }
+        v[0] += (double)zi * (double)ri;
+        v[1] += (double)ri * (double)ri;
+    }
+    double t[2];
+    if (grid_reduce<2>(v, rb, t) && threadIdx.x == 0) {
+        if (fresh) {
+            s->beta = 0.0;
+            s->pk = 0;
+        } else {
+            s->beta = s->rho > 0 ? s->beta * (t[0] / s->rho) : 0.0;
+        }
+        s->rho = t[0];
+        s->norm = sqrt(t[1]);
+    }
+}
+
+// Warp-specialised, persistent (one CTA per SM): warp kConsumerWarps is the producer, its
+// lane 0 streams, per tile, the tile's band block (one bulk copy, L2 evict-first) and, for
+// interior tiles, the 2*NG windows of z and p_old its stencil columns span (kTile+8 values
+// from a 16-byte aligned start) into a kStages ring; consumer warps compute one row per
+// thread from shared memory and release the stage through an `empty` mbarrier.  Tiles near
+// the two ends read z and p_old with clamped loads.  All waits are bounded: on timeout the
+// kernel records ST_TIMEOUT and returns.
+template <int NB>
+__global__ void __launch_bounds__(kTile + 32, 1) k_f32_spmv_tma(const float* __restrict__ band,
+                                                                const __grid_constant__ TmaBandArgs ta,
+                                                                const float* __restrict__ z,
+                                                                float* __restrict__ P0, float* __restrict__ P1,
+                                                                float* __restrict__ q, ReduceBuf rb, Scal* s)
+{
+    constexpr int NG = NB / 3;
+    constexpr int kBand = NB * kTile;
+    constexpr int kWin = NG * kPWin;
+    constexpr int kStage = kBand + 2 * kWin;
     extern __shared__ __align__(128) float smem[];
-    __shared__ __align__(8) uint64_t bars[kStages];
+    __shared__ __align__(8) uint64_t full[kStages], empty[kStages];
     __shared__ int bad;
     if (s->done) return;
+    const float beta = (float)s->beta;
+    const float* __restrict__ pold = (s->pk & 1) ? P1 : P0;
+    float* __restrict__ pnew = (s->pk & 1) ? P0 : P1;
     const int t = threadIdx.x;
+    const int warp = t >> 5;
     const int64_t n = ta.n;
     const int64_t ntiles = (n + kTile - 1) / kTile;
-    // tiles of this CTA: blockIdx.x, blockIdx.x + gridDim.x, ...
     const int64_t my_tiles = blockIdx.x < ntiles ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
     if (t == 0) {
-        for (int k = 0; k < kStages; ++k) mbar_init(&bars[k], 1);
+        for (int k = 0; k < kStages; ++k) {
+            mbar_init(&full[k], 1);
+            mbar_init(&empty[k], kConsumerWarps);
+        }
         bad = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
-
     auto interior = [&](int64_t i0) { return i0 - ta.halo - 8 >= 0 && i0 + kTile + ta.halo + 8 <= n; };
-    auto issue = [&](int64_t k) {  // tile number k of this CTA into stage k % kStages
-        const int st = (int)(k % kStages);
-        const int64_t i0 = (blockIdx.x + k * gridDim.x) * (int64_t)kTile;
-        float* dst = smem + (size_t)st * kStageFloats;
-        const bool in = interior(i0);
-        const uint32_t bytes = NB * kTile * 4 + (in ? NG * kPWin * 4 : 0);
-        mbar_expect_tx(&bars[st], bytes);
-        for (int b = 0; b < NB; ++b) bulk_g2s(dst + b * kTile, band + (size_t)b * ta.npad + i0, kTile * 4, &bars[st]);
-        if (in)
-            for (int g = 0; g < NG; ++g) {
-                const int64_t a = (i0 + ta.goff[g]) & ~(int64_t)3;
-                bulk_g2s(dst + NB * kTile + g * kPWin, p + a, kPWin * 4, &bars[st]);
-            }
-    };
-
-    if (t == 0)
-        for (int64_t k = 0; k < kStages - 1 && k < my_tiles; ++k) issue(k);
 
     double v[1] = {0.0};
-    for (int64_t k = 0; k < my_tiles; ++k) {
-        const int st = (int)(k % kStages);
-        if (t == 0 && k + kStages - 1 < my_tiles) {
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            issue(k + kStages - 1);
+    int64_t issued = 0;
+    if (warp == kConsumerWarps) {
+        // ---------------- producer
+        if ((t & 31) == 0) {
+            const uint64_t pol = evict_first_policy();
+            for (int64_t k = 0; k < my_tiles; ++k, issued = k) {
+                const int st = (int)(k % kStages);
+                if (k >= kStages && !mbar_wait(&empty[st], (uint32_t)(((k / kStages) - 1) & 1))) {
+                    bad = 1;
+                    break;
+                }
+                const int64_t tile = blockIdx.x + k * gridDim.x;
+                const int64_t i0 = tile * kTile;
+                float* dst = smem + (size_t)st * kStage;
+                const bool in = interior(i0);
+                mbar_expect_tx(&full[st], kBand * 4 + (in ? 2 * kWin * 4 : 0));
+                bulk_g2s_hint(dst, band + (size_t)tile * kBand, kBand * 4, &full[st], pol);
+                if (in)
+                    for (int g = 0; g < NG; ++g) {
+                        const int64_t a = (i0 + ta.goff[g]) & ~(int64_t)3;
+                        bulk_g2s(dst + kBand + g * kPWin, z + a, kPWin * 4, &full[st]);
+                        bulk_g2s(dst + kBand + kWin + g * kPWin, pold + a, kPWin * 4, &full[st]);
+                    }
+            }
         }
-        // bounded wait for this tile's copies
-        const uint32_t parity = (uint32_t)((k / kStages) & 1);
-        int tries = 0;
-        while (!mbar_try_wait(&bars[st], parity)) {
-            if (++tries > (1 << 22)) {
+    } else {
+        // ---------------- consumers: row i0 + t of every tile
+        for (int64_t k = 0; k < my_tiles; ++k) {
+            const int st = (int)(k % kStages);
+            if (!mbar_wait(&full[st], (uint32_t)((k / kStages) & 1))) {
                 bad = 1;
                 break;
             }
-        }
-        const float* bs = smem + (size_t)st * kStageFloats;
-        const int64_t i0 = (blockIdx.x + k * gridDim.x) * (int64_t)kTile;
-        const int64_t i = i0 + t;
-        float acc = 0.f, pi = 0.f;
-        if (interior(i0)) {
-            const float* pw = bs + NB * kTile;
+            const float* bs = smem + (size_t)st * kStage;
+            const int64_t i0 = (blockIdx.x + k * gridDim.x) * (int64_t)kTile;
+            const int64_t i = i0 + t;
+            float acc = 0.f, pi = 0.f;
+            if (interior(i0)) {
+                const float* zw = bs + kBand;
+                const float* pw = bs + kBand + kWin;
 #pragma unroll
-            for (int g = 0; g < NG; ++g) {
-                const int base = (int)((i0 + ta.goff[g]) - ((i0 + ta.goff[g]) & ~(int64_t)3)) + t;
-                const float* w = pw + g * kPWin + base;
-                acc = fmaf(bs[(3 * g + 0) * kTile + t], w[0], acc);
-                acc = fmaf(bs[(3 * g + 1) * kTile + t], w[1], acc);
-                acc = fmaf(bs[(3 * g + 2) * kTile + t], w[2], acc);
-                if (3 * g + 1 == NB / 2) pi = w[1];
-            }
-        } else {
+                for (int g = 0; g < NG; ++g) {
+                    const int base = (int)((i0 + ta.goff[g]) & 3) + t + g * kPWin;
 #pragma unroll
-            for (int b = 0; b < NB; ++b) {
-                const int64_t j = min(max(i + ta.off[b], (int64_t)0), n - 1);
-                const float pj = __ldg(p + j);
-                acc = fmaf(bs[b * kTile + t], pj, acc);
-                if (b == NB / 2) pi = pj;
-            }
-        }
-        if (i < n) {
-            q[i] = acc;
-            v[0] += (double)acc * (double)pi;
-        }
-        __syncthreads();  // stage st is free for the copy issued in a later iteration
-        if (bad) {
-            // give the copies already issued for later tiles a bounded chance to land
-            // before the CTA's shared memory is released
-            if (t == 0)
-                for (int64_t kk = k + 1; kk < my_tiles && kk < k + kStages; ++kk) {
-                    const uint32_t par = (uint32_t)((kk / kStages) & 1);
-                    for (int tries = 0; tries < (1 << 20) && !mbar_try_wait(&bars[kk % kStages], par); ++tries) {
+                    for (int m = 0; m < 3; ++m) {
+                        const float pj = fmaf(beta, pw[base + m], zw[base + m]);
+                        acc = fmaf(bs[(3 * g + m) * kTile + t], pj, acc);
+                        if (3 * g + m == NB / 2) pi = pj;
                     }
                 }
-            break;
+            } else {
+#pragma unroll
+                for (int b = 0; b < NB; ++b) {
+                    const int64_t j = min(max(i + ta.off[b], (int64_t)0), n - 1);
+                    const float pj = fmaf(beta, __ldg(pold + j), __ldg(z + j));
+                    acc = fmaf(bs[b * kTile + t], pj, acc);
+                    if (b == NB / 2) pi = pj;
+                }
+            }
+            __syncwarp();
+            if ((t & 31) == 0) mbar_arrive(&empty[st]);
+            if (i < n) {
+                pnew[i] = pi;
+                q[i] = acc;
+                v[0] += (double)acc * (double)pi;
+            }
         }
     }
+    __syncthreads();
     if (bad) {
+        // let the copies this CTA issued land (bounded) before its shared memory is released
+        if (warp == kConsumerWarps && (t & 31) == 0)
+            for (int64_t k = issued > kStages ? issued - kStages : 0; k < issued; ++k)
+                for (int tries = 0; tries < (1 << 20) && !mbar_try_wait(&full[k % kStages], (uint32_t)((k / kStages) & 1));
+                     ++tries) {
+                }
         if (t == 0) {
             s->status = ST_TIMEOUT;
             s->done = 1;
@@ -795,12 +785,13 @@ __global__ void __launch_bounds__(kTile, 1) k_f32_spmv_tma(const float* __restri
 __global__ void __launch_bounds__(kThreads) k_f32_update(int64_t n, float* __restrict__ d,
                                                          float* __restrict__ r,
                                                          const float* __restrict__ q,
-                                                         const float* __restrict__ p,
+                                                         const float* P0, const float* P1,
                                                          const float* __restrict__ dinv,
                                                          float* __restrict__ z, ReduceBuf rb, Scal* s)
 {
     if (s->done) return;
     const float alpha = (float)s->alpha;
+    const float* __restrict__ p = (s->pk & 1) ? P0 : P1;  // the direction just formed
     double v[2] = {0.0, 0.0};
     const int64_t nv = n >> 2;
     for (int64_t k = gtid(); k < nv; k += gstride()) {
@@ -829,6 +820,7 @@ __global__ void __launch_bounds__(kThreads) k_f32_update(int64_t n, float* __res
     if (grid_reduce<2>(v, rb, t) && threadIdx.x == 0) {
         const long long it = s->iter + 1;
         s->iter = it;
+        s->pk += 1;
         const double norm = sqrt(t[1]);
         s->norm = norm;
         s->beta = t[0] / s->rho;
@@ -844,23 +836,6 @@ __global__ void __launch_bounds__(kThreads) k_f32_update(int64_t n, float* __res
             s->status = ST_BREAK;
             s->done = 1;
         }
-    }
-}
-
-__global__ void __launch_bounds__(kThreads) k_f32_pupdate(int64_t n, const float* __restrict__ z,
-                                                          float* __restrict__ p, const Scal* s)
-{
-    if (s->done) return;
-    const float beta = (float)s->beta;
-    const int64_t nv = n >> 2;
-    for (int64_t k = gtid(); k < nv; k += gstride()) {
-        const float4 z0 = ld4(z, k), p0 = ld4(p, k);
-        st4(p, k, make_float4(fmaf(beta, p0.x, z0.x), fmaf(beta, p0.y, z0.y), fmaf(beta, p0.z, z0.z),
-                              fmaf(beta, p0.w, z0.w)));
-    }
-    if (gtid() < (n & 3)) {
-        const int64_t i = (nv << 2) + gtid();
-        p[i] = fmaf(beta, p[i], z[i]);
     }
 }
 
@@ -1056,7 +1031,7 @@ int launch_f32_spmv_tma(Matrix* m)
     Workspace* w = m->ws;
     const Domain* d = m->dom;
     constexpr int NG = NB / 3;
-    const size_t smem = sizeof(float) * kStages * (NB * kTile + NG * kPWin);
+    const size_t smem = sizeof(float) * kStages * (NB * kTile + 2 * NG * kPWin);
     TmaBandArgs ta;
     int64_t h = 0;
     for (int b = 0; b < NB; ++b) {
@@ -1065,12 +1040,11 @@ int launch_f32_spmv_tma(Matrix* m)
     }
     for (int g = 0; g < NG; ++g) ta.goff[g] = (int)d->band_off[3 * g];  // dx = -1 member
     ta.n = d->n;
-    ta.npad = d->npad;
     ta.halo = h;
     const int64_t ntiles = (d->n + kTile - 1) / kTile;
     const int grid = (int)std::min<int64_t>(ntiles, sm_count());
-    RG_TIMED(T_F32_SPMV, (k_f32_spmv_tma<NB><<<grid, kTile, smem, stream()>>>(m->band32, ta, w->p32, w->q32,
-                                                                             rbuf(w), w->s)));
+    RG_TIMED(T_F32_SPMV, (k_f32_spmv_tma<NB><<<grid, kTile + 32, smem, stream()>>>(
+                             m->band32, ta, w->z32, w->p32[0], w->p32[1], w->q32, rbuf(w), w->s)));
     RG_CHECK_LAUNCH();
     return RG_OK;
 }
@@ -1080,9 +1054,9 @@ int tma_attributes()
     static bool done = false;
     if (!done) {
         RG_CHECK_CUDA(cudaFuncSetAttribute(k_f32_spmv_tma<27>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)(sizeof(float) * kStages * (27 * kTile + 9 * kPWin))));
+                                           (int)(sizeof(float) * kStages * (27 * kTile + 2 * 9 * kPWin))));
         RG_CHECK_CUDA(cudaFuncSetAttribute(k_f32_spmv_tma<9>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)(sizeof(float) * kStages * (9 * kTile + 3 * kPWin))));
+                                           (int)(sizeof(float) * kStages * (9 * kTile + 2 * 3 * kPWin))));
         done = true;
     }
     return RG_OK;
@@ -1095,8 +1069,8 @@ int f32_step(Matrix* m)
     int rc = d->nbands == 27 ? launch_f32_spmv_tma<27>(m) : launch_f32_spmv_tma<9>(m);
     if (rc) return rc;
     RG_TIMED(T_F32_UPDATE, (k_f32_update<<<w->grid_vec, kThreads, 0, stream()>>>(
-                               d->n, w->d32, w->r32, w->q32, w->p32, m->dinv32, w->z32, rbuf(w), w->s)));
-    RG_TIMED(T_VECTOR, (k_f32_pupdate<<<w->grid_vec, kThreads, 0, stream()>>>(d->n, w->z32, w->p32, w->s)));
+                               d->n, w->d32, w->r32, w->q32, w->p32[0], w->p32[1], m->dinv32, w->z32, rbuf(w),
+                               w->s)));
     RG_CHECK_LAUNCH();
     return RG_OK;
 }
@@ -1244,7 +1218,7 @@ int solve_f32(Matrix* m, const rg_solver_opts* o, OuterState& st, rg_diag& dg)
     Workspace* w = m->ws;
     const int64_t n = m->dom->n;
     const int eg = grid_for(n, kThreads, 8);
-    const int chunk = chunk_for(n, 4 * 27 + 64);
+    const int chunk = chunk_for(n, 4 * 27 + 60);
     const double seg = std::fmin(std::fmax(o->inner_tolerance > 0 ? o->inner_tolerance : 1e-3, 1e-6), 0.5);
     const double scale = st.nmb;  // fixed FP32 scaling of the recurrence
     bool conv = false;
@@ -1255,8 +1229,8 @@ int solve_f32(Matrix* m, const rg_solver_opts* o, OuterState& st, rg_diag& dg)
     long long done_iters = 0;
     for (;;) {
         // (re)seed the FP32 recurrence from the FP64 residual; keep p after the first time
-        RG_TIMED(T_VECTOR, (k_f32_init<<<eg, kThreads, 0, stream()>>>(n, w->r, m->dinv32, w->r32, w->z32, w->p32,
-                                                                      w->d32, first ? 1 : 0, first ? 1 : 0, rbuf(w),
+        RG_TIMED(T_VECTOR, (k_f32_init<<<eg, kThreads, 0, stream()>>>(n, w->r, m->dinv32, w->r32, w->z32,
+                                                                      w->p32[0], w->d32, first ? 1 : 0, rbuf(w),
                                                                       w->s, 1.0 / scale)));
         RG_CHECK_LAUNCH();
         if ((rc = read_scal(w))) return rc;
@@ -1297,7 +1271,7 @@ void free_workspace(Matrix* m)
     if (!w) return;
     double* dd[] = {w->r, w->x, w->rs, w->x2, w->q, w->z, w->p, w->bb, w->partials};
     for (double* p : dd) cudaFree(p);
-    float* ff[] = {w->r32, w->d32, w->q32, w->z32, w->p32};
+    float* ff[] = {w->r32, w->d32, w->q32, w->z32, w->p32[0], w->p32[1]};
     for (float* p : ff) cudaFree(p);
     cudaFree(w->counter);
     cudaFree(w->s);
