@@ -60,6 +60,7 @@ void free_domain(Domain* d)
 void free_matrix(Matrix* m)
 {
     free_workspace(m);
+    free_residual_scratch(m);
     if (m->val) cudaFree(m->val);
     if (m->bv) cudaFree(m->bv);
     if (m->dinv) cudaFree(m->dinv);
@@ -383,7 +384,7 @@ void rg_solver_opts_default(rg_solver_opts* o)
     o->mode = RG_MODE_PASO;
     o->precision = RG_PREC_FP64;
     o->layout = RG_LAYOUT_CSR;
-    o->inner_tolerance = 1e-5;
+    o->inner_tolerance = 1e-2;
 }
 
 int rg_solve(rg_matrix* mat, const double* rhs, double* x, const rg_solver_opts* opts, rg_diag* diag)

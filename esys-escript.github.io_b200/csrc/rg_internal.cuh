@@ -64,7 +64,8 @@ struct Domain {
     Q1Tables q1;
 };
 
-struct Workspace;  // solver vectors, allocated lazily (rg_solver.cu)
+struct Workspace;        // solver vectors, allocated lazily (rg_solver.cu)
+struct ResidualScratch;  // reduction scratch of rg_residual_norms (rg_residual.cu)
 
 struct Matrix {
     Domain* dom;
@@ -77,6 +78,7 @@ struct Matrix {
     float* band32 = nullptr;   // [nbands][npad] FP32 copy of the balanced matrix
     float* dinv32 = nullptr;
     Workspace* ws = nullptr;
+    ResidualScratch* rs = nullptr;
 };
 
 // ---------------------------------------------------------------- deterministic reductions
@@ -215,6 +217,7 @@ int launch_spmv64(const Domain* d, const double* val, double alpha, const double
 int launch_balance(Matrix* m, int scale, int* d_bad, bool want_band);
 int solve(Matrix* m, const double* rhs, double* x, const rg_solver_opts* o, rg_diag* diag);
 void free_workspace(Matrix* m);
+void free_residual_scratch(Matrix* m);
 
 }  // namespace rg
 

@@ -43,7 +43,9 @@ struct Scal {
     double n2, nm;             // norms from norm kernels
     long long iter, maxit;
     long long pk;              // FP32 path: parity counter of the two search-direction buffers
-    int done, status, pad0, pad1;
+    double best;               // FP32 path: smallest recursive residual norm of the segment
+    int since;                 // iterations since `best` last dropped by 5%
+    int done, status, pad0;
 };
 
 enum { ST_RUN = 0, ST_CONV = 1, ST_MAXIT = 3, ST_BREAK = 4 };
@@ -826,7 +828,16 @@ __global__ void __launch_bounds__(kThreads) k_f32_update(int64_t n, float* __res
         s->beta = t[0] / s->rho;
         const bool brk = !(fabs(t[0]) > 0.0);
         s->rho = t[0];
-        if (norm <= s->tol) {
+        // the FP32 recurrence has stagnated when no new minimum (5% below the best)
+        // appeared for 50 iterations: end the segment so that the FP64 residual is
+        // recomputed and fed back
+        if (norm < 0.95 * s->best) {
+            s->best = norm;
+            s->since = 0;
+        } else {
+            s->since += 1;
+        }
+        if (norm <= s->tol || s->since > 50) {
             s->status = ST_CONV;
             s->done = 1;
         } else if (it >= s->maxit) {
@@ -869,6 +880,8 @@ int write_scal_fields(Workspace* w, double tol, long long maxit, long long iter0
     h.tol = tol;
     h.maxit = maxit;
     h.iter = iter0;
+    h.best = h.norm;
+    h.since = 0;
     h.done = 0;
     h.status = ST_RUN;
     *w->hs = h;
@@ -1219,7 +1232,9 @@ int solve_f32(Matrix* m, const rg_solver_opts* o, OuterState& st, rg_diag& dg)
     const int64_t n = m->dom->n;
     const int eg = grid_for(n, kThreads, 8);
     const int chunk = chunk_for(n, 4 * 27 + 60);
-    const double seg = std::fmin(std::fmax(o->inner_tolerance > 0 ? o->inner_tolerance : 1e-3, 1e-6), 0.5);
+    // segment reduction factor: 1e-2 keeps the FP32 recurrence within a few ulps of the
+    // true residual (smaller factors let it drift and cost iterations)
+    const double seg = std::fmin(std::fmax(o->inner_tolerance > 0 ? o->inner_tolerance : 1e-2, 1e-4), 0.5);
     const double scale = st.nmb;  // fixed FP32 scaling of the recurrence
     bool conv = false;
     double n2r = 0, nmr = 0;

@@ -510,7 +510,7 @@ class SolverBuddy:
         self.__mode = SolverOptions.MODE_PASO
         self.__precision = SolverOptions.PRECISION_FP64
         self.__layout = SolverOptions.LAYOUT_CSR
-        self.__inner_tolerance = 1e-5
+        self.__inner_tolerance = 1e-2
         self.__initial_guess = None
         self.resetDiagnostics(all=True)
 
@@ -769,6 +769,16 @@ class SystemMatrix:
         options._updateDiagnostics(d)
         L.check(st)
 
+    def residualNorms(self, rhs, u):
+        """(||rhs - A u||_2, ||rhs - A u||_inf) of the assembled system."""
+        b = rhs._dev(self._domain._n)
+        x = u._dev(self._domain._n)
+        l2, lm = C.c_double(), C.c_double()
+        L.set_stream_from_torch()
+        L.check(L.lib().rg_residual_norms(self._handle, C.c_void_p(b.data_ptr()), C.c_void_p(x.data_ptr()),
+                                          C.byref(l2), C.byref(lm)))
+        return l2.value, lm.value
+
     def saveMM(self, filename):
         L.check(L.lib().rg_save_mm(self._handle, str(filename).encode()))
 
@@ -982,6 +992,12 @@ class LinearPDE:
             mat, f = self.getSystem()
             self._solution = mat.solve(f, self._options)
         return self._solution
+
+    def getResidualNorms(self, u=None):
+        """l2 and max norms of the residual rhs - A u of the current system
+        (LinearPDE.getResidual measured in paso's stopping norms)."""
+        mat, f = self.getSystem()
+        return mat.residualNorms(f, self.getSolution() if u is None else u)
 
     def isUsingLumping(self):
         return False

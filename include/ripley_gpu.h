@@ -120,6 +120,11 @@ int rg_spmv(rg_matrix* mat, double alpha, const double* x, double beta, double* 
    (NE x Q x ncomp), or ReducedFunction (element mean) when reduced != 0 */
 int rg_interpolate_nodes(const rg_domain* dom, const double* nodal, int ncomp, double* out,
                          int reduced);
+/* norms of rhs - A*x with A the matrix as assembled (also after a solve balanced it in
+   place), like Lsup/L2 of LinearPDE.getResidual (escriptcore/py_src/linearPDEs.py).  The
+   reduction scratch is allocated with the matrix on first use. */
+int rg_residual_norms(rg_matrix* mat, const double* rhs, const double* x, double* l2_host,
+                      double* linf_host);
 /* MatrixMarket coordinate real general, 1-based (SystemMatrix::saveMM) */
 int rg_save_mm(rg_matrix* mat, const char* path);
 
@@ -146,7 +151,8 @@ typedef struct {
     int mode;                   /* RG_MODE_*                                                */
     int precision;              /* RG_PREC_*                                                */
     int layout;                 /* RG_LAYOUT_*                                              */
-    double inner_tolerance;     /* FP32_REFINE: relative reduction per inner solve (1e-5)   */
+    double inner_tolerance;     /* FP32_REFINE: reduction of the FP32 recursive residual    
+                                   between FP64 residual replacements (default 1e-2)      */
     const double* initial_guess;/* STANDARD mode only: device x0 (unbalanced units) or NULL */
 } rg_solver_opts;
 

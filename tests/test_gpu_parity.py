@@ -260,3 +260,32 @@ def test_solver_errors_are_reported(cuda, golden):
     assert st == 0 and dg.converged and not bool(x.any())
     st, _ = R.solve(m, rhs, x, R.opts(sweeps=2))
     assert st == L.RG_NOT_SUPPORTED
+
+
+def _residual_norms(m, rhs_t, x_t):
+    import ctypes
+    l2, lm = ctypes.c_double(), ctypes.c_double()
+    L.check(R.lib().rg_residual_norms(m.h, R.ptr(rhs_t), R.ptr(x_t), ctypes.byref(l2), ctypes.byref(lm)))
+    return l2.value, lm.value
+
+
+def test_residual_norms_before_and_after_balancing(cuda, golden):
+    """rg_residual_norms measures b - A x of the assembled system, also once a solve has
+    balanced the matrix in place."""
+    d, m, rhs, _ = _system(golden, "3d")
+    ne = tuple(int(v) for v in golden["solve3d_ne"])
+    pat = O.pattern(3, ne)
+    val = golden["solve3d_val"]
+    rng = np.random.default_rng(13)
+    x0 = rng.standard_normal(d.n)
+    r = golden["solve3d_rhs"] - O.spmv(pat, val, x0)
+    l2, lm = _residual_norms(m, rhs, R.dev(x0))
+    assert abs(l2 - np.linalg.norm(r)) <= 1e-12 * np.linalg.norm(r)
+    assert abs(lm - np.abs(r).max()) <= 1e-12 * np.abs(r).max()
+    x = torch.zeros(d.n, dtype=torch.float64, device="cuda")
+    assert R.solve(m, rhs, x, R.opts(tolerance=1e-10))[0] == 0
+    l2b, lmb = _residual_norms(m, rhs, R.dev(x0))
+    assert abs(l2b - l2) <= 1e-12 * l2 and abs(lmb - lm) <= 1e-12 * lm
+    # the solution's residual is small relative to the right hand side
+    l2s, _ = _residual_norms(m, rhs, x)
+    assert l2s <= 1e-8 * np.linalg.norm(golden["solve3d_rhs"])
