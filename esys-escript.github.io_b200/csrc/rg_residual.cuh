@@ -16,6 +16,8 @@ constexpr int kMaxBlocks = 148 * 8;                      // grid cap (multiple o
 // grid for n rows (<= kMaxBlocks)
 inline int grid(int64_t n) { return grid_for(n, kRowsPerBlock, 8); }
 
+namespace {  // internal linkage: the kernel may be compiled into several translation units
+
 // out[0] = sum r_i^2, out[1] = max |r_i|; rb is the reduction scratch (partials of
 // gridDim.x * 2 doubles and a zeroed counter)
 __global__ void __launch_bounds__(kThreads) k_residual_norms(int64_t n, const int32_t* __restrict__ ptr,
@@ -54,5 +56,6 @@ __global__ void __launch_bounds__(kThreads) k_residual_norms(int64_t n, const in
     }
 }
 
+}  // namespace
 }  // namespace residual
 }  // namespace rg
