@@ -87,6 +87,8 @@ _SIGNATURES = {
     "rg_save_mm": (C.c_int, [C.c_void_p, C.c_char_p]),
     "rg_residual_norms": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_double),
                                     C.POINTER(C.c_double)]),
+    "rg_residual_norms_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_double),
+                                            C.POINTER(C.c_double)]),
     "rg_solver_opts_default": (None, [C.POINTER(rg_solver_opts)]),
     "rg_solve": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(rg_solver_opts),
                            C.POINTER(rg_diag)]),

@@ -125,6 +125,17 @@ int rg_interpolate_nodes(const rg_domain* dom, const double* nodal, int ncomp, d
    reduction scratch is allocated with the matrix on first use. */
 int rg_residual_norms(rg_matrix* mat, const double* rhs, const double* x, double* l2_host,
                       double* linf_host);
+/* The same residual norms computed without any device allocation: the reduction scratch
+   is a fixed static device array (18,976 bytes, at most 1184 CTAs' partial sums) that every
+   GPU loading the library holds until exit.  No counterpart in the reference: it is for
+   callers that cannot let a library call cudaMalloc (a host whose own pool owns the
+   device memory, or a latency-critical loop that cannot absorb the implicit
+   synchronisation of cudaMalloc/cudaFree).  All calls share the array: calls that overlap
+   on the GPU race and must be serialised.  The first call on a device looks up the array's
+   address (make it before any stream capture).  Sizes whose reduction would need more
+   partial sums than the array holds are rejected with RG_INVALID_ARG. */
+int rg_residual_norms_noalloc(rg_matrix* mat, const double* rhs, const double* x,
+                              double* l2_host, double* linf_host);
 /* MatrixMarket coordinate real general, 1-based (SystemMatrix::saveMM) */
 int rg_save_mm(rg_matrix* mat, const char* path);
 
