@@ -1,0 +1,316 @@
+// 3x3x3 convolutions of the warm-start network on the 5th-generation tensor cores
+// (tcgen05 UMMA, bf16 operands, fp32 accumulators in tensor memory).
+//
+// Activations are bf16, channels-last, with one zero slice before and after every
+// sample along depth: x[z][h][w][c] with z = n*(D+2) + 1 + d, so a 3x3x3 stencil never
+// crosses into the neighbouring sample, and the W/H borders are the zero fill of the TMA
+// loads.
+//
+// Forward (and data-gradient) convolution as an implicit GEMM: one CTA computes a tile of
+// 128 output positions (a BW x BH x BZ box) x Cout channels.  K runs over the 27 taps x
+// Cin/16 channel chunks; for each (tap, chunk) the producer warp loads with TMA the input
+// box shifted by the tap (128 positions x 16 channels, 32-byte swizzle) and the tap's
+// 16-channel weight slice (Cout x 16), the MMA warp issues one 128 x Cout x 16 UMMA into
+// tensor memory and releases the stage through tcgen05.commit, and four epilogue warps
+// read the accumulator (one TMEM lane = one output position per thread), add the bias,
+// apply ReLU and/or the ReLU mask of the layer below (data gradient), and store bf16.
+#include <cuda.h>
+
+#include <string>
+
+#include "rg_internal.cuh"
+#include "ws_conv.cuh"
+
+namespace rg {
+namespace ws {
+
+constexpr int kStages = 8;
+constexpr int kConvThreads = 192;  // warp 0 TMA, warp 1 MMA + TMEM, warps 2-5 epilogue
+constexpr int kATile = 128 * 32;   // 128 positions x 16 bf16
+
+struct ConvArgs {
+    CUtensorMap xmap;  // input: dims (Cin, W, H, Z), box (16, BW, BH, BZ), 32B swizzle
+    CUtensorMap wmap;  // weights [27][Cout][Cin]: dims (Cin, 27*Cout), box (16, Cout), 32B swizzle
+    const float* bias;          // Cout or null
+    __nv_bfloat16* out;         // [Z][H][W][Cout]
+    const __nv_bfloat16* mask;  // [Z][H][W][Cout] or null: out *= (mask > 0)
+    int W, H, D, Cin;
+    int BW, BH, BZ;
+    int tiles_w, tiles_h, tiles_z;
+    int relu;
+    int* err;
+};
+
+template <int COUT>
+struct ConvSmem {
+    static constexpr int kB = COUT * 32;
+    static constexpr int kBPad = (kB + 1023) / 1024 * 1024;
+    static constexpr int kStage = kATile + kBPad;
+    static constexpr int kBytes = kStages * kStage + 1024;  // + alignment slack
+};
+
+template <int COUT>
+__global__ void __launch_bounds__(kConvThreads) k_conv3(const __grid_constant__ ConvArgs a)
+{
+    using S = ConvSmem<COUT>;
+    constexpr int kTmemCols = COUT <= 32 ? 32 : (COUT <= 64 ? 64 : (COUT <= 128 ? 128 : 256));
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    __shared__ __align__(8) uint64_t full[kStages], empty[kStages], acc_full;
+    __shared__ uint32_t tmem_slot;
+    __shared__ int bad;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    // tile coordinates
+    int tile = blockIdx.x;
+    const int tw = tile % a.tiles_w;
+    tile /= a.tiles_w;
+    const int th = tile % a.tiles_h;
+    const int tz = tile / a.tiles_h;
+    const int per_sample = a.D / a.BZ;
+    const int w0 = tw * a.BW, h0 = th * a.BH;
+    const int z0 = (tz / per_sample) * (a.D + 2) + 1 + (tz % per_sample) * a.BZ;
+    const int chunks = a.Cin / 16;
+    const int ksteps = 27 * chunks;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kStages; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(&acc_full, 1);
+        bad = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        tmem_alloc(&tmem_slot, kTmemCols);
+        tmem_relinquish();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = tmem_slot;
+
+    if (warp == 0 && lane == 0) {
+        // ---------------- producer
+        for (int k = 0; k < ksteps; ++k) {
+            const int s = k % kStages;
+            if (k >= kStages && !mbar_wait(&empty[s], (uint32_t)(((k / kStages) - 1) & 1))) {
+                bad = 1;
+                break;
+            }
+            const int tap = k / chunks, c = k % chunks;
+            const int kw = tap % 3, kh = (tap / 3) % 3, kd = tap / 9;
+            uint8_t* st = smem + s * S::kStage;
+            mbar_expect_tx(&full[s], kATile + S::kB);
+            tma_load_4d(st, &a.xmap, c * 16, w0 + kw - 1, h0 + kh - 1, z0 + kd - 1, &full[s]);
+            tma_load_2d(st + kATile, &a.wmap, c * 16, tap * COUT, &full[s]);
+        }
+    } else if (warp == 1 && lane == 0) {
+        // ---------------- MMA issuer
+        constexpr uint32_t idesc = idesc_bf16(COUT, 0, 0);
+        bool ok = true;
+        for (int k = 0; k < ksteps; ++k) {
+            const int s = k % kStages;
+            if (!mbar_wait(&full[s], (uint32_t)((k / kStages) & 1))) {
+                bad = 1;
+                ok = false;
+                break;
+            }
+            tc_fence_after();
+            const uint8_t* st = smem + s * S::kStage;
+            const uint64_t ad = smem_desc(st, 16, 256, LAYOUT_SW32);
+            const uint64_t bd = smem_desc(st + kATile, 16, 256, LAYOUT_SW32);
+            umma_f16(tmem, ad, bd, idesc, k > 0 ? 1u : 0u);
+            umma_commit(&empty[s]);
+        }
+        if (ok) umma_commit(&acc_full);
+    } else if (warp >= 2) {
+        // ---------------- epilogue: TMEM lane quarter (warp % 4) -> 32 output positions
+        const int q = warp & 3;
+        const int m = 32 * q + lane;
+        // one decision per warp: the TMEM loads below are warp-collective
+        const bool ready = __all_sync(0xffffffffu, mbar_wait(&acc_full, 0));
+        tc_fence_after();
+        if (!ready) {
+            bad = 1;
+        } else {
+            const int w = w0 + m % a.BW;
+            const int h = h0 + (m / a.BW) % a.BH;
+            const int z = z0 + m / (a.BW * a.BH);
+            const size_t row = ((size_t)z * a.H + h) * a.W + w;
+            __nv_bfloat16* o = a.out + row * COUT;
+            const __nv_bfloat16* mk = a.mask ? a.mask + row * COUT : nullptr;
+#pragma unroll
+            for (int c0 = 0; c0 < COUT; c0 += 16) {
+                float v[16];
+                tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)c0, v);
+                __align__(16) __nv_bfloat16 ob[16];
+                __align__(16) __nv_bfloat16 mb[16];
+                if (mk) {
+                    *reinterpret_cast<uint4*>(mb) = *reinterpret_cast<const uint4*>(mk + c0);
+                    *reinterpret_cast<uint4*>(mb + 8) = *reinterpret_cast<const uint4*>(mk + c0 + 8);
+                }
+#pragma unroll
+                for (int i = 0; i < 16; ++i) {
+                    float x = v[i] + (a.bias ? a.bias[c0 + i] : 0.f);
+                    if (a.relu) x = fmaxf(x, 0.f);
+                    if (mk && !(__bfloat162float(mb[i]) > 0.f)) x = 0.f;
+                    ob[i] = __float2bfloat16_rn(x);
+                }
+                *reinterpret_cast<uint4*>(o + c0) = *reinterpret_cast<const uint4*>(ob);
+                *reinterpret_cast<uint4*>(o + c0 + 8) = *reinterpret_cast<const uint4*>(ob + 8);
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        tc_fence_after();
+        tmem_dealloc(tmem, kTmemCols);
+    }
+    if (bad && threadIdx.x == 0) atomicOr(a.err, 1);
+}
+
+// ------------------------------------------------------------------ host side
+using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                 const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+int encode_fn(EncodeTiled* out)
+{
+    static EncodeTiled fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q);
+        if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !p) {
+            set_error("cuTensorMapEncodeTiled is not available from the driver");
+            return RG_CUDA_ERROR;
+        }
+        fn = reinterpret_cast<EncodeTiled>(p);
+    }
+    *out = fn;
+    return RG_OK;
+}
+
+// activation map: dims (C, W, H, Z) with box (16, bw, bh, bz), 32-byte swizzle
+int make_act_map(CUtensorMap* map, const void* base, int C, int W, int H, int Z, int bw, int bh, int bz)
+{
+    EncodeTiled enc;
+    int rc = encode_fn(&enc);
+    if (rc) return rc;
+    RG_REQUIRE(C % 16 == 0 && bw * bh * bz == 128, "activation map: C must be a multiple of 16 and the box 128 positions");
+    RG_REQUIRE((reinterpret_cast<uintptr_t>(base) & 15) == 0, "activation map: base must be 16-byte aligned");
+    cuuint64_t dims[4] = {(cuuint64_t)C, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)Z};
+    cuuint64_t strides[3] = {(cuuint64_t)C * 2, (cuuint64_t)W * C * 2, (cuuint64_t)H * W * C * 2};
+    cuuint32_t box[4] = {16, (cuuint32_t)bw, (cuuint32_t)bh, (cuuint32_t)bz};
+    cuuint32_t es[4] = {1, 1, 1, 1};
+    CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void*>(base), dims, strides, box, es,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_32B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        set_error("cuTensorMapEncodeTiled (activations) failed with code " + std::to_string((int)r));
+        return RG_CUDA_ERROR;
+    }
+    return RG_OK;
+}
+
+// weight map: [rows][K] bf16 (K contiguous), box (16, box_rows), 32-byte swizzle
+int make_weight_map(CUtensorMap* map, const void* base, int K, int rows, int box_rows)
+{
+    EncodeTiled enc;
+    int rc = encode_fn(&enc);
+    if (rc) return rc;
+    RG_REQUIRE(K % 16 == 0 && box_rows <= 256, "weight map: K must be a multiple of 16");
+    RG_REQUIRE((reinterpret_cast<uintptr_t>(base) & 15) == 0, "weight map: base must be 16-byte aligned");
+    cuuint64_t dims[2] = {(cuuint64_t)K, (cuuint64_t)rows};
+    cuuint64_t strides[1] = {(cuuint64_t)K * 2};
+    cuuint32_t box[2] = {16, (cuuint32_t)box_rows};
+    cuuint32_t es[2] = {1, 1};
+    CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box, es,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_32B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        set_error("cuTensorMapEncodeTiled (weights) failed with code " + std::to_string((int)r));
+        return RG_CUDA_ERROR;
+    }
+    return RG_OK;
+}
+
+// 128-position box for a W x H slice grid
+void tile_box(int W, int H, int D, int* bw, int* bh, int* bz)
+{
+    *bw = W >= 128 ? 128 : W;
+    *bh = 128 / *bw;
+    if (*bh > H) *bh = H;
+    *bz = 128 / (*bw * *bh);
+    (void)D;
+}
+
+template <int COUT>
+int launch_conv3(ConvArgs& a, int ntiles)
+{
+    static bool attr = false;
+    if (!attr) {
+        RG_CHECK_CUDA(cudaFuncSetAttribute(k_conv3<COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           ConvSmem<COUT>::kBytes));
+        attr = true;
+    }
+    k_conv3<COUT><<<ntiles, kConvThreads, ConvSmem<COUT>::kBytes, stream()>>>(a);
+    RG_CHECK_LAUNCH();
+    return RG_OK;
+}
+
+}  // namespace ws
+}  // namespace rg
+
+using namespace rg;
+
+extern "C" int rg_ws_conv3(const rg_act* x, const void* weights, const float* bias, rg_act* y, int relu,
+                           const rg_act* mask, int* err_dev)
+{
+    RG_REQUIRE(x && weights && y && err_dev, "rg_ws_conv3: NULL argument");
+    RG_REQUIRE(x->n == y->n && x->d == y->d && x->h == y->h && x->w == y->w, "rg_ws_conv3: x and y shapes differ");
+    RG_REQUIRE(x->c % 16 == 0 && x->c <= 256, "rg_ws_conv3: input channels must be a multiple of 16");
+    const int cout = y->c;
+    RG_REQUIRE(cout == 16 || cout == 32 || cout == 48 || cout == 64 || cout == 80 || cout == 112 || cout == 128,
+               "rg_ws_conv3: output channels must be 16, 32, 48, 64, 80, 112 or 128");
+    RG_REQUIRE(!mask || (mask->c == cout && mask->n == y->n && mask->d == y->d && mask->h == y->h && mask->w == y->w),
+               "rg_ws_conv3: mask shape must equal the output shape");
+    int bw, bh, bz;
+    ws::tile_box(x->w, x->h, x->d, &bw, &bh, &bz);
+    RG_REQUIRE(x->w % bw == 0 && x->h % bh == 0 && x->d % bz == 0 && bw * bh * bz == 128,
+               "rg_ws_conv3: spatial sizes must tile into 128-position boxes");
+    ws::ConvArgs a;
+    const int Z = x->n * (x->d + 2);
+    int rc = ws::make_act_map(&a.xmap, x->ptr, x->c, x->w, x->h, Z, bw, bh, bz);
+    if (rc) return rc;
+    rc = ws::make_weight_map(&a.wmap, weights, x->c, 27 * cout, cout);
+    if (rc) return rc;
+    a.bias = bias;
+    a.out = static_cast<__nv_bfloat16*>(y->ptr);
+    a.mask = mask ? static_cast<const __nv_bfloat16*>(mask->ptr) : nullptr;
+    a.W = x->w;
+    a.H = x->h;
+    a.D = x->d;
+    a.Cin = x->c;
+    a.BW = bw;
+    a.BH = bh;
+    a.BZ = bz;
+    a.tiles_w = x->w / bw;
+    a.tiles_h = x->h / bh;
+    a.tiles_z = x->n * x->d / bz;
+    a.relu = relu;
+    a.err = err_dev;
+    const int ntiles = a.tiles_w * a.tiles_h * a.tiles_z;
+    switch (cout) {
+    case 16: return ws::launch_conv3<16>(a, ntiles);
+    case 32: return ws::launch_conv3<32>(a, ntiles);
+    case 48: return ws::launch_conv3<48>(a, ntiles);
+    case 64: return ws::launch_conv3<64>(a, ntiles);
+    case 80: return ws::launch_conv3<80>(a, ntiles);
+    case 112: return ws::launch_conv3<112>(a, ntiles);
+    default: return ws::launch_conv3<128>(a, ntiles);
+    }
+}

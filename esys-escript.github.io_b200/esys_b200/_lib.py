@@ -48,6 +48,11 @@ class rg_solver_opts(C.Structure):
                 ("initial_guess", C.c_void_p)]
 
 
+class rg_act(C.Structure):
+    _fields_ = [("ptr", C.c_void_p), ("n", C.c_int), ("d", C.c_int), ("h", C.c_int), ("w", C.c_int),
+                ("c", C.c_int)]
+
+
 class rg_diag(C.Structure):
     _fields_ = [("num_iter", C.c_int64), ("num_outer", C.c_int64),
                 ("residual_norm", C.c_double), ("residual_max", C.c_double),
@@ -92,6 +97,8 @@ _SIGNATURES = {
     "rg_solver_opts_default": (None, [C.POINTER(rg_solver_opts)]),
     "rg_solve": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(rg_solver_opts),
                            C.POINTER(rg_diag)]),
+    "rg_ws_conv3": (C.c_int, [C.POINTER(rg_act), C.c_void_p, C.c_void_p, C.POINTER(rg_act), C.c_int,
+                              C.POINTER(rg_act), C.c_void_p]),
     "rg_timers_enable": (C.c_int, [C.c_int]),
     "rg_timers_reset": (C.c_int, []),
     "rg_timers_count": (C.c_int, []),

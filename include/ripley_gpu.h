@@ -196,6 +196,21 @@ int rg_timers_count(void);
 const char* rg_timer_name(int kind);
 int rg_timers_read(int kind, int64_t* launches, int64_t* timed, double* total_ms);
 
+/* ---- warm-start network: tensor-core 3x3x3 convolutions (bf16, fp32 accumulation) ------ */
+/* bf16 channels-last activations with one zero slice before and after every sample along
+   depth: element (n, d, h, w, c) at ptr[(((n*(d_+2) + 1 + d)*h_ + h)*w_ + w)*c_ + c]. */
+typedef struct {
+    void* ptr;
+    int n, d, h, w, c;
+} rg_act;
+/* y = act(conv3x3x3(x, weights) + bias) with zero padding.  weights: bf16 [27][c_out][c_in],
+   tap = kw + 3 kh + 9 kd.  relu != 0 applies max(0, .); mask (shape of y) zeroes the
+   outputs where mask <= 0 (ReLU derivative of the layer below, for data gradients).
+   x->c a multiple of 16; y->c one of 16, 32, 48, 64, 80, 112, 128; spatial sizes must tile
+   into 128-position boxes.  *err_dev is set non-zero when a bounded device wait gave up. */
+int rg_ws_conv3(const rg_act* x, const void* weights, const float* bias, rg_act* y, int relu,
+                const rg_act* mask, int* err_dev);
+
 #ifdef __cplusplus
 }
 #endif
