@@ -218,6 +218,9 @@ int launch_balance(Matrix* m, int scale, int* d_bad, bool want_band);
 int solve(Matrix* m, const double* rhs, double* x, const rg_solver_opts* o, rg_diag* diag);
 void free_workspace(Matrix* m);
 void free_residual_scratch(Matrix* m);
+// l2 norm of b - A x with the matrix's values as they are (unbalance: undo an in-place
+// balancing on the fly); synchronises the stream
+int residual_l2(Matrix* m, const double* b, const double* x, bool unbalance, double* l2);
 
 }  // namespace rg
 

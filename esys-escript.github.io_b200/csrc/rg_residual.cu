@@ -23,6 +23,34 @@ void free_residual_scratch(Matrix* m)
     m->rs = nullptr;
 }
 
+int ensure_residual_scratch(Matrix* m)
+{
+    if (m->rs) return RG_OK;
+    ResidualScratch* s = new ResidualScratch();
+    m->rs = s;
+    RG_CHECK_CUDA(cudaMalloc((void**)&s->partials, sizeof(double) * residual::kMaxBlocks * 2));
+    RG_CHECK_CUDA(cudaMalloc((void**)&s->counter, sizeof(unsigned)));
+    RG_CHECK_CUDA(cudaMalloc((void**)&s->out, sizeof(double) * 2));
+    RG_CHECK_CUDA(cudaMemsetAsync(s->counter, 0, sizeof(unsigned), stream()));
+    return RG_OK;
+}
+
+int residual_l2(Matrix* m, const double* b, const double* x, bool unbalance, double* l2)
+{
+    int rc = ensure_residual_scratch(m);
+    if (rc) return rc;
+    const Domain* d = m->dom;
+    RG_TIMED(T_NORMS, (residual::k_residual_norms<<<residual::grid(d->n), residual::kThreads, 0, stream()>>>(
+                          d->n, d->ptr, d->idx, m->val, unbalance && m->balanced ? m->bv : nullptr, b, x,
+                          ReduceBuf{m->rs->partials, m->rs->counter}, m->rs->out)));
+    RG_CHECK_LAUNCH();
+    double h[2];
+    RG_CHECK_CUDA(cudaMemcpyAsync(h, m->rs->out, sizeof(h), cudaMemcpyDeviceToHost, stream()));
+    RG_CHECK_CUDA(cudaStreamSynchronize(stream()));
+    *l2 = std::sqrt(h[0]);
+    return RG_OK;
+}
+
 }  // namespace rg
 
 using namespace rg;
@@ -33,14 +61,8 @@ extern "C" int rg_residual_norms(rg_matrix* mat, const double* rhs, const double
     RG_REQUIRE(mat && rhs && x, "rg_residual_norms: NULL argument");
     Matrix* m = &mat->m;
     const Domain* d = m->dom;
-    if (!m->rs) {
-        ResidualScratch* s = new ResidualScratch();
-        m->rs = s;
-        RG_CHECK_CUDA(cudaMalloc((void**)&s->partials, sizeof(double) * residual::kMaxBlocks * 2));
-        RG_CHECK_CUDA(cudaMalloc((void**)&s->counter, sizeof(unsigned)));
-        RG_CHECK_CUDA(cudaMalloc((void**)&s->out, sizeof(double) * 2));
-        RG_CHECK_CUDA(cudaMemsetAsync(s->counter, 0, sizeof(unsigned), stream()));
-    }
+    int rc = ensure_residual_scratch(m);
+    if (rc) return rc;
     const int grid = residual::grid(d->n);
     RG_TIMED(T_NORMS, (residual::k_residual_norms<<<grid, residual::kThreads, 0, stream()>>>(
                           d->n, d->ptr, d->idx, m->val, m->balanced ? m->bv : nullptr, rhs, x,

@@ -1402,6 +1402,16 @@ int solve_impl(Matrix* m, const double* rhs, double* x, const rg_solver_opts* o,
             RG_TIMED(T_VECTOR, (k_mul<<<eg, kThreads, 0, stream()>>>(n, m->dinv, w->bb, w->x)));
         } else if (o->initial_guess) {
             RG_TIMED(T_VECTOR, (k_div<<<eg, kThreads, 0, stream()>>>(n, o->initial_guess, m->bv, w->x)));
+            RG_CHECK_LAUNCH();
+            // a guess whose residual exceeds the right hand side's is worse than zero: drop it
+            double r0;
+            if ((rc = residual_l2(m, w->bb, w->x, false, &r0))) return rc;
+            dg.guess_residual = r0;
+            if (!(r0 <= st.n2b)) {
+                RG_CHECK_CUDA(cudaMemsetAsync(w->x, 0, sizeof(double) * n, stream()));
+                dg.guess_rejected = 1;
+                if (o->verbose) printf("Solver: initial guess rejected (residual %g > %g).\n", r0, st.n2b);
+            }
         } else {
             RG_CHECK_CUDA(cudaMemsetAsync(w->x, 0, sizeof(double) * n, stream()));
         }

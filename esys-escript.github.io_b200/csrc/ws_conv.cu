@@ -172,6 +172,166 @@ __global__ void __launch_bounds__(kConvThreads) k_conv3(const __grid_constant__ 
     if (bad && threadIdx.x == 0) atomicOr(a.err, 1);
 }
 
+// ------------------------------------------------------------------ weight gradient
+// dW[tap][co][ci] = sum_pos X[pos + off(tap)][ci] * G[pos][co] as a GEMM with
+//   M = 128 rows = 8 (tap, 16-channel chunk) pairs x 16 channels,  N = Cout,  K = positions.
+// Both operands are M/N-major with 32-byte swizzle: for each pair the producer loads the
+// input box shifted by the pair's tap (kWgKP positions x 16 channels) and for each
+// 16-channel group of Cout the gradient box (kWgKP positions x 16 channels).  A CTA
+// accumulates the positions of its K split in TMEM and writes its 128 x Cout partial sums;
+// k_wgrad_reduce adds the splits in a fixed order into dW (fp32, [27][Cout][Cin]).
+constexpr int kWgKP = 64;                  // positions per stage (4 UMMAs of K = 16)
+constexpr int kWgStages = 3;
+constexpr int kWgA = 8 * kWgKP * 32;       // 16 KB
+
+struct WgradArgs {
+    CUtensorMap xmap;  // input activations, box (16, BW, BH, BZ) with BW*BH*BZ = kWgKP
+    CUtensorMap gmap;  // output gradient (Cout channels), same box
+    float* partials;   // [ksplit][mtiles*128][Cout]
+    int W, H, D, Cin, npairs;
+    int BW, BH, BZ, tiles_w, tiles_h, tiles_z;
+    int ptiles, ksplit, mtiles;
+    int* err;
+};
+
+template <int COUT>
+struct WgSmem {
+    static constexpr int kB = (COUT / 16) * kWgKP * 32;
+    static constexpr int kStage = kWgA + (kB + 1023) / 1024 * 1024;
+    static constexpr int kBytes = kWgStages * kStage + 1024;
+};
+
+template <int COUT>
+__global__ void __launch_bounds__(kConvThreads) k_wgrad(const __grid_constant__ WgradArgs a)
+{
+    using S = WgSmem<COUT>;
+    constexpr int kTmemCols = COUT <= 32 ? 32 : (COUT <= 64 ? 64 : (COUT <= 128 ? 128 : 256));
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    __shared__ __align__(8) uint64_t full[kWgStages], empty[kWgStages], acc_full;
+    __shared__ uint32_t tmem_slot;
+    __shared__ int bad;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int mt = blockIdx.x % a.mtiles;
+    const int ks = blockIdx.x / a.mtiles;
+    // this split's position tiles
+    const int per = (a.ptiles + a.ksplit - 1) / a.ksplit;
+    const int pt0 = ks * per;
+    const int pt1 = min(a.ptiles, pt0 + per);
+    const int nk = pt1 > pt0 ? pt1 - pt0 : 0;
+    const int per_sample = a.D / a.BZ;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kWgStages; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(&acc_full, 1);
+        bad = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        tmem_alloc(&tmem_slot, kTmemCols);
+        tmem_relinquish();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = tmem_slot;
+
+    if (warp == 0 && lane == 0) {
+        for (int k = 0; k < nk; ++k) {
+            const int s = k % kWgStages;
+            if (k >= kWgStages && !mbar_wait(&empty[s], (uint32_t)(((k / kWgStages) - 1) & 1))) {
+                bad = 1;
+                break;
+            }
+            int t = pt0 + k;
+            const int tw = t % a.tiles_w;
+            t /= a.tiles_w;
+            const int th = t % a.tiles_h;
+            const int tz = t / a.tiles_h;
+            const int w0 = tw * a.BW, h0 = th * a.BH;
+            const int z0 = (tz / per_sample) * (a.D + 2) + 1 + (tz % per_sample) * a.BZ;
+            uint8_t* st = smem + s * S::kStage;
+            mbar_expect_tx(&full[s], kWgA + S::kB);
+            for (int p = 0; p < 8; ++p) {
+                // pairs past the end re-load the last pair; their rows are discarded
+                const int pair = min(mt * 8 + p, a.npairs - 1);
+                const int chunks = a.Cin / 16;
+                const int tap = pair / chunks, c = pair % chunks;
+                const int kw = tap % 3, kh = (tap / 3) % 3, kd = tap / 9;
+                tma_load_4d(st + p * kWgKP * 32, &a.xmap, c * 16, w0 + kw - 1, h0 + kh - 1, z0 + kd - 1, &full[s]);
+            }
+            for (int g = 0; g < COUT / 16; ++g)
+                tma_load_4d(st + kWgA + g * kWgKP * 32, &a.gmap, g * 16, w0, h0, z0, &full[s]);
+        }
+    } else if (warp == 1 && lane == 0) {
+        constexpr uint32_t idesc = idesc_bf16(COUT, 1, 1);
+        bool ok = true;
+        for (int k = 0; k < nk; ++k) {
+            const int s = k % kWgStages;
+            if (!mbar_wait(&full[s], (uint32_t)((k / kWgStages) & 1))) {
+                bad = 1;
+                ok = false;
+                break;
+            }
+            tc_fence_after();
+            const uint8_t* st = smem + s * S::kStage;
+#pragma unroll
+            for (int j = 0; j < kWgKP / 16; ++j) {
+                // K slice j: 16 positions = 2 groups of 8 rows of 32 B
+                const uint64_t ad = smem_desc(st + j * 512, kWgKP * 32, 256, LAYOUT_SW32);
+                const uint64_t bd = smem_desc(st + kWgA + j * 512, kWgKP * 32, 256, LAYOUT_SW32);
+                umma_f16(tmem, ad, bd, idesc, (k > 0 || j > 0) ? 1u : 0u);
+            }
+            umma_commit(&empty[s]);
+        }
+        if (ok) umma_commit(&acc_full);
+    } else if (warp >= 2) {
+        const int q = warp & 3;
+        const int m = 32 * q + lane;
+        const bool ready = nk == 0 || __all_sync(0xffffffffu, mbar_wait(&acc_full, 0));
+        tc_fence_after();
+        float* dst = a.partials + ((size_t)ks * a.mtiles * 128 + (size_t)mt * 128 + m) * COUT;
+        if (!ready) {
+            bad = 1;
+        } else if (nk == 0) {
+            for (int c = 0; c < COUT; ++c) dst[c] = 0.f;
+        } else {
+#pragma unroll
+            for (int c0 = 0; c0 < COUT; c0 += 16) {
+                float v[16];
+                tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)c0, v);
+#pragma unroll
+                for (int i = 0; i < 16; i += 4)
+                    *reinterpret_cast<float4*>(dst + c0 + i) = make_float4(v[i], v[i + 1], v[i + 2], v[i + 3]);
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        tc_fence_after();
+        tmem_dealloc(tmem, kTmemCols);
+    }
+    if (bad && threadIdx.x == 0) atomicOr(a.err, 1);
+}
+
+// dW[tap][co][ci] = sum over splits (fixed order) of partials[split][pair*16 + ci%16][co]
+__global__ void k_wgrad_reduce(const float* __restrict__ partials, float* __restrict__ dw, int ksplit, int mtiles,
+                               int cout, int cin, int accumulate)
+{
+    const int total = 27 * cout * cin;
+    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += gridDim.x * blockDim.x) {
+        const int ci = idx % cin, co = (idx / cin) % cout, tap = idx / (cin * cout);
+        const int row = (tap * (cin / 16) + ci / 16) * 16 + ci % 16;
+        float s = 0.f;
+        for (int k = 0; k < ksplit; ++k) s += partials[((size_t)k * mtiles * 128 + row) * cout + co];
+        dw[idx] = accumulate ? dw[idx] + s : s;
+    }
+}
+
 // ------------------------------------------------------------------ host side
 using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
@@ -195,12 +355,15 @@ int encode_fn(EncodeTiled* out)
 }
 
 // activation map: dims (C, W, H, Z) with box (16, bw, bh, bz), 32-byte swizzle
-int make_act_map(CUtensorMap* map, const void* base, int C, int W, int H, int Z, int bw, int bh, int bz)
+// box of 16 channels x (bw, bh, bz) positions, bw * bh * bz == positions
+int make_act_map(CUtensorMap* map, const void* base, int C, int W, int H, int Z, int bw, int bh, int bz,
+                 int positions)
 {
     EncodeTiled enc;
     int rc = encode_fn(&enc);
     if (rc) return rc;
-    RG_REQUIRE(C % 16 == 0 && bw * bh * bz == 128, "activation map: C must be a multiple of 16 and the box 128 positions");
+    RG_REQUIRE(C % 16 == 0 && bw * bh * bz == positions,
+               "activation map: C must be a multiple of 16 and the box must hold the kernel's positions");
     RG_REQUIRE((reinterpret_cast<uintptr_t>(base) & 15) == 0, "activation map: base must be 16-byte aligned");
     cuuint64_t dims[4] = {(cuuint64_t)C, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)Z};
     cuuint64_t strides[3] = {(cuuint64_t)C * 2, (cuuint64_t)W * C * 2, (cuuint64_t)H * W * C * 2};
@@ -262,6 +425,29 @@ int launch_conv3(ConvArgs& a, int ntiles)
     return RG_OK;
 }
 
+template <int COUT>
+int launch_wgrad(WgradArgs& a, int grid)
+{
+    static bool attr = false;
+    if (!attr) {
+        RG_CHECK_CUDA(cudaFuncSetAttribute(k_wgrad<COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           WgSmem<COUT>::kBytes));
+        attr = true;
+    }
+    k_wgrad<COUT><<<grid, kConvThreads, WgSmem<COUT>::kBytes, stream()>>>(a);
+    RG_CHECK_LAUNCH();
+    return RG_OK;
+}
+
+// 64-position box for the weight gradient's K slices
+void wg_box(int W, int H, int* bw, int* bh, int* bz)
+{
+    *bw = W >= 64 ? 64 : W;
+    *bh = 64 / *bw;
+    if (*bh > H) *bh = H;
+    *bz = 64 / (*bw * *bh);
+}
+
 }  // namespace ws
 }  // namespace rg
 
@@ -284,7 +470,7 @@ extern "C" int rg_ws_conv3(const rg_act* x, const void* weights, const float* bi
                "rg_ws_conv3: spatial sizes must tile into 128-position boxes");
     ws::ConvArgs a;
     const int Z = x->n * (x->d + 2);
-    int rc = ws::make_act_map(&a.xmap, x->ptr, x->c, x->w, x->h, Z, bw, bh, bz);
+    int rc = ws::make_act_map(&a.xmap, x->ptr, x->c, x->w, x->h, Z, bw, bh, bz, 128);
     if (rc) return rc;
     rc = ws::make_weight_map(&a.wmap, weights, x->c, 27 * cout, cout);
     if (rc) return rc;
@@ -313,4 +499,65 @@ extern "C" int rg_ws_conv3(const rg_act* x, const void* weights, const float* bi
     case 112: return ws::launch_conv3<112>(a, ntiles);
     default: return ws::launch_conv3<128>(a, ntiles);
     }
+}
+
+extern "C" int rg_ws_conv3_wgrad(const rg_act* x, const rg_act* g, float* dw, float* partials,
+                                 int64_t partials_floats, int accumulate, int* err_dev)
+{
+    RG_REQUIRE(x && g && dw && partials && err_dev, "rg_ws_conv3_wgrad: NULL argument");
+    RG_REQUIRE(x->n == g->n && x->d == g->d && x->h == g->h && x->w == g->w, "rg_ws_conv3_wgrad: x and g shapes differ");
+    RG_REQUIRE(x->c % 16 == 0 && x->c <= 256, "rg_ws_conv3_wgrad: input channels must be a multiple of 16");
+    const int cout = g->c;
+    RG_REQUIRE(cout == 16 || cout == 32 || cout == 48 || cout == 64 || cout == 80 || cout == 112 || cout == 128,
+               "rg_ws_conv3_wgrad: gradient channels must be 16, 32, 48, 64, 80, 112 or 128");
+    int bw, bh, bz;
+    ws::wg_box(x->w, x->h, &bw, &bh, &bz);
+    RG_REQUIRE(x->w % bw == 0 && x->h % bh == 0 && x->d % bz == 0 && bw * bh * bz == ws::kWgKP,
+               "rg_ws_conv3_wgrad: spatial sizes must tile into 64-position boxes");
+    ws::WgradArgs a;
+    const int Z = x->n * (x->d + 2);
+    int rc = ws::make_act_map(&a.xmap, x->ptr, x->c, x->w, x->h, Z, bw, bh, bz, ws::kWgKP);
+    if (rc) return rc;
+    rc = ws::make_act_map(&a.gmap, g->ptr, cout, g->w, g->h, Z, bw, bh, bz, ws::kWgKP);
+    if (rc) return rc;
+    a.W = x->w;
+    a.H = x->h;
+    a.D = x->d;
+    a.Cin = x->c;
+    a.npairs = 27 * (x->c / 16);
+    a.BW = bw;
+    a.BH = bh;
+    a.BZ = bz;
+    a.tiles_w = x->w / bw;
+    a.tiles_h = x->h / bh;
+    a.tiles_z = x->n * x->d / bz;
+    a.ptiles = a.tiles_w * a.tiles_h * a.tiles_z;
+    a.mtiles = (a.npairs + 7) / 8;
+    // about four CTAs per SM in total
+    int ksplit = (4 * kNumSMs + a.mtiles - 1) / a.mtiles;
+    if (ksplit > a.ptiles) ksplit = a.ptiles;
+    const int64_t need = (int64_t)ksplit * a.mtiles * 128 * cout;
+    if (need > partials_floats) {
+        ksplit = (int)(partials_floats / ((int64_t)a.mtiles * 128 * cout));
+        RG_REQUIRE(ksplit >= 1, "rg_ws_conv3_wgrad: partials buffer too small");
+    }
+    a.ksplit = ksplit;
+    a.partials = partials;
+    a.err = err_dev;
+    const int grid = a.mtiles * ksplit;
+    switch (cout) {
+    case 16: rc = ws::launch_wgrad<16>(a, grid); break;
+    case 32: rc = ws::launch_wgrad<32>(a, grid); break;
+    case 48: rc = ws::launch_wgrad<48>(a, grid); break;
+    case 64: rc = ws::launch_wgrad<64>(a, grid); break;
+    case 80: rc = ws::launch_wgrad<80>(a, grid); break;
+    case 112: rc = ws::launch_wgrad<112>(a, grid); break;
+    default: rc = ws::launch_wgrad<128>(a, grid); break;
+    }
+    if (rc) return rc;
+    const int total = 27 * cout * x->c;
+    ws::k_wgrad_reduce<<<(total + 255) / 256, 256, 0, stream()>>>(partials, dw, ksplit, a.mtiles, cout, x->c,
+                                                                 accumulate);
+    RG_CHECK_LAUNCH();
+    return RG_OK;
 }

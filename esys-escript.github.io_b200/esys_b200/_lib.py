@@ -57,7 +57,8 @@ class rg_diag(C.Structure):
     _fields_ = [("num_iter", C.c_int64), ("num_outer", C.c_int64),
                 ("residual_norm", C.c_double), ("residual_max", C.c_double),
                 ("rhs_norm", C.c_double), ("converged", C.c_int), ("time", C.c_double),
-                ("set_up_time", C.c_double), ("net_time", C.c_double)]
+                ("set_up_time", C.c_double), ("net_time", C.c_double),
+                ("guess_residual", C.c_double), ("guess_rejected", C.c_int)]
 
 
 _lib = None
@@ -99,6 +100,27 @@ _SIGNATURES = {
                            C.POINTER(rg_diag)]),
     "rg_ws_conv3": (C.c_int, [C.POINTER(rg_act), C.c_void_p, C.c_void_p, C.POINTER(rg_act), C.c_int,
                               C.POINTER(rg_act), C.c_void_p]),
+    "rg_ws_conv3_wgrad": (C.c_int, [C.POINTER(rg_act), C.POINTER(rg_act), C.c_void_p, C.c_void_p, C.c_int64, C.c_int,
+                                    C.c_void_p]),
+    "rg_ws_avgpool": (C.c_int, [C.POINTER(rg_act), C.POINTER(rg_act)]),
+    "rg_ws_avgpool_bwd": (C.c_int, [C.POINTER(rg_act), C.POINTER(rg_act), C.POINTER(rg_act), C.c_int, C.POINTER(rg_act)]),
+    "rg_ws_upcat": (C.c_int, [C.POINTER(rg_act), C.POINTER(rg_act), C.POINTER(rg_act)]),
+    "rg_ws_upcat_bwd": (C.c_int, [C.POINTER(rg_act), C.POINTER(rg_act), C.POINTER(rg_act)]),
+    "rg_ws_head": (C.c_int, [C.POINTER(rg_act), C.c_void_p, C.c_void_p, C.c_void_p]),
+    "rg_ws_head_bwd_x": (C.c_int, [C.POINTER(rg_act), C.c_void_p, C.c_void_p, C.POINTER(rg_act)]),
+    "rg_ws_colsum": (C.c_int, [C.POINTER(rg_act), C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
+    "rg_ws_mse": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p,
+                            C.c_void_p]),
+    "rg_ws_adam": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_float,
+                             C.c_float, C.c_float, C.c_float, C.c_int]),
+    "rg_ws_weights_bf16": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int]),
+    "rg_ws_field_stats": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int64, C.c_double, C.c_void_p,
+                                    C.c_void_p]),
+    "rg_ws_pack_input": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.POINTER(rg_act), C.c_void_p]),
+    "rg_ws_nodes_to_cells": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p,
+                                       C.c_void_p]),
+    "rg_ws_cells_to_nodes": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int,
+                                       C.c_int, C.c_int, C.c_void_p, C.c_void_p]),
     "rg_timers_enable": (C.c_int, [C.c_int]),
     "rg_timers_reset": (C.c_int, []),
     "rg_timers_count": (C.c_int, []),

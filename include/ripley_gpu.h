@@ -164,7 +164,8 @@ typedef struct {
     int layout;                 /* RG_LAYOUT_*                                              */
     double inner_tolerance;     /* FP32_REFINE: reduction of the FP32 recursive residual    
                                    between FP64 residual replacements (default 1e-2)      */
-    const double* initial_guess;/* STANDARD mode only: device x0 (unbalanced units) or NULL */
+    const double* initial_guess;/* STANDARD mode only: device x0 (unbalanced units) or NULL;
+                                   dropped for zero when ||B(b - A x0)|| > ||B b||          */
 } rg_solver_opts;
 
 typedef struct {
@@ -177,6 +178,9 @@ typedef struct {
     double time;                /* seconds, whole solve (SolverBuddy time)                  */
     double set_up_time;         /* balancing + preconditioner                               */
     double net_time;            /* iterations                                               */
+    double guess_residual;      /* l2 norm of the balanced residual of the initial guess    */
+    int guess_rejected;         /* 1: the guess's residual exceeded the right hand side's
+                                   and the solve started from zero instead                  */
 } rg_diag;
 
 void rg_solver_opts_default(rg_solver_opts* opts);
@@ -210,6 +214,62 @@ typedef struct {
    into 128-position boxes.  *err_dev is set non-zero when a bounded device wait gave up. */
 int rg_ws_conv3(const rg_act* x, const void* weights, const float* bias, rg_act* y, int relu,
                 const rg_act* mask, int* err_dev);
+/* Weight gradient of rg_ws_conv3: dw[tap][c_out][c_in] (fp32) = sum over positions p of
+   g(p, c_out) x(p + offset(tap), c_in), g the gradient at the conv output (after the ReLU
+   mask).  Split over position tiles; the splits' partial sums go to `partials`
+   (partials_floats floats; more lets more CTAs run) and are added in a fixed order, so the
+   result is deterministic.  accumulate != 0 adds into dw.  Spatial sizes must tile into
+   64-position boxes.  Data gradients are rg_ws_conv3 of g with rg_ws_weights_bf16's
+   flipped weights and the mask of the layer below. */
+int rg_ws_conv3_wgrad(const rg_act* x, const rg_act* g, float* dw, float* partials,
+                      int64_t partials_floats, int accumulate, int* err_dev);
+
+/* Memory-bound layers of the network (all on the library stream, bf16 activations). */
+/* out = 2x2x2 average of in (out spatial sizes are half of in's) */
+int rg_ws_avgpool(const rg_act* in, rg_act* out);
+/* din = (dout upsampled / 8 [+ dskip channels skip_off..]) where in > 0, else 0; dskip may be
+   NULL (the gradient reaching a pooled tensor's skip connection) */
+int rg_ws_avgpool_bwd(const rg_act* dout, const rg_act* in, const rg_act* dskip, int skip_off,
+                      rg_act* din);
+/* out = concat(nearest-upsample-2x(a), b) along channels */
+int rg_ws_upcat(const rg_act* a, const rg_act* b, rg_act* out);
+/* da = sum over each parent's 8 children of dcat's first da->c channels, zero where the
+   upsampled tensor a <= 0 (its ReLU derivative; a may be NULL) */
+int rg_ws_upcat_bwd(const rg_act* dcat, const rg_act* a, rg_act* da);
+/* 1x1x1 output head: out[pos] = b[0] + sum_c w[c] x(pos, c); out fp32 [n][d][h][w] */
+int rg_ws_head(const rg_act* x, const float* w, const float* b, float* out);
+/* dx(pos, c) = w[c] dout[pos] where x(pos, c) > 0, else 0 */
+int rg_ws_head_bwd_x(const rg_act* x, const float* w, const float* dout, rg_act* dx);
+/* out[c] (+)= sum over positions of v(pos, c) [* dout[pos] when dout != NULL]; bias gradients
+   (dout NULL) and the head's weight gradient.  work: 592 * v->c floats, v->c <= 128 */
+int rg_ws_colsum(const rg_act* v, const float* dout, float* out, float* work, int accumulate);
+/* *loss_dev = mean (out - target)^2 (fp64), dout = its gradient, *dsum_dev = sum of dout
+   (may be NULL); work: 1184 doubles */
+int rg_ws_mse(const float* out, const float* target, int64_t count, float* dout, double* loss_dev,
+              float* dsum_dev, double* work);
+/* Adam step `step` (>= 1, bias-corrected) on fp32 master weights */
+int rg_ws_adam(float* w, const float* g, float* m, float* v, int64_t count, float lr, float beta1,
+               float beta2, float eps, int step);
+/* fp32 weights [27][c_out][c_in] -> bf16 forward copy (same layout) and/or bf16 data-gradient
+   copy [27][c_in][c_out] with taps reversed (tap' = 26 - tap); either output may be NULL */
+int rg_ws_weights_bf16(const float* w, void* w_fwd, void* w_dgrad, int c_out, int c_in);
+/* Glue between the PDE's fields and the network.  Fields are fp32 per element of a fine
+   grid (x fastest, samples consecutive); the network grid is the fine grid coarsened by an
+   integer factor.  rg_ws_field_stats writes 4 floats per sample: mu = mean log kappa,
+   sY = max |Y|, kappa_g = exp(mu), u_unit = 10 sY h_net^2 / kappa_g (work: 128 * nsamples
+   doubles).  The network sees (log kappa - mu, Y / sY) averaged over each of its cells and
+   predicts u / u_unit per cell. */
+int rg_ws_field_stats(const float* kappa, const float* y, int nsamples, int64_t per_sample, double h_net,
+                      float* stats, double* work);
+int rg_ws_pack_input(const float* kappa, const float* y, int factor, rg_act* x, const float* stats);
+/* training target per network cell: mean of the nodal solution u (fp64, (f d+1)(f h+1)(f w+1)
+   nodes per sample) over the cell, in units of u_unit */
+int rg_ws_nodes_to_cells(const double* u, int factor, int nsamples, int d, int h, int w, const float* stats,
+                         float* target);
+/* initial guess on nd x nh x nw nodes per sample: trilinear interpolation of the cell values
+   (cell centres, clamped at the faces) times u_unit; 0 where q > 0 (q may be NULL) */
+int rg_ws_cells_to_nodes(const float* cells, int nsamples, int d, int h, int w, const float* stats, int nd, int nh,
+                         int nw, const double* q, double* u);
 
 #ifdef __cplusplus
 }
