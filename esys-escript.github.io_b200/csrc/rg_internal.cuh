@@ -186,7 +186,7 @@ inline int grid_for(int64_t work_items, int items_per_block, int blocks_per_sm =
 enum TimerKind {
     T_PATTERN = 0, T_ASSEMBLE, T_BOUNDARY, T_CONSTRAINT, T_SPMV, T_BALANCE, T_NORMS, T_RESIDUAL,
     T_PASO_SPMV, T_PASO_UPDATE1, T_PASO_UPDATE2, T_STD_SPMV, T_STD_UPDATE, T_F32_SPMV,
-    T_F32_UPDATE, T_VECTOR, T_COUNT
+    T_F32_UPDATE, T_VECTOR, T_BATCH_SPMV, T_BATCH_UPDATE, T_BATCH_OUTER, T_COUNT
 };
 void timer_begin(int kind);
 void timer_end(int kind);
@@ -216,6 +216,9 @@ int launch_spmv64(const Domain* d, const double* val, double alpha, const double
 // want_band) from the current values; *d_bad is set when a diagonal is zero or missing
 int launch_balance(Matrix* m, int scale, int* d_bad, bool want_band);
 int solve(Matrix* m, const double* rhs, double* x, const rg_solver_opts* o, rg_diag* diag);
+// balance the matrix in place (first time) and build its solver data, the FP32 band copy
+// included when `band` (what rg_solve does before iterating)
+int solver_prepare(Matrix* m, bool band);
 void free_workspace(Matrix* m);
 void free_residual_scratch(Matrix* m);
 // l2 norm of b - A x with the matrix's values as they are (unbalance: undo an in-place

@@ -222,6 +222,23 @@ __global__ void __launch_bounds__(kThreads) k_residual(int64_t n, const int32_t*
     }
 }
 
+// one damped Jacobi sweep on the balanced system: y = x + omega D^-1 (bb - A x)
+__global__ void __launch_bounds__(kThreads) k_jacobi_sweep(int64_t n, const int32_t* __restrict__ ptr,
+                                                           const int32_t* __restrict__ idx,
+                                                           const double* __restrict__ val,
+                                                           const double* __restrict__ dinv,
+                                                           const double* __restrict__ x,
+                                                           const double* __restrict__ bb, double omega,
+                                                           double* __restrict__ y)
+{
+    RG_ROW_LOOP(n)
+    {
+        double acc = row < n ? csr_row_dot(ptr, idx, val, x, row, lane) : 0.0;
+        acc = group_sum(acc);
+        if (row < n && lane == 0) y[row] = x[row] + omega * dinv[row] * (bb[row] - acc);
+    }
+}
+
 __global__ void k_mul(int64_t n, const double* __restrict__ a, const double* __restrict__ b,
                       double* __restrict__ out)
 {
@@ -829,7 +846,7 @@ __global__ void __launch_bounds__(kThreads) k_f32_update(int64_t n, float* __res
         const bool brk = !(fabs(t[0]) > 0.0);
         s->rho = t[0];
         // the FP32 recurrence has stagnated when no new minimum (5% below the best)
-        // appeared for 50 iterations: end the segment so that the FP64 residual is
+        // appeared for 200 iterations: end the segment so that the FP64 residual is
         // recomputed and fed back
         if (norm < 0.95 * s->best) {
             s->best = norm;
@@ -837,7 +854,7 @@ __global__ void __launch_bounds__(kThreads) k_f32_update(int64_t n, float* __res
         } else {
             s->since += 1;
         }
-        if (norm <= s->tol || s->since > 50) {
+        if (norm <= s->tol || s->since > 200) {
             s->status = ST_CONV;
             s->done = 1;
         } else if (it >= s->maxit) {
@@ -1267,6 +1284,15 @@ int solve_f32(Matrix* m, const rg_solver_opts* o, OuterState& st, rg_diag& dg)
         st.last2 = n2r;
         st.lastm = nmr;
         rc = outer_residual(m, o, st, dg, &conv, &n2r, &nmr, false);
+        if (rc == RG_DIVERGENCE) {
+            // the FP32 corrections stopped reducing the FP64 residual (rounding the values of
+            // a badly conditioned matrix to FP32 bounds what refinement can reach): finish
+            // with FP64 PCG from the current x
+            if (o->verbose) printf("Solver: FP32 refinement stalled; continuing in FP64.\n");
+            set_error("");
+            dg.fp64_fallback = 1;
+            return solve_fp64(m, o, false, st, dg);
+        }
         if (rc || conv) return rc;
         if (o->verbose) printf(" (FP32 segment of %lld iterations).\n", it);
         bool restart = false;
@@ -1279,6 +1305,13 @@ int solve_f32(Matrix* m, const rg_solver_opts* o, OuterState& st, rg_diag& dg)
 }
 
 }  // namespace
+
+int solver_prepare(Matrix* m, bool band)
+{
+    int rc = ensure_workspace(m, band);
+    if (rc) return rc;
+    return prepare(m, band);
+}
 
 void free_workspace(Matrix* m)
 {
@@ -1357,6 +1390,7 @@ int solve_impl(Matrix* m, const double* rhs, double* x, const rg_solver_opts* o,
     RG_REQUIRE(o->preconditioner == RG_PRECOND_JACOBI, "solver: only the Jacobi preconditioner is implemented");
     RG_REQUIRE(o->tolerance >= 100. * EPS, "Solver: Tolerance is too small.");
     RG_REQUIRE(o->tolerance <= 1., "Solver: Tolerance must be less than one.");
+    RG_REQUIRE(o->guess_sweeps >= 0 && o->guess_sweeps <= 1000, "solver: guess_sweeps must be in [0, 1000]");
     if (o->sweeps > 1) {
         set_error("solver: Jacobi with more than one sweep is not implemented on the GPU");
         return RG_NOT_SUPPORTED;
@@ -1403,6 +1437,18 @@ int solve_impl(Matrix* m, const double* rhs, double* x, const rg_solver_opts* o,
         } else if (o->initial_guess) {
             RG_TIMED(T_VECTOR, (k_div<<<eg, kThreads, 0, stream()>>>(n, o->initial_guess, m->bv, w->x)));
             RG_CHECK_LAUNCH();
+            // damped Jacobi sweeps remove the guess's rough error (which dominates its residual)
+            // and keep its smooth part, which is what PCG is slow to find
+            const Domain* dm = m->dom;
+            for (int k = 0; k < o->guess_sweeps; ++k) {
+                const double* src = (k & 1) ? w->x2 : w->x;
+                double* dst = (k & 1) ? w->x : w->x2;
+                RG_TIMED(T_VECTOR, (k_jacobi_sweep<<<w->grid_rows, kThreads, 0, stream()>>>(
+                                       n, dm->ptr, dm->idx, m->val, m->dinv, src, w->bb, 0.6, dst)));
+                RG_CHECK_LAUNCH();
+            }
+            if (o->guess_sweeps > 0 && (o->guess_sweeps & 1))
+                RG_CHECK_CUDA(cudaMemcpyAsync(w->x, w->x2, sizeof(double) * n, cudaMemcpyDeviceToDevice, stream()));
             // a guess whose residual exceeds the right hand side's is worse than zero: drop it
             double r0;
             if ((rc = residual_l2(m, w->bb, w->x, false, &r0))) return rc;

@@ -27,7 +27,8 @@ cudaEvent_t g_open[T_COUNT] = {};
 const char* kNames[T_COUNT] = {"pattern", "assemble", "assemble_boundary", "insert_constraint",
                                "spmv", "balance", "norms", "residual", "paso_spmv",
                                "paso_update1", "paso_update2", "std_spmv", "std_update",
-                               "f32_spmv", "f32_update", "vector"};
+                               "f32_spmv", "f32_update", "vector", "batch_spmv", "batch_update",
+                               "batch_outer"};
 
 cudaEvent_t get_event()
 {

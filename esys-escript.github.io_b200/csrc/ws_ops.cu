@@ -205,6 +205,61 @@ __global__ void k_mse_finish(const double* __restrict__ part, int nblocks, size_
     }
 }
 
+// loss = (sum_i e_i^2 + lambda sum over neighbouring cell pairs (e_i - e_j)^2) / count with
+// e = out - t on a (n, d, h, w) grid: the squared error plus a discrete gradient (H1
+// seminorm) term, which weighs the rough error that dominates a guess's residual.
+// dout_i = (2 e_i + 2 lambda sum_{j adjacent to i} (e_i - e_j)) / count.
+__global__ void k_h1_loss(const float* __restrict__ out, const float* __restrict__ t, int n, int d_, int h_, int w_,
+                          float lambda, float* __restrict__ dout, double* __restrict__ part)
+{
+    __shared__ double sh[2][256];
+    const size_t count = (size_t)n * d_ * h_ * w_;
+    const float inv = 1.f / (float)count;
+    double s = 0.0, g = 0.0;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += (size_t)gridDim.x * blockDim.x) {
+        const int x = (int)(i % w_), y = (int)((i / w_) % h_), z = (int)((i / ((size_t)w_ * h_)) % d_);
+        const float e = out[i] - t[i];
+        float lap = 0.f, pairs = 0.f;
+        const size_t sy = (size_t)w_, sz = (size_t)w_ * h_;
+        if (x > 0) lap += e - (out[i - 1] - t[i - 1]);
+        if (x + 1 < w_) {
+            const float f = e - (out[i + 1] - t[i + 1]);
+            lap += f;
+            pairs += f * f;
+        }
+        if (y > 0) lap += e - (out[i - sy] - t[i - sy]);
+        if (y + 1 < h_) {
+            const float f = e - (out[i + sy] - t[i + sy]);
+            lap += f;
+            pairs += f * f;
+        }
+        if (z > 0) lap += e - (out[i - sz] - t[i - sz]);
+        if (z + 1 < d_) {
+            const float f = e - (out[i + sz] - t[i + sz]);
+            lap += f;
+            pairs += f * f;
+        }
+        const float de = (2.f * e + 2.f * lambda * lap) * inv;
+        dout[i] = de;
+        s += (double)e * e + (double)lambda * pairs;
+        g += 2.0 * e * inv;
+    }
+    sh[0][threadIdx.x] = s;
+    sh[1][threadIdx.x] = g;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) {
+            sh[0][threadIdx.x] += sh[0][threadIdx.x + o];
+            sh[1][threadIdx.x] += sh[1][threadIdx.x + o];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        part[2 * blockIdx.x] = sh[0][0];
+        part[2 * blockIdx.x + 1] = sh[1][0];
+    }
+}
+
 // Adam on fp32 master weights (bias-corrected), grads fp32
 __global__ void k_adam(float* __restrict__ w, const float* __restrict__ g, float* __restrict__ m, float* __restrict__ v,
                        size_t count, float lr, float b1, float b2, float eps, float c1, float c2)
@@ -286,8 +341,8 @@ __global__ void k_field_stats_finish(const double* __restrict__ part, int nblock
     stats[4 * n + 3] = (float)(10.0 * sy * h * h / kg);
 }
 
-// network input (channel 0 = log kappa - mu, 1 = Y / sY, others 0), each network cell the
-// mean over its f^3 fine elements
+// network input: channel 0 = log kappa - mu, 1 = Y / sY (each the mean over the network
+// cell's f^3 fine elements), 2..4 = the cell centre's (z, y, x) in the unit cube, others 0
 __global__ void k_pack_input(const float* __restrict__ kappa, const float* __restrict__ y, int f, Act x,
                              const float* __restrict__ stats)
 {
@@ -308,7 +363,14 @@ __global__ void k_pack_input(const float* __restrict__ kappa, const float* __res
         __nv_bfloat16* xp = x.p + x.at(n, d, h, w);
         xp[0] = tobf(lk * inv - stats[4 * n]);
         xp[1] = tobf(yy * inv / stats[4 * n + 1]);
-        for (int c = 2; c < x.c; ++c) xp[c] = tobf(0.f);
+        // the cell centre's position in the unit cube: convolutions with zero padding cannot
+        // tell the Dirichlet face (z = 1) from the others without it
+        if (x.c > 4) {
+            xp[2] = tobf(((float)d + 0.5f) / (float)x.d);
+            xp[3] = tobf(((float)h + 0.5f) / (float)x.h);
+            xp[4] = tobf(((float)w + 0.5f) / (float)x.w);
+        }
+        for (int c = 5; c < x.c; ++c) xp[c] = tobf(0.f);
     }
 }
 
@@ -495,6 +557,20 @@ int rg_ws_mse(const float* out, const float* target, int64_t count, float* dout,
     return RG_OK;
 }
 
+int rg_ws_h1_loss(const float* out, const float* target, int n, int d, int h, int w, float lambda, float* dout,
+                  double* loss_dev, float* dsum_dev, double* work)
+{
+    RG_REQUIRE(out && target && dout && loss_dev && work && n > 0 && d > 0 && h > 0 && w > 0 && lambda >= 0.f,
+               "rg_ws_h1_loss: invalid argument");
+    const int blocks = kNumSMs * 4;
+    const size_t count = (size_t)n * d * h * w;
+    k_h1_loss<<<blocks, 256, 0, stream()>>>(out, target, n, d, h, w, lambda, dout, work);
+    RG_CHECK_LAUNCH();
+    k_mse_finish<<<1, 32, 0, stream()>>>(work, blocks, count, loss_dev, dsum_dev);
+    RG_CHECK_LAUNCH();
+    return RG_OK;
+}
+
 int rg_ws_adam(float* w, const float* g, float* m, float* v, int64_t count, float lr, float beta1, float beta2,
                float eps, int step)
 {
@@ -532,7 +608,7 @@ int rg_ws_field_stats(const float* kappa, const float* y, int nsamples, int64_t 
 int rg_ws_pack_input(const float* kappa, const float* y, int factor, rg_act* x, const float* stats)
 {
     RG_ACT_OK(x, "rg_ws_pack_input");
-    RG_REQUIRE(kappa && y && stats && x->c >= 2 && factor >= 1, "rg_ws_pack_input: invalid argument");
+    RG_REQUIRE(kappa && y && stats && x->c >= 5 && factor >= 1, "rg_ws_pack_input: invalid argument");
     const Act xa = act(x);
     k_pack_input<<<grid_elems(xa.positions()), 256, 0, stream()>>>(kappa, y, factor, xa, stats);
     RG_CHECK_LAUNCH();

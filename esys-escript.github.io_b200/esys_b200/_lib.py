@@ -45,7 +45,7 @@ class rg_solver_opts(C.Structure):
                 ("iter_max", C.c_int64), ("sweeps", C.c_int), ("verbose", C.c_int),
                 ("accept_convergence_failure", C.c_int), ("mode", C.c_int),
                 ("precision", C.c_int), ("layout", C.c_int), ("inner_tolerance", C.c_double),
-                ("initial_guess", C.c_void_p)]
+                ("initial_guess", C.c_void_p), ("guess_sweeps", C.c_int)]
 
 
 class rg_act(C.Structure):
@@ -58,7 +58,7 @@ class rg_diag(C.Structure):
                 ("residual_norm", C.c_double), ("residual_max", C.c_double),
                 ("rhs_norm", C.c_double), ("converged", C.c_int), ("time", C.c_double),
                 ("set_up_time", C.c_double), ("net_time", C.c_double),
-                ("guess_residual", C.c_double), ("guess_rejected", C.c_int)]
+                ("guess_residual", C.c_double), ("guess_rejected", C.c_int), ("fp64_fallback", C.c_int)]
 
 
 _lib = None
@@ -111,6 +111,8 @@ _SIGNATURES = {
     "rg_ws_colsum": (C.c_int, [C.POINTER(rg_act), C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
     "rg_ws_mse": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p,
                             C.c_void_p]),
+    "rg_ws_h1_loss": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float,
+                                C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "rg_ws_adam": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_float,
                              C.c_float, C.c_float, C.c_float, C.c_int]),
     "rg_ws_weights_bf16": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int]),
@@ -121,6 +123,13 @@ _SIGNATURES = {
                                        C.c_void_p]),
     "rg_ws_cells_to_nodes": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int,
                                        C.c_int, C.c_int, C.c_void_p, C.c_void_p]),
+    "rg_batch_create": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
+    "rg_batch_destroy": (C.c_int, [C.c_void_p]),
+    "rg_batch_tune": (C.c_int, [C.c_void_p]),
+    "rg_batch_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int),
+                                C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_double)]),
+    "rg_batch_solve": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(rg_solver_opts),
+                                 C.c_void_p]),
     "rg_timers_enable": (C.c_int, [C.c_int]),
     "rg_timers_reset": (C.c_int, []),
     "rg_timers_count": (C.c_int, []),

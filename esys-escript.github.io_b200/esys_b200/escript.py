@@ -634,7 +634,7 @@ class SolverBuddy:
         self.__diag = {"num_iter": 0, "num_level": 0, "num_inner_iter": 0, "time": 0.0,
                        "set_up_time": 0.0, "net_time": 0.0, "residual_norm": 0.0,
                        "converged": False, "num_outer": 0, "guess_rejected": False,
-                       "guess_residual": 0.0}
+                       "guess_residual": 0.0, "fp64_fallback": False}
         if all or not cum:
             cum = {"cum_num_iter": 0, "cum_time": 0.0, "cum_set_up_time": 0.0,
                    "cum_net_time": 0.0, "cum_num_inner_iter": 0}
@@ -645,7 +645,8 @@ class SolverBuddy:
                            residual_norm=float(d.residual_norm), converged=bool(d.converged),
                            time=float(d.time), set_up_time=float(d.set_up_time),
                            net_time=float(d.net_time), guess_rejected=bool(d.guess_rejected),
-                           guess_residual=float(d.guess_residual))
+                           guess_residual=float(d.guess_residual),
+                           fp64_fallback=bool(d.fp64_fallback))
         self.__diag["cum_num_iter"] += int(d.num_iter)
         self.__diag["cum_time"] += float(d.time)
         self.__diag["cum_set_up_time"] += float(d.set_up_time)

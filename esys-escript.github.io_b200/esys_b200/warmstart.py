@@ -136,6 +136,12 @@ def mse(out, target, dout, loss, dsum, work):
     L.check(L.lib().rg_ws_mse(_p(out), _p(target), out.numel(), _p(dout), _p(loss), _p(dsum), _p(work)))
 
 
+def h1_loss(out, target, lam, dout, loss, dsum, work):
+    n, d, h, w = out.shape
+    L.check(L.lib().rg_ws_h1_loss(_p(out), _p(target), n, d, h, w, float(lam), _p(dout), _p(loss), _p(dsum),
+                                  _p(work)))
+
+
 def weights_bf16(w, w_fwd, w_dgrad):
     _, cout, cin = w.shape
     L.check(L.lib().rg_ws_weights_bf16(_p(w), _p(w_fwd), _p(w_dgrad), cout, cin))
@@ -217,11 +223,11 @@ class UNet:
 
     # -- parameters
     def init(self, seed=0):
-        """He-normal weights (fan-in 27 c_in; 27 x 2 for the two live input channels), zero
+        """He-normal weights (fan-in 27 c_in; 27 x 5 for the five live input channels), zero
         biases, small head."""
         gen = torch.Generator().manual_seed(seed)
         for name, cin, cout in self.layers:
-            fan = 27 * (2 if name == "enc0a" else cin)
+            fan = 27 * (5 if name == "enc0a" else cin)
             w = torch.randn((27, cout, cin), generator=gen) * math.sqrt(2.0 / fan)
             self.p[name + ".w"].copy_(w)
             self.p[name + ".b"].zero_()
@@ -283,10 +289,14 @@ class UNet:
         if dx is not None:
             conv3(g, self.wd[name], None, dx, relu=False, mask=mask, err=self.err)
 
-    def loss_and_backward(self, ws):
-        """self.loss = mse(ws.out, ws.target); self.grad = its gradient (forward must have run)."""
+    def loss_and_backward(self, ws, grad_weight=0.0):
+        """self.loss = mse(ws.out, ws.target) (+ grad_weight x the squared differences of the
+        error between adjacent cells); self.grad = its gradient (forward must have run)."""
         L.set_stream_from_torch()
-        mse(ws.out, ws.target, ws.dout, self.loss, self.g["head.b"], self.work64)
+        if grad_weight > 0:
+            h1_loss(ws.out, ws.target, grad_weight, ws.dout, self.loss, self.g["head.b"], self.work64)
+        else:
+            mse(ws.out, ws.target, ws.dout, self.loss, self.g["head.b"], self.work64)
         colsum(ws.d0, ws.dout, self.g["head.w"], self.work)
         head_bwd_x(ws.d0, self.p["head.w"], ws.dout, ws.g_d0)
         b = self._bwd
@@ -386,47 +396,64 @@ class WarmStart:
 # synthetic problems (GPU)
 # ---------------------------------------------------------------------------------------------
 
+def _shape3(ne):
+    """(nx, ny, nz) from an edge length or a 3-tuple."""
+    return (ne, ne, ne) if isinstance(ne, int) else tuple(int(v) for v in ne)
+
+
 def gaussian_random_field(n, ne, corr_cells, gen, device="cuda"):
-    """n zero-mean, unit-variance fields on ne^3 cells: white noise smoothed by a periodic
-    Gaussian of standard deviation corr_cells cells, (n, ne, ne, ne) fp32, x fastest."""
-    noise = torch.randn((n, ne, ne, ne), generator=gen, device=device, dtype=torch.float32)
-    f = torch.fft.fftfreq(ne, device=device) * (2 * math.pi)
-    fr = torch.fft.rfftfreq(ne, device=device) * (2 * math.pi)
-    k2 = f[:, None, None] ** 2 + f[None, :, None] ** 2 + fr[None, None, :] ** 2
+    """n zero-mean, unit-variance fields on ne^3 (or nx x ny x nz) cells: white noise
+    smoothed by a periodic Gaussian of standard deviation corr_cells cells,
+    (n, nz, ny, nx) fp32, x fastest."""
+    nx, ny, nz = _shape3(ne)
+    noise = torch.randn((n, nz, ny, nx), generator=gen, device=device, dtype=torch.float32)
+    fz = torch.fft.fftfreq(nz, device=device) * (2 * math.pi)
+    fy = torch.fft.fftfreq(ny, device=device) * (2 * math.pi)
+    fx = torch.fft.rfftfreq(nx, device=device) * (2 * math.pi)
+    k2 = fz[:, None, None] ** 2 + fy[None, :, None] ** 2 + fx[None, None, :] ** 2
     g = torch.fft.irfftn(torch.fft.rfftn(noise, dim=(1, 2, 3)) * torch.exp(-0.5 * corr_cells ** 2 * k2),
-                         s=(ne, ne, ne), dim=(1, 2, 3))
+                         s=(nz, ny, nx), dim=(1, 2, 3))
     g = g - g.mean(dim=(1, 2, 3), keepdim=True)
-    return g / g.std(dim=(1, 2, 3), keepdim=True)
+    # a correlation length of the order of the grid leaves (almost) a constant: zero field
+    return g / g.std(dim=(1, 2, 3), keepdim=True).clamp_min(1e-6)
 
 
 def gaussian_blobs(n, ne, width_cells, gen, nblobs=4, device="cuda"):
-    """sum of nblobs Gaussian blobs per sample, amplitudes U(-1, 1), centres U(0, 1)^3,
-    sampled at the element centres of ne^3 cells on the unit cube; (n, ne, ne, ne) fp32."""
+    """sum of nblobs Gaussian blobs per sample, amplitudes U(-1, 1), centres uniform in the
+    domain, sampled at the element centres of ne^3 (or nx x ny x nz) unit cells scaled to
+    the unit cube (cell sizes 1/nx, 1/ny, 1/nz; widths in cells of each axis);
+    (n, nz, ny, nx) fp32."""
+    nx, ny, nz = _shape3(ne)
     amps = torch.rand((n, nblobs), generator=gen, device=device) * 2 - 1
     ctr = torch.rand((n, nblobs, 3), generator=gen, device=device)
-    h = 1.0 / ne
-    xc = (torch.arange(ne, device=device, dtype=torch.float32) + 0.5) * h
-    w2 = 2 * (width_cells * h) ** 2
-    y = torch.zeros((n, ne, ne, ne), device=device)
+    y = torch.zeros((n, nz, ny, nx), device=device)
+    axes = []
+    for cnt in (nx, ny, nz):
+        axes.append((torch.arange(cnt, device=device, dtype=torch.float32) + 0.5) / cnt)
     for b in range(nblobs):
-        fx = torch.exp(-(xc[None, :] - ctr[:, b, 0:1]) ** 2 / w2)
-        fy = torch.exp(-(xc[None, :] - ctr[:, b, 1:2]) ** 2 / w2)
-        fz = torch.exp(-(xc[None, :] - ctr[:, b, 2:3]) ** 2 / w2)
-        y += amps[:, b, None, None, None] * fz[:, :, None, None] * fy[:, None, :, None] * fx[:, None, None, :]
+        f = []
+        for d, cnt in enumerate((nx, ny, nz)):
+            w2 = 2 * (width_cells / cnt) ** 2
+            f.append(torch.exp(-(axes[d][None, :] - ctr[:, b, d:d + 1]) ** 2 / w2))
+        y += amps[:, b, None, None, None] * f[2][:, :, None, None] * f[1][:, None, :, None] * f[0][:, None, None, :]
     return y
 
 
 class BrickProblem:
-    """-div(kappa grad u) = Y on a Brick of ne^3 elements, u = 0 on the top face z = 1, with
-    kappa and Y per element, assembled and solved through the C entry points."""
+    """-div(kappa grad u) = Y on a Brick of ne^3 (or nx x ny x nz) elements on [0,1]^3 (each
+    axis), u = 0 on the top face z = 1, with kappa and Y per element, assembled and solved
+    through the C entry points."""
 
     def __init__(self, ne, device="cuda"):
         lib = L.lib()
+        self.shape = _shape3(ne)
         self.ne = ne
+        nx, ny, nz = self.shape
+        self.nel = nx * ny * nz
         self.device = torch.device(device)
         self.dom = C.c_void_p()
         L.set_stream_from_torch()
-        L.check(lib.rg_domain_create(3, (C.c_int64 * 3)(ne, ne, ne), (C.c_double * 3)(0, 0, 0),
+        L.check(lib.rg_domain_create(3, (C.c_int64 * 3)(nx, ny, nz), (C.c_double * 3)(0, 0, 0),
                                      (C.c_double * 3)(1, 1, 1), C.byref(self.dom)))
         n = C.c_int64()
         L.check(lib.rg_domain_info(self.dom, C.byref(n), None, None, None, None))
@@ -435,11 +462,10 @@ class BrickProblem:
         L.check(lib.rg_matrix_create(self.dom, C.byref(self.mat)))
         self.rhs = torch.zeros(self.n, dtype=torch.float64, device=self.device)
         self.x = torch.zeros(self.n, dtype=torch.float64, device=self.device)
-        nn = ne + 1
         self.q = torch.zeros(self.n, dtype=torch.float64, device=self.device)
-        self.q[(nn - 1) * nn * nn:] = 1.0
-        self.A = torch.zeros((ne ** 3, 3, 3), dtype=torch.float64, device=self.device)
-        self.Y = torch.zeros(ne ** 3, dtype=torch.float64, device=self.device)
+        self.q[nz * (nx + 1) * (ny + 1):] = 1.0
+        self.A = torch.zeros((self.nel, 3, 3), dtype=torch.float64, device=self.device)
+        self.Y = torch.zeros(self.nel, dtype=torch.float64, device=self.device)
 
     def close(self):
         lib = L.lib()
@@ -457,7 +483,7 @@ class BrickProblem:
             self.A[:, i, i] = kappa_elem.reshape(-1)
         L.set_stream_from_torch()
         L.check(lib.rg_matrix_reset(self.mat))
-        self.set_rhs(y_elem if y_elem is not None else torch.zeros(self.ne ** 3, device=self.device),
+        self.set_rhs(y_elem if y_elem is not None else torch.zeros(self.nel, device=self.device),
                      with_matrix=True)
 
     def set_rhs(self, y_elem, with_matrix=False):
@@ -478,7 +504,7 @@ class BrickProblem:
                                            C.byref(e), C.byref(e), C.byref(cY)))
             L.check(lib.rg_insert_constraint(self.mat, _p(self.rhs), _p(self.q), None, 1))
 
-    def solve(self, tol=1e-8, fp32=True, guess=None, iter_max=100000):
+    def solve(self, tol=1e-8, fp32=True, guess=None, iter_max=100000, guess_sweeps=0):
         lib = L.lib()
         o = L.rg_solver_opts()
         lib.rg_solver_opts_default(C.byref(o))
@@ -489,6 +515,7 @@ class BrickProblem:
         o.layout = L.RG_LAYOUT_BAND if fp32 else L.RG_LAYOUT_CSR
         if guess is not None:
             o.initial_guess = guess.data_ptr()
+            o.guess_sweeps = guess_sweeps
         d = L.rg_diag()
         L.set_stream_from_torch()
         L.check(lib.rg_solve(self.mat, _p(self.rhs), _p(self.x), C.byref(o), C.byref(d)))

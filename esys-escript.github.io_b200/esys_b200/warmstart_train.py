@@ -47,7 +47,7 @@ def generate(nsamples, rhs_per_kappa, seed, device="cuda", tol=1e-10, log=print,
                 break
             if r:
                 prob.set_rhs(ys[r].double())
-            d = prob.solve(tol=tol, fp32=True)
+            d = prob.solve(tol=tol, fp32=False)
             if not d.converged:
                 raise RuntimeError(f"training solve {i} did not converge")
             iters.append(int(d.num_iter))
@@ -67,7 +67,17 @@ def generate(nsamples, rhs_per_kappa, seed, device="cuda", tol=1e-10, log=print,
                     "tol": tol, "rhs_per_kappa": rhs_per_kappa, "seed": seed}
 
 
-def train(net, xs, ts, epochs, batch, lr, val_frac=0.02, log=print, time_limit=None, seed=0):
+def cell_centres(ne, device="cuda"):
+    """(ne, ne, ne, 3) cell-centre coordinates (z, y, x) in the unit cube: the input channels
+    2..4 that rg_ws_pack_input writes."""
+    c = (torch.arange(ne, device=device, dtype=torch.float32) + 0.5) / ne
+    z, y, x = torch.meshgrid(c, c, c, indexing="ij")
+    return torch.stack([z, y, x], dim=-1)
+
+
+def train(net, xs, ts, epochs, batch, lr, val_frac=0.02, log=print, time_limit=None, seed=0, grad_weight=0.0,
+          warmup=300):
+    """Adam with a linear warm-up over `warmup` steps and a cosine decay to 1% of lr."""
     n = xs.shape[0]
     nval = max(batch, int(n * val_frac)) if n > 4 * batch else 0
     ntr = n - nval
@@ -76,6 +86,7 @@ def train(net, xs, ts, epochs, batch, lr, val_frac=0.02, log=print, time_limit=N
     g = torch.Generator(device="cpu").manual_seed(seed)
     t0, step, hist = time.time(), 0, []
     W.interior(ws.x0).zero_()
+    W.interior(ws.x0)[..., 2:5].copy_(cell_centres(NET, net.device).to(torch.bfloat16))
     while step < steps:
         perm = torch.randperm(ntr, generator=g)
         for b0 in range(0, ntr - batch + 1, batch):
@@ -83,8 +94,8 @@ def train(net, xs, ts, epochs, batch, lr, val_frac=0.02, log=print, time_limit=N
             W.interior(ws.x0)[..., :2].copy_(xs.index_select(0, idx))
             ws.target.copy_(ts.index_select(0, idx))
             net.forward(ws)
-            net.loss_and_backward(ws)
-            cur = lr * 0.5 * (1 + math.cos(math.pi * step / steps))
+            net.loss_and_backward(ws, grad_weight)
+            cur = lr * 0.5 * (1 + math.cos(math.pi * step / steps)) * min(1.0, (step + 1) / max(warmup, 1))
             net.adam_step(max(cur, lr * 0.01))
             step += 1
             if step % 200 == 0 or step == steps:
@@ -112,13 +123,62 @@ def train(net, xs, ts, epochs, batch, lr, val_frac=0.02, log=print, time_limit=N
             "val_rel_l2": val, "loss_history": hist}
 
 
+def evaluate(net, ne, nprob, seed, tol=1e-8, corr=8.0, width=3.0, device="cuda", log=print, sweeps=(0, 4, 16)):
+    """A/B on fresh seeded problems of ne^3 elements (kappa correlation `corr` cells, blobs
+    `width` cells wide): PCG (FP32 inner, FP64 refinement) from zero and from the network's
+    guess, to the same tolerance.  Times are CUDA-event times of guess + solve."""
+    gen = torch.Generator(device=device).manual_seed(seed)
+    prob = W.BrickProblem(ne, device=device)
+    ws = W.WarmStart(net)
+    guess = torch.zeros(prob.n, dtype=torch.float64, device=device)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    rows = []
+    for k in range(nprob):
+        kappa = torch.exp(W.gaussian_random_field(1, ne, corr, gen, device=device))[0]
+        y = W.gaussian_blobs(1, ne, width, gen, device=device)[0]
+        prob.assemble(kappa.double(), y.double())
+        prob.solve(tol=tol)                         # balances the matrix (set-up out of the timing)
+        ev[0].record()
+        d0 = prob.solve(tol=tol)
+        ev[1].record()
+        x0 = prob.x.clone()
+        row = {"zero_iters": int(d0.num_iter), "zero_ms": ev[0].elapsed_time(ev[1])}
+        for sw in sweeps:
+            ev[2].record()
+            ws.guess(kappa[None], y[None], (ne,) * 3, q=prob.q, out=guess)
+            d1 = prob.solve(tol=tol, guess=guess, guess_sweeps=sw)
+            ev[3].record()
+            torch.cuda.synchronize()
+            row.update({f"warm{sw}_iters": int(d1.num_iter), f"warm{sw}_ms": ev[2].elapsed_time(ev[3]),
+                        f"guess{sw}_rel_residual": d1.guess_residual / d1.rhs_norm,
+                        f"rejected{sw}": bool(d1.guess_rejected),
+                        f"diff{sw}": float((prob.x - x0).norm() / x0.norm())})
+        row["guess_rel_error"] = float((guess - x0).norm() / x0.norm())
+        rows.append(row)
+        if log:
+            log(json.dumps({"ne": ne, "problem": k, **row}))
+    prob.close()
+    agg = {k: float(np.mean([r[k] for r in rows])) for k in rows[0]}
+    agg["n"] = nprob
+    return agg, rows
+
+
+def _residual(prob, x):
+    import ctypes as C
+    from . import _lib as L
+    l2, lm = C.c_double(), C.c_double()
+    L.check(L.lib().rg_residual_norms(prob.mat, C.c_void_p(prob.rhs.data_ptr()), C.c_void_p(x.data_ptr()),
+                                      C.byref(l2), C.byref(lm)))
+    return l2.value, lm.value
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
     ap.add_argument("--samples", type=int, default=20000)
     ap.add_argument("--rhs-per-kappa", type=int, default=4)
-    ap.add_argument("--epochs", type=int, default=4)
+    ap.add_argument("--epochs", type=int, default=6)
     ap.add_argument("--batch", type=int, default=8)
-    ap.add_argument("--lr", type=float, default=2e-3)
+    ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--seed", type=int, default=12345)
     ap.add_argument("--gen-time-limit", type=float, default=None)
     ap.add_argument("--train-time-limit", type=float, default=None)

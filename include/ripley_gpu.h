@@ -166,6 +166,8 @@ typedef struct {
                                    between FP64 residual replacements (default 1e-2)      */
     const double* initial_guess;/* STANDARD mode only: device x0 (unbalanced units) or NULL;
                                    dropped for zero when ||B(b - A x0)|| > ||B b||          */
+    int guess_sweeps;           /* damped Jacobi sweeps (omega 0.6) applied to initial_guess
+                                   before that test; default 0                            */
 } rg_solver_opts;
 
 typedef struct {
@@ -181,6 +183,8 @@ typedef struct {
     double guess_residual;      /* l2 norm of the balanced residual of the initial guess    */
     int guess_rejected;         /* 1: the guess's residual exceeded the right hand side's
                                    and the solve started from zero instead                  */
+    int fp64_fallback;          /* FP32_REFINE: 1 when the FP32 corrections stopped reducing
+                                   the FP64 residual and the solve finished in FP64 PCG     */
 } rg_diag;
 
 void rg_solver_opts_default(rg_solver_opts* opts);
@@ -189,6 +193,28 @@ void rg_solver_opts_default(rg_solver_opts* opts);
 int rg_solve(rg_matrix* mat, const double* rhs, double* x, const rg_solver_opts* opts,
              rg_diag* diag);
 
+
+/* ---- batched solves (no reference counterpart: many independent systems at once) ------- */
+/* A batch holds assembled matrices of the same dimension (any sizes) that are solved
+   together, each with nrhs right hand sides (1, 2, 4 or 8), by PCG + Jacobi with FP32 inner
+   iterations and FP64 refinement: paso's dual-norm stopping test per right hand side.  The
+   matrices are balanced and prepared at creation; they must not change while the batch
+   lives.  Every kernel launch advances all systems; chunks of iterations replay as CUDA
+   graphs; grid sizes and the chunk length come from rg_batch_tune (run by the first solve
+   when not called). */
+typedef struct rg_batch rg_batch;
+int rg_batch_create(rg_matrix* const* mats, int nsystems, int nrhs, rg_batch** out);
+int rg_batch_destroy(rg_batch* batch);
+int rg_batch_tune(rg_batch* batch);
+/* rows: padded batch rows; tiles: 256-row tiles; grids in CTAs; iter_us: measured time of
+   one iteration of all systems at the tuned grids */
+int rg_batch_info(const rg_batch* batch, int64_t* rows, int64_t* tiles, int* grid_spmv, int* grid_update,
+                  int* chunk, double* iter_us);
+/* rhs[i], x[i]: device arrays of n_i * nrhs doubles for system i, right hand side k at
+   offset k * n_i.  opts: tolerance, iter_max, inner_tolerance, accept_convergence_failure
+   (NULL: defaults).  diag: nsystems * nrhs entries (system-major) or NULL. */
+int rg_batch_solve(rg_batch* batch, const double* const* rhs, double* const* x, const rg_solver_opts* opts,
+                   rg_diag* diag);
 
 /* ---- instrumentation ------------------------------------------------------------------ */
 /* Every kernel launch of the library is counted per kind; with timers enabled each launch
@@ -247,6 +273,10 @@ int rg_ws_colsum(const rg_act* v, const float* dout, float* out, float* work, in
    (may be NULL); work: 1184 doubles */
 int rg_ws_mse(const float* out, const float* target, int64_t count, float* dout, double* loss_dev,
               float* dsum_dev, double* work);
+/* as rg_ws_mse on an (n, d, h, w) grid with a gradient term: loss = (sum e_i^2 + lambda sum over
+   face-adjacent cell pairs (e_i - e_j)^2) / count, e = out - target */
+int rg_ws_h1_loss(const float* out, const float* target, int n, int d, int h, int w, float lambda, float* dout,
+                  double* loss_dev, float* dsum_dev, double* work);
 /* Adam step `step` (>= 1, bias-corrected) on fp32 master weights */
 int rg_ws_adam(float* w, const float* g, float* m, float* v, int64_t count, float lr, float beta1,
                float beta2, float eps, int step);
@@ -258,6 +288,7 @@ int rg_ws_weights_bf16(const float* w, void* w_fwd, void* w_dgrad, int c_out, in
    integer factor.  rg_ws_field_stats writes 4 floats per sample: mu = mean log kappa,
    sY = max |Y|, kappa_g = exp(mu), u_unit = 10 sY h_net^2 / kappa_g (work: 128 * nsamples
    doubles).  The network sees (log kappa - mu, Y / sY) averaged over each of its cells and
+   the cell centre's (z, y, x) in the unit cube (channels 0..4, x->c >= 5; others zero), and
    predicts u / u_unit per cell. */
 int rg_ws_field_stats(const float* kappa, const float* y, int nsamples, int64_t per_sample, double h_net,
                       float* stats, double* work);

@@ -247,7 +247,11 @@ def test_field_maps_are_consistent(cuda):
     xi = W.interior(x0).float()
     assert torch.allclose(xi[..., 0], lk, atol=2e-2, rtol=1e-2)
     assert torch.allclose(xi[..., 1], yy, atol=2e-2, rtol=1e-2)
-    assert not bool(xi[..., 2:].any())
+    c = (torch.arange(8, device="cuda", dtype=torch.float32) + 0.5) / 8
+    assert torch.allclose(xi[0, :, 0, 0, 2], c, atol=4e-3)
+    assert torch.allclose(xi[0, 0, :, 0, 3], c, atol=4e-3)
+    assert torch.allclose(xi[0, 0, 0, :, 4], c, atol=4e-3)
+    assert not bool(xi[..., 5:].any())
     # a linear nodal field: cell means are exact, and interpolating them back reproduces
     # every node at least half a cell away from the faces
     nn = fine[0] + 1
@@ -336,3 +340,24 @@ def test_training_steps_reduce_the_loss(cuda):
     torch.cuda.synchronize()
     net.err.check()
     assert losses[-1] < 0.5 * losses[0], losses
+
+
+def test_h1_loss_matches_torch(cuda):
+    torch.manual_seed(10)
+    n, d, h, w, lam = 2, 8, 16, 16, 5.0
+    out = torch.randn(n, d, h, w, device="cuda")
+    t = torch.randn(n, d, h, w, device="cuda")
+    dout = torch.empty_like(out)
+    loss = torch.zeros(1, dtype=torch.float64, device="cuda")
+    dsum = torch.zeros(1, device="cuda")
+    W.h1_loss(out, t, lam, dout, loss, dsum, torch.zeros(1184, dtype=torch.float64, device="cuda"))
+    o = out.double().cpu().requires_grad_(True)
+    e = o - t.double().cpu()
+    ref = (e * e).sum()
+    for ax in (1, 2, 3):
+        ref = ref + lam * (torch.diff(e, dim=ax) ** 2).sum()
+    ref = ref / e.numel()
+    ref.backward()
+    assert abs(loss.item() - ref.item()) <= 1e-6 * ref.item()
+    assert torch.allclose(dout.double().cpu(), o.grad, rtol=1e-4, atol=1e-7)
+    assert abs(dsum.item() - o.grad.sum().item()) <= 1e-5

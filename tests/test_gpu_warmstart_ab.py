@@ -1,0 +1,49 @@
+"""What the trained warm-start network gains over the zero initial guess (A/B), and the
+fallback when a guess is worse than zero.
+
+The committed weights (esys_b200/data/warmstart_unet.npz) were trained by
+`python -m esys_b200.warmstart_train --samples 20000 --epochs 6` on problems from generator
+seed 12345; the problems here come from other seeds.  Both arms solve with FP32 inner
+iterations and FP64 refinement to rtol 1e-8, so both meet the same residual test."""
+import numpy as np
+import pytest
+import torch
+
+from esys_b200 import warmstart as W
+from esys_b200 import warmstart_train as T
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def net(cuda):
+    return W.UNet.load()
+
+
+def test_trained_guess_saves_iterations_at_64(net):
+    agg, rows = T.evaluate(net, 64, 6, seed=777, log=None, sweeps=(64,))
+    for r in rows:
+        assert not r["rejected64"]
+        assert r["diff64"] < 1e-6          # same solution to the tolerance's accuracy
+    print({k: v for k, v in agg.items()})
+    assert agg["warm64_iters"] < agg["zero_iters"]
+    assert agg["guess_rel_error"] < 0.6    # the network knows the solution's shape
+
+
+def test_guess_worse_than_zero_falls_back(net):
+    prob = W.BrickProblem(32)
+    gen = torch.Generator(device="cuda").manual_seed(5)
+    kappa = torch.exp(W.gaussian_random_field(1, 32, 4.0, gen))[0]
+    y = W.gaussian_blobs(1, 32, 1.5, gen)[0]
+    prob.assemble(kappa.double(), y.double())
+    d0 = prob.solve(tol=1e-8)
+    x0 = prob.x.clone()
+    bad = torch.randn(prob.n, dtype=torch.float64, device="cuda") * 1e3 * float(x0.abs().max())
+    d1 = prob.solve(tol=1e-8, guess=bad)
+    assert d1.guess_rejected == 1 and d1.guess_residual > d1.rhs_norm
+    assert d1.num_iter == d0.num_iter
+    assert torch.allclose(prob.x, x0, rtol=0, atol=1e-12 * float(x0.abs().max()))
+    # the exact solution is kept and converges at once
+    d2 = prob.solve(tol=1e-8, guess=x0)
+    assert d2.guess_rejected == 0 and d2.num_iter <= 1
+    prob.close()
