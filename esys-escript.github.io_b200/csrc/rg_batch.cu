@@ -48,7 +48,13 @@ struct Inst {
     const int32_t* idx;
     const double* val;
     const double* bv;     // balance vector
+    int64_t nunits;       // work units of the iteration kernels (current tile-group size)
 };
+
+// A work unit of the iteration kernels: up to `group` consecutive tiles of one system (the
+// autotuned tile-group size); one partial sum per unit.  .x system, .y first batch tile,
+// .z tiles, .w the unit's index within its system.
+using Unit = int4;
 
 // per right hand side state (device); host reads and writes it between segments
 struct Rhs {
@@ -78,6 +84,9 @@ struct Batch {
     std::vector<Matrix*> mats;
     Inst* d_inst = nullptr;
     int* d_tile_inst = nullptr;
+    Unit* d_units = nullptr;      // iteration work units (capacity ntiles)
+    int64_t nunits = 0;
+    int group = 4;                // tiles per work unit
     int* d_inst_active = nullptr;
     int* d_nactive = nullptr;     // number of active right hand sides
     int* h_nactive = nullptr;     // pinned
@@ -176,25 +185,25 @@ __device__ void block_sum_to(double (&v)[NV], double* out)
     __syncthreads();
 }
 
-// Ticket of system i: true in the CTA that wrote the system's last tile partial, which then
-// reduces the partials of all its tiles (fixed order) into tot[0..NV).
+// Ticket of system i: true in the CTA that wrote the last of the system's `count` partials
+// (slots first..first+count-1), which then reduces them in a fixed order into tot[0..NV).
 template <int NV>
-__device__ bool last_tile_reduce(const Inst& I, int i, unsigned* cnt, const double* part, int stride,
-                                 double (&tot)[NV])
+__device__ bool last_reduce(int i, int64_t first, int64_t count, unsigned* cnt, const double* part, int stride,
+                            double (&tot)[NV])
 {
     __shared__ bool last;
     __threadfence();
     __syncthreads();
-    if (threadIdx.x == 0) last = atomicAdd(&cnt[i], 1u) == (unsigned)(I.ntiles - 1);
+    if (threadIdx.x == 0) last = atomicAdd(&cnt[i], 1u) == (unsigned)(count - 1);
     __syncthreads();
     if (!last) return false;
     __threadfence();
     double a[NV];
 #pragma unroll
     for (int j = 0; j < NV; ++j) a[j] = 0.0;
-    for (int64_t t = threadIdx.x; t < I.ntiles; t += kTile)
+    for (int64_t t = threadIdx.x; t < count; t += kTile)
 #pragma unroll
-        for (int j = 0; j < NV; ++j) a[j] += __ldcg(part + (I.tile0 + t) * stride + j);
+        for (int j = 0; j < NV; ++j) a[j] += __ldcg(part + (first + t) * stride + j);
     __shared__ double res[NV];
     block_sum_to<NV>(a, res);
 #pragma unroll
@@ -203,49 +212,88 @@ __device__ bool last_tile_reduce(const Inst& I, int i, unsigned* cnt, const doub
     return true;
 }
 
+template <int NV>
+__device__ bool last_tile_reduce(const Inst& I, int i, unsigned* cnt, const double* part, int stride,
+                                 double (&tot)[NV])
+{
+    return last_reduce<NV>(i, I.tile0, I.ntiles, cnt, part, stride, tot);
+}
+
+
 // ------------------------------------------------------------------ inner iteration kernels
-// q = A p for every row of every active system, and the p.q partial sums
+// q = A p for every row of every active system, and the p.q partial sums.  A warp holds 32
+// consecutive rows, so of the three columns dx = -1, 0, +1 of a stencil line only dx = 0 is
+// loaded: the other two come from the neighbouring lanes (lanes 0 and 31 load their outer
+// value), a third of the vector traffic of one load per band.
 template <int R, int NB>
-__global__ void __launch_bounds__(kTile) k_b_spmv(const Inst* __restrict__ insts, const int* __restrict__ tile_inst,
-                                                  int64_t ntiles, const int* __restrict__ inst_active,
+__global__ void __launch_bounds__(kTile, 3) k_b_spmv(const Inst* __restrict__ insts, const Unit* __restrict__ units,
+                                                  int64_t nunits, const int* __restrict__ inst_active,
                                                   const float* __restrict__ p, float* __restrict__ q,
                                                   double* __restrict__ part, unsigned* __restrict__ cnt,
                                                   Rhs* __restrict__ st)
 {
-    for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
-        const int i = tile_inst[t];
+    constexpr int NL = NB / 3;  // stencil lines (dy, dz)
+    const int lane = threadIdx.x & 31;
+    for (int64_t u = blockIdx.x; u < nunits; u += gridDim.x) {
+        const Unit un = units[u];
+        const int i = un.x;
         if (!inst_active[i]) continue;
         const Inst& I = insts[i];
-        const int64_t lt = t - I.tile0;
-        const int64_t row = lt * kTile + threadIdx.x;
-        const bool valid = row < I.n;
-        float acc[R], self[R];
+        const int64_t n = I.n;
+        int64_t off[NL];
 #pragma unroll
-        for (int r = 0; r < R; ++r) acc[r] = self[r] = 0.f;
-        if (valid) {
+        for (int g = 0; g < NL; ++g) off[g] = I.off[3 * g + 1];
+        const float* pv = p + I.voff * R;
+        float vf[R];  // per-thread partial over the unit's rows (at most 8 terms)
+#pragma unroll
+        for (int r = 0; r < R; ++r) vf[r] = 0.f;
+        for (int k = 0; k < un.z; ++k) {
+            const int64_t lt = un.y + k - I.tile0;
+            const int64_t row = lt * kTile + threadIdx.x;
+            float acc[R], self[R];
+#pragma unroll
+            for (int r = 0; r < R; ++r) acc[r] = self[r] = 0.f;
             const float* bt = I.band + lt * NB * kTile + threadIdx.x;
-            const float* pv = p + I.voff * R;
-#pragma unroll 9
-            for (int b = 0; b < NB; ++b) {
-                const float a = __ldcs(bt + b * kTile);
-                int64_t j = row + I.off[b];
-                j = j < 0 ? 0 : (j >= I.n ? I.n - 1 : j);  // absent neighbours have a == 0
-                float v[R];
-                Vec<R>::ld(pv + j * R, v);
 #pragma unroll
-                for (int r = 0; r < R; ++r) acc[r] = fmaf(a, v[r], acc[r]);
-                if (b == NB / 2)
+            for (int g = 0; g < NL; ++g) {
+                const float am = __ldcs(bt + (3 * g) * kTile);
+                const float a0 = __ldcs(bt + (3 * g + 1) * kTile);
+                const float ap = __ldcs(bt + (3 * g + 2) * kTile);
+                const int64_t c = row + off[g];
+                const int64_t j = c < 0 ? 0 : (c >= n ? n - 1 : c);  // absent neighbours have a == 0
+                float w[R], lv[R], rv[R];
+                Vec<R>::ld(pv + j * R, w);
 #pragma unroll
-                    for (int r = 0; r < R; ++r) self[r] = v[r];
+                for (int r = 0; r < R; ++r) {
+                    lv[r] = __shfl_up_sync(0xffffffffu, w[r], 1);
+                    rv[r] = __shfl_down_sync(0xffffffffu, w[r], 1);
+                }
+                if (lane == 0) {
+                    const int64_t jl = c - 1 < 0 ? 0 : (c - 1 >= n ? n - 1 : c - 1);
+                    Vec<R>::ld(pv + jl * R, lv);
+                }
+                if (lane == 31) {
+                    const int64_t jr = c + 1 < 0 ? 0 : (c + 1 >= n ? n - 1 : c + 1);
+                    Vec<R>::ld(pv + jr * R, rv);
+                }
+#pragma unroll
+                for (int r = 0; r < R; ++r) acc[r] = fmaf(am, lv[r], fmaf(a0, w[r], fmaf(ap, rv[r], acc[r])));
+                if (g == NL / 2)
+#pragma unroll
+                    for (int r = 0; r < R; ++r) self[r] = w[r];
             }
-            Vec<R>::st(q + (I.voff + row) * R, acc);
+            if (row < n) {
+                Vec<R>::st(q + (I.voff + row) * R, acc);
+#pragma unroll
+                for (int r = 0; r < R; ++r) vf[r] = fmaf(self[r], acc[r], vf[r]);
+            }
         }
         double v[R];
 #pragma unroll
-        for (int r = 0; r < R; ++r) v[r] = (double)self[r] * (double)acc[r];
-        block_sum_to<R>(v, part + t * 2 * R);
+        for (int r = 0; r < R; ++r) v[r] = vf[r];
+        block_sum_to<R>(v, part + u * 2 * R);
         double tot[R];
-        if (last_tile_reduce<R>(I, i, cnt, part, 2 * R, tot) && threadIdx.x < R) {
+        if (last_reduce<R>(i, u - un.w, I.nunits, cnt, part, 2 * R, tot) && threadIdx.x < R) {
             Rhs& s = st[i * R + threadIdx.x];
             if (s.active) {
                 const double pq = tot[threadIdx.x];
@@ -264,15 +312,16 @@ __global__ void __launch_bounds__(kTile) k_b_spmv(const Inst* __restrict__ insts
 // d += alpha p, r -= alpha q, z = dinv r; partial r.z and r.r; the last CTA of a system
 // sets beta and pauses right hand sides that met their segment target or stagnated
 template <int R>
-__global__ void __launch_bounds__(kTile) k_b_update(const Inst* __restrict__ insts, const int* __restrict__ tile_inst,
-                                                    int64_t ntiles, int* __restrict__ inst_active,
+__global__ void __launch_bounds__(kTile, 3) k_b_update(const Inst* __restrict__ insts, const Unit* __restrict__ units,
+                                                    int64_t nunits, int* __restrict__ inst_active,
                                                     const float* __restrict__ p, const float* __restrict__ q,
                                                     float* __restrict__ r32, float* __restrict__ d32,
                                                     double* __restrict__ part, unsigned* __restrict__ cnt,
                                                     Rhs* __restrict__ st, int* __restrict__ nactive, int maxit)
 {
-    for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
-        const int i = tile_inst[t];
+    for (int64_t u = blockIdx.x; u < nunits; u += gridDim.x) {
+        const Unit un = units[u];
+        const int i = un.x;
         if (!inst_active[i]) continue;
         const Inst& I = insts[i];
         __shared__ float alpha[8];
@@ -283,34 +332,39 @@ __global__ void __launch_bounds__(kTile) k_b_update(const Inst* __restrict__ ins
             alpha[threadIdx.x] = (float)s.alpha;
         }
         __syncthreads();
-        const int64_t row = (t - I.tile0) * kTile + threadIdx.x;
+        float vf[2 * R];  // per-thread partials over the unit's rows (at most 8 terms)
+#pragma unroll
+        for (int r = 0; r < 2 * R; ++r) vf[r] = 0.f;
+        for (int k = 0; k < un.z; ++k) {
+            const int64_t row = (un.y + k - I.tile0) * kTile + threadIdx.x;
+            if (row < I.n) {
+                const int64_t o = (I.voff + row) * R;
+                float pv[R], qv[R], rv[R], dv[R];
+                Vec<R>::ld(p + o, pv);
+                Vec<R>::ld(q + o, qv);
+                Vec<R>::ld(r32 + o, rv);
+                Vec<R>::ld(d32 + o, dv);
+                const float di = I.dinv32[row];
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    if (act[r]) {
+                        dv[r] = fmaf(alpha[r], pv[r], dv[r]);
+                        rv[r] = fmaf(-alpha[r], qv[r], rv[r]);
+                    }
+                    const float z = di * rv[r];
+                    vf[r] = fmaf(rv[r], z, vf[r]);
+                    vf[R + r] = fmaf(rv[r], rv[r], vf[R + r]);
+                }
+                Vec<R>::st(r32 + o, rv);
+                Vec<R>::st(d32 + o, dv);
+            }
+        }
         double v[2 * R];
 #pragma unroll
-        for (int r = 0; r < 2 * R; ++r) v[r] = 0.0;
-        if (row < I.n) {
-            const int64_t o = (I.voff + row) * R;
-            float pv[R], qv[R], rv[R], dv[R];
-            Vec<R>::ld(p + o, pv);
-            Vec<R>::ld(q + o, qv);
-            Vec<R>::ld(r32 + o, rv);
-            Vec<R>::ld(d32 + o, dv);
-            const float di = I.dinv32[row];
-#pragma unroll
-            for (int r = 0; r < R; ++r) {
-                if (act[r]) {
-                    dv[r] = fmaf(alpha[r], pv[r], dv[r]);
-                    rv[r] = fmaf(-alpha[r], qv[r], rv[r]);
-                }
-                const float z = di * rv[r];
-                v[r] = (double)rv[r] * z;
-                v[R + r] = (double)rv[r] * rv[r];
-            }
-            Vec<R>::st(r32 + o, rv);
-            Vec<R>::st(d32 + o, dv);
-        }
-        block_sum_to<2 * R>(v, part + t * 2 * R);
+        for (int r = 0; r < 2 * R; ++r) v[r] = vf[r];
+        block_sum_to<2 * R>(v, part + u * 2 * R);
         double tot[2 * R];
-        if (last_tile_reduce<2 * R>(I, i, cnt, part, 2 * R, tot)) {
+        if (last_reduce<2 * R>(i, u - un.w, I.nunits, cnt, part, 2 * R, tot)) {
             __shared__ int any;
             if (threadIdx.x == 0) any = 0;
             __syncthreads();
@@ -347,18 +401,20 @@ __global__ void __launch_bounds__(kTile) k_b_update(const Inst* __restrict__ ins
             __syncthreads();
             if (threadIdx.x == 0) inst_active[i] = any;
         }
+        __syncthreads();
     }
 }
 
 // p = dinv r + beta p for the active right hand sides
 template <int R>
-__global__ void __launch_bounds__(kTile) k_b_pupdate(const Inst* __restrict__ insts, const int* __restrict__ tile_inst,
-                                                     int64_t ntiles, const int* __restrict__ inst_active,
+__global__ void __launch_bounds__(kTile) k_b_pupdate(const Inst* __restrict__ insts, const Unit* __restrict__ units,
+                                                     int64_t nunits, const int* __restrict__ inst_active,
                                                      float* __restrict__ p, const float* __restrict__ r32,
                                                      const Rhs* __restrict__ st)
 {
-    for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
-        const int i = tile_inst[t];
+    for (int64_t u = blockIdx.x; u < nunits; u += gridDim.x) {
+        const Unit un = units[u];
+        const int i = un.x;
         if (!inst_active[i]) continue;
         const Inst& I = insts[i];
         __shared__ float beta[8];
@@ -369,17 +425,19 @@ __global__ void __launch_bounds__(kTile) k_b_pupdate(const Inst* __restrict__ in
             beta[threadIdx.x] = (float)s.beta;
         }
         __syncthreads();
-        const int64_t row = (t - I.tile0) * kTile + threadIdx.x;
-        if (row < I.n) {
-            const int64_t o = (I.voff + row) * R;
-            float pv[R], rv[R];
-            Vec<R>::ld(p + o, pv);
-            Vec<R>::ld(r32 + o, rv);
-            const float di = I.dinv32[row];
+        for (int k = 0; k < un.z; ++k) {
+            const int64_t row = (un.y + k - I.tile0) * kTile + threadIdx.x;
+            if (row < I.n) {
+                const int64_t o = (I.voff + row) * R;
+                float pv[R], rv[R];
+                Vec<R>::ld(p + o, pv);
+                Vec<R>::ld(r32 + o, rv);
+                const float di = I.dinv32[row];
 #pragma unroll
-            for (int r = 0; r < R; ++r)
-                if (act[r]) pv[r] = fmaf(beta[r], pv[r], di * rv[r]);
-            Vec<R>::st(p + o, pv);
+                for (int r = 0; r < R; ++r)
+                    if (act[r]) pv[r] = fmaf(beta[r], pv[r], di * rv[r]);
+                Vec<R>::st(p + o, pv);
+            }
         }
         __syncthreads();
     }
@@ -642,19 +700,19 @@ int iter_step(Batch* b)
     const int nb = b->dim == 3 ? 27 : 9;
     if (nb == 27)
         RG_TIMED(T_BATCH_SPMV, (k_b_spmv<R, 27><<<b->grid_spmv, kTile, 0, stream()>>>(
-                                   b->d_inst, b->d_tile_inst, b->ntiles, b->d_inst_active, b->p, b->q, b->d_part,
+                                   b->d_inst, b->d_units, b->nunits, b->d_inst_active, b->p, b->q, b->d_part,
                                    b->d_cnt, b->d_rhs)));
     else
         RG_TIMED(T_BATCH_SPMV, (k_b_spmv<R, 9><<<b->grid_spmv, kTile, 0, stream()>>>(
-                                   b->d_inst, b->d_tile_inst, b->ntiles, b->d_inst_active, b->p, b->q, b->d_part,
+                                   b->d_inst, b->d_units, b->nunits, b->d_inst_active, b->p, b->q, b->d_part,
                                    b->d_cnt, b->d_rhs)));
     RG_CHECK_LAUNCH();
     RG_TIMED(T_BATCH_UPDATE, (k_b_update<R><<<b->grid_upd, kTile, 0, stream()>>>(
-                                 b->d_inst, b->d_tile_inst, b->ntiles, b->d_inst_active, b->p, b->q, b->r32, b->d32,
+                                 b->d_inst, b->d_units, b->nunits, b->d_inst_active, b->p, b->q, b->r32, b->d32,
                                  b->d_part, b->d_cnt, b->d_rhs, b->d_nactive, b->maxit)));
     RG_CHECK_LAUNCH();
     RG_TIMED(T_BATCH_UPDATE, (k_b_pupdate<R><<<b->grid_upd, kTile, 0, stream()>>>(
-                                 b->d_inst, b->d_tile_inst, b->ntiles, b->d_inst_active, b->p, b->r32, b->d_rhs)));
+                                 b->d_inst, b->d_units, b->nunits, b->d_inst_active, b->p, b->r32, b->d_rhs)));
     RG_CHECK_LAUNCH();
     return RG_OK;
 }
@@ -673,7 +731,7 @@ int launch_seed(Batch* b)
                                 b->d_part, b->d_cnt, b->d_rhs, b->d_nactive)));
     RG_CHECK_LAUNCH();
     RG_TIMED(T_BATCH_UPDATE, (k_b_pupdate<R><<<b->grid_upd, kTile, 0, stream()>>>(
-                                 b->d_inst, b->d_tile_inst, b->ntiles, b->d_inst_active, b->p, b->r32, b->d_rhs)));
+                                 b->d_inst, b->d_units, b->nunits, b->d_inst_active, b->p, b->r32, b->d_rhs)));
     RG_CHECK_LAUNCH();
     return RG_OK;
 }
@@ -859,31 +917,71 @@ int seed_all_active(Batch* b)
     return seed(b);
 }
 
+// work units of `group` consecutive tiles per system (the last unit of a system may be short)
+int set_group(Batch* b, int group)
+{
+    std::vector<Unit> units;
+    for (int i = 0; i < b->ninst; ++i) {
+        Inst& I = b->h_inst[i];
+        int w = 0;
+        for (int64_t t = 0; t < I.ntiles; t += group, ++w)
+            units.push_back(make_int4(i, (int)(I.tile0 + t), (int)std::min<int64_t>(group, I.ntiles - t), w));
+        I.nunits = w;
+    }
+    b->nunits = (int64_t)units.size();
+    b->group = group;
+    RG_CHECK_CUDA(cudaMemcpyAsync(b->d_units, units.data(), sizeof(Unit) * units.size(), cudaMemcpyHostToDevice,
+                                  stream()));
+    RG_CHECK_CUDA(cudaMemcpyAsync(b->d_inst, b->h_inst.data(), sizeof(Inst) * b->ninst, cudaMemcpyHostToDevice,
+                                  stream()));
+    RG_CHECK_CUDA(cudaStreamSynchronize(stream()));  // the host vectors go out of scope
+    if (b->graph) {
+        cudaGraphExecDestroy(b->graph);
+        b->graph = nullptr;
+    }
+    return RG_OK;
+}
+
 int tune(Batch* b)
 {
+    // candidates: tiles per work unit x CTAs per SM, the same grid for the three kernels
+    // first, then the update kernels' grid on its own
     int rc;
-    const int cands[] = {1, 2, 4, 8, 16};
+    const int groups[] = {1, 2, 4, 8};
+    const int cands[] = {2, 4, 8, 16};
     const int saved_maxit = b->maxit;
     b->maxit = 1 << 30;
     double best = 1e30;
-    int best_s = 4, best_u = 4;
-    // spmv grid first (update kernels at 8 CTAs/SM), then the update grid
-    for (int pass = 0; pass < 2; ++pass) {
+    int best_g = 4, best_s = 8, best_u = 8;
+    for (int g : groups) {
+        if ((rc = set_group(b, g))) return rc;
         for (int c : cands) {
-            if ((int64_t)c * kNumSMs > b->ntiles * 2 && c > 1) break;
-            b->grid_spmv = kNumSMs * (pass == 0 ? c : best_s);
-            b->grid_upd = kNumSMs * (pass == 0 ? 8 : c);
+            if (c > 2 && (int64_t)c * kNumSMs > b->nunits) break;
+            b->grid_spmv = b->grid_upd = kNumSMs * c;
             if ((rc = seed_all_active(b))) return rc;
             double ms;
-            if ((rc = time_iters(b, 2, &ms))) return rc;   // warm
+            if ((rc = time_iters(b, 2, &ms))) return rc;  // warm
             if ((rc = time_iters(b, 6, &ms))) return rc;
             if (ms < best) {
                 best = ms;
-                if (pass == 0) best_s = c;
-                else best_u = c;
+                best_g = g;
+                best_s = best_u = c;
             }
         }
-        if (pass == 0) best = 1e30;
+    }
+    if ((rc = set_group(b, best_g))) return rc;
+    for (int c : cands) {
+        if (c == best_s || (c > 2 && (int64_t)c * kNumSMs > b->nunits)) continue;
+        b->grid_spmv = kNumSMs * best_s;
+        b->grid_upd = kNumSMs * c;
+        if ((rc = seed_all_active(b))) return rc;
+        double ms;
+        if ((rc = time_iters(b, 2, &ms))) return rc;
+        if ((rc = time_iters(b, 6, &ms))) return rc;
+        if (ms < best) {
+            best = ms;
+            best_u = c;
+        }
     }
     b->grid_spmv = kNumSMs * best_s;
     b->grid_upd = kNumSMs * best_u;
@@ -903,6 +1001,7 @@ void destroy(Batch* b)
     if (!b) return;
     cudaFree(b->d_inst);
     cudaFree(b->d_tile_inst);
+    cudaFree(b->d_units);
     cudaFree(b->d_inst_active);
     cudaFree(b->d_nactive);
     cudaFreeHost(b->h_nactive);
@@ -1013,6 +1112,7 @@ int rg_batch_create(rg_matrix* const* mats, int ninst, int nrhs, rg_batch** out)
     };
     A((void**)&b->d_inst, sizeof(Inst) * ninst);
     A((void**)&b->d_tile_inst, sizeof(int) * b->ntiles);
+    A((void**)&b->d_units, sizeof(Unit) * b->ntiles);
     A((void**)&b->d_inst_active, sizeof(int) * ninst);
     A((void**)&b->d_nactive, sizeof(int));
     A((void**)&b->d_rhs, sizeof(Rhs) * b->h_rhs.size());
@@ -1055,7 +1155,12 @@ int rg_batch_create(rg_matrix* const* mats, int ninst, int nrhs, rg_batch** out)
         set_error(std::string("rg_batch_create: ") + cudaGetErrorString(e));
         return fail(RG_CUDA_ERROR);
     }
-    b->grid_spmv = b->grid_upd = grid_for(b->ntiles, 1, 8);
+    {
+        OnPrivate on(b);
+        rc = set_group(b, 4);
+        if (rc) return fail(rc);
+    }
+    b->grid_spmv = b->grid_upd = grid_for(b->nunits, 1, 8);
     *out = h;
     return RG_OK;
 }
@@ -1066,13 +1171,14 @@ int rg_batch_destroy(rg_batch* h)
     return RG_OK;
 }
 
-int rg_batch_info(const rg_batch* h, int64_t* rows, int64_t* tiles, int* grid_spmv, int* grid_update, int* chunk,
-                  double* iter_us)
+int rg_batch_info(const rg_batch* h, int64_t* rows, int64_t* tiles, int* group, int* grid_spmv, int* grid_update,
+                  int* chunk, double* iter_us)
 {
     RG_REQUIRE(h, "rg_batch_info: NULL batch");
     const Batch* b = &h->b;
     if (rows) *rows = b->rows;
     if (tiles) *tiles = b->ntiles;
+    if (group) *group = b->group;
     if (grid_spmv) *grid_spmv = b->grid_spmv;
     if (grid_update) *grid_update = b->grid_upd;
     if (chunk) *chunk = b->chunk;

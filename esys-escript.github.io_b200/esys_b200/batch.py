@@ -53,12 +53,12 @@ class BatchSolver:
 
     def info(self):
         rows, tiles = C.c_int64(), C.c_int64()
-        gs, gu, ch = C.c_int(), C.c_int(), C.c_int()
+        grp, gs, gu, ch = C.c_int(), C.c_int(), C.c_int(), C.c_int()
         us = C.c_double()
-        L.check(L.lib().rg_batch_info(self._h, C.byref(rows), C.byref(tiles), C.byref(gs), C.byref(gu),
-                                      C.byref(ch), C.byref(us)))
-        return {"rows": rows.value, "tiles": tiles.value, "grid_spmv": gs.value, "grid_update": gu.value,
-                "chunk": ch.value, "iter_us": us.value}
+        L.check(L.lib().rg_batch_info(self._h, C.byref(rows), C.byref(tiles), C.byref(grp), C.byref(gs),
+                                      C.byref(gu), C.byref(ch), C.byref(us)))
+        return {"rows": rows.value, "tiles": tiles.value, "group": grp.value, "grid_spmv": gs.value,
+                "grid_update": gu.value, "chunk": ch.value, "iter_us": us.value}
 
     def solve(self, rhs, x, tol=1e-8, iter_max=100000, inner_tolerance=1e-2, accept_failure=False):
         """Solves all systems; returns the list of rg_diag (system-major)."""

@@ -206,10 +206,11 @@ typedef struct rg_batch rg_batch;
 int rg_batch_create(rg_matrix* const* mats, int nsystems, int nrhs, rg_batch** out);
 int rg_batch_destroy(rg_batch* batch);
 int rg_batch_tune(rg_batch* batch);
-/* rows: padded batch rows; tiles: 256-row tiles; grids in CTAs; iter_us: measured time of
-   one iteration of all systems at the tuned grids */
-int rg_batch_info(const rg_batch* batch, int64_t* rows, int64_t* tiles, int* grid_spmv, int* grid_update,
-                  int* chunk, double* iter_us);
+/* rows: padded batch rows; tiles: 256-row tiles; group: tiles per work unit of the
+   iteration kernels; grids in CTAs; iter_us: measured time of one iteration of all systems
+   at the tuned configuration */
+int rg_batch_info(const rg_batch* batch, int64_t* rows, int64_t* tiles, int* group, int* grid_spmv,
+                  int* grid_update, int* chunk, double* iter_us);
 /* rhs[i], x[i]: device arrays of n_i * nrhs doubles for system i, right hand side k at
    offset k * n_i.  opts: tolerance, iter_max, inner_tolerance, accept_convergence_failure
    (NULL: defaults).  diag: nsystems * nrhs entries (system-major) or NULL. */
