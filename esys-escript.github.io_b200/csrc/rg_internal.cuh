@@ -186,7 +186,7 @@ inline int grid_for(int64_t work_items, int items_per_block, int blocks_per_sm =
 enum TimerKind {
     T_PATTERN = 0, T_ASSEMBLE, T_BOUNDARY, T_CONSTRAINT, T_SPMV, T_BALANCE, T_NORMS, T_RESIDUAL,
     T_PASO_SPMV, T_PASO_UPDATE1, T_PASO_UPDATE2, T_STD_SPMV, T_STD_UPDATE, T_F32_SPMV,
-    T_F32_UPDATE, T_VECTOR, T_BATCH_SPMV, T_BATCH_UPDATE, T_BATCH_OUTER, T_COUNT
+    T_F32_UPDATE, T_VECTOR, T_BATCH_SPMV, T_BATCH_UPDATE, T_BATCH_OUTER, T_WS_CONV, T_WS_WGRAD, T_WS_OPS, T_COUNT
 };
 void timer_begin(int kind);
 void timer_end(int kind);

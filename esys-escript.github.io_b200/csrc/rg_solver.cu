@@ -222,21 +222,48 @@ __global__ void __launch_bounds__(kThreads) k_residual(int64_t n, const int32_t*
     }
 }
 
-// one damped Jacobi sweep on the balanced system: y = x + omega D^-1 (bb - A x)
-__global__ void __launch_bounds__(kThreads) k_jacobi_sweep(int64_t n, const int32_t* __restrict__ ptr,
-                                                           const int32_t* __restrict__ idx,
-                                                           const double* __restrict__ val,
-                                                           const double* __restrict__ dinv,
-                                                           const double* __restrict__ x,
-                                                           const double* __restrict__ bb, double omega,
-                                                           double* __restrict__ y)
+// One step of Chebyshev smoothing with the Jacobi preconditioner on the balanced system
+// (the semi-iterative method for D^-1 A with eigenvalues in [a, b]):
+//   d = c_d d + c_r D^-1 (bb - A x),  y = x + d
+// (step 0: c_d = 0, c_r = 1/theta).  It damps the error components of D^-1 A in [a, b]
+// uniformly, the rough part of a guess that dominates its residual.
+__global__ void __launch_bounds__(kThreads) k_cheb_step(int64_t n, const int32_t* __restrict__ ptr,
+                                                        const int32_t* __restrict__ idx,
+                                                        const double* __restrict__ val,
+                                                        const double* __restrict__ dinv,
+                                                        const double* __restrict__ x,
+                                                        const double* __restrict__ bb, double c_d, double c_r,
+                                                        double* __restrict__ d, double* __restrict__ y)
 {
     RG_ROW_LOOP(n)
     {
         double acc = row < n ? csr_row_dot(ptr, idx, val, x, row, lane) : 0.0;
         acc = group_sum(acc);
-        if (row < n && lane == 0) y[row] = x[row] + omega * dinv[row] * (bb[row] - acc);
+        if (row < n && lane == 0) {
+            const double dn = c_d * (c_d != 0.0 ? d[row] : 0.0) + c_r * dinv[row] * (bb[row] - acc);
+            d[row] = dn;
+            y[row] = x[row] + dn;
+        }
     }
+}
+
+// Gershgorin bound of the spectrum of D^-1 A: max over rows of sum_j |a_ij| / a_ii
+__global__ void __launch_bounds__(kThreads) k_gershgorin(int64_t n, const int32_t* __restrict__ ptr,
+                                                         const double* __restrict__ val,
+                                                         const double* __restrict__ dinv, ReduceBuf rb,
+                                                         double* __restrict__ out)
+{
+    double v[1] = {0.0};
+    RG_ROW_LOOP(n)
+    {
+        double acc = 0.0;
+        if (row < n)
+            for (int32_t k = ptr[row] + lane; k < ptr[row + 1]; k += kLpr) acc += fabs(val[k]);
+        acc = group_sum(acc);
+        if (row < n && lane == 0) v[0] = fmax(v[0], acc * fabs(dinv[row]));
+    }
+    double t[1];
+    if (grid_reduce<1, 1u>(v, rb, t) && threadIdx.x == 0) *out = t[0];
 }
 
 __global__ void k_mul(int64_t n, const double* __restrict__ a, const double* __restrict__ b,
@@ -1437,18 +1464,36 @@ int solve_impl(Matrix* m, const double* rhs, double* x, const rg_solver_opts* o,
         } else if (o->initial_guess) {
             RG_TIMED(T_VECTOR, (k_div<<<eg, kThreads, 0, stream()>>>(n, o->initial_guess, m->bv, w->x)));
             RG_CHECK_LAUNCH();
-            // damped Jacobi sweeps remove the guess's rough error (which dominates its residual)
-            // and keep its smooth part, which is what PCG is slow to find
-            const Domain* dm = m->dom;
-            for (int k = 0; k < o->guess_sweeps; ++k) {
-                const double* src = (k & 1) ? w->x2 : w->x;
-                double* dst = (k & 1) ? w->x : w->x2;
-                RG_TIMED(T_VECTOR, (k_jacobi_sweep<<<w->grid_rows, kThreads, 0, stream()>>>(
-                                       n, dm->ptr, dm->idx, m->val, m->dinv, src, w->bb, 0.6, dst)));
+            // Chebyshev smoothing removes the guess's rough error (which dominates its residual)
+            // and keeps its smooth part, which is what PCG is slow to find: eigenvalues of
+            // D^-1 A in [lmax/30, lmax], lmax from Gershgorin
+            if (o->guess_sweeps > 0) {
+                const Domain* dm = m->dom;
+                RG_TIMED(T_NORMS, (k_gershgorin<<<w->grid_rows, kThreads, 0, stream()>>>(n, dm->ptr, m->val, m->dinv,
+                                                                                      rbuf(w), &w->s->tau_next)));
                 RG_CHECK_LAUNCH();
+                if ((rc = read_scal(w))) return rc;
+                const double lmax = w->hs->tau_next, lmin = lmax / 30.0;
+                const double theta = 0.5 * (lmax + lmin), delta = 0.5 * (lmax - lmin), sigma = theta / delta;
+                double rho = 1.0 / sigma;
+                for (int k = 0; k < o->guess_sweeps; ++k) {
+                    const double* src = (k & 1) ? w->x2 : w->x;
+                    double* dst = (k & 1) ? w->x : w->x2;
+                    double c_d = 0.0, c_r = 1.0 / theta;
+                    if (k > 0) {
+                        const double rho_n = 1.0 / (2.0 * sigma - rho);
+                        c_d = rho_n * rho;
+                        c_r = 2.0 * rho_n / delta;
+                        rho = rho_n;
+                    }
+                    RG_TIMED(T_VECTOR, (k_cheb_step<<<w->grid_rows, kThreads, 0, stream()>>>(
+                                           n, dm->ptr, dm->idx, m->val, m->dinv, src, w->bb, c_d, c_r, w->z, dst)));
+                    RG_CHECK_LAUNCH();
+                }
+                if (o->guess_sweeps & 1)
+                    RG_CHECK_CUDA(
+                        cudaMemcpyAsync(w->x, w->x2, sizeof(double) * n, cudaMemcpyDeviceToDevice, stream()));
             }
-            if (o->guess_sweeps > 0 && (o->guess_sweeps & 1))
-                RG_CHECK_CUDA(cudaMemcpyAsync(w->x, w->x2, sizeof(double) * n, cudaMemcpyDeviceToDevice, stream()));
             // a guess whose residual exceeds the right hand side's is worse than zero: drop it
             double r0;
             if ((rc = residual_l2(m, w->bb, w->x, false, &r0))) return rc;

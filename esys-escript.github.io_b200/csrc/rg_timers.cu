@@ -28,7 +28,7 @@ const char* kNames[T_COUNT] = {"pattern", "assemble", "assemble_boundary", "inse
                                "spmv", "balance", "norms", "residual", "paso_spmv",
                                "paso_update1", "paso_update2", "std_spmv", "std_update",
                                "f32_spmv", "f32_update", "vector", "batch_spmv", "batch_update",
-                               "batch_outer"};
+                               "batch_outer", "ws_conv", "ws_wgrad", "ws_ops"};
 
 cudaEvent_t get_event()
 {

@@ -420,7 +420,7 @@ int launch_conv3(ConvArgs& a, int ntiles)
                                            ConvSmem<COUT>::kBytes));
         attr = true;
     }
-    k_conv3<COUT><<<ntiles, kConvThreads, ConvSmem<COUT>::kBytes, stream()>>>(a);
+    RG_TIMED(T_WS_CONV, (k_conv3<COUT><<<ntiles, kConvThreads, ConvSmem<COUT>::kBytes, stream()>>>(a)));
     RG_CHECK_LAUNCH();
     return RG_OK;
 }
@@ -434,7 +434,7 @@ int launch_wgrad(WgradArgs& a, int grid)
                                            WgSmem<COUT>::kBytes));
         attr = true;
     }
-    k_wgrad<COUT><<<grid, kConvThreads, WgSmem<COUT>::kBytes, stream()>>>(a);
+    RG_TIMED(T_WS_WGRAD, (k_wgrad<COUT><<<grid, kConvThreads, WgSmem<COUT>::kBytes, stream()>>>(a)));
     RG_CHECK_LAUNCH();
     return RG_OK;
 }
@@ -556,8 +556,8 @@ extern "C" int rg_ws_conv3_wgrad(const rg_act* x, const rg_act* g, float* dw, fl
     }
     if (rc) return rc;
     const int total = 27 * cout * x->c;
-    ws::k_wgrad_reduce<<<(total + 255) / 256, 256, 0, stream()>>>(partials, dw, ksplit, a.mtiles, cout, x->c,
-                                                                 accumulate);
+    RG_TIMED(T_WS_WGRAD, (ws::k_wgrad_reduce<<<(total + 255) / 256, 256, 0, stream()>>>(partials, dw, ksplit, a.mtiles, cout, x->c,
+                                                                 accumulate)));
     RG_CHECK_LAUNCH();
     return RG_OK;
 }

@@ -456,7 +456,7 @@ int rg_ws_avgpool(const rg_act* in, rg_act* out)
     RG_REQUIRE(out->d * 2 == in->d && out->h * 2 == in->h && out->w * 2 == in->w && out->c == in->c && out->n == in->n,
                "rg_ws_avgpool: out must be in halved");
     const Act o = act(out);
-    k_avgpool<<<grid_elems(o.positions() * o.c), 256, 0, stream()>>>(act(in), o);
+    RG_TIMED(T_WS_OPS, (k_avgpool<<<grid_elems(o.positions() * o.c), 256, 0, stream()>>>(act(in), o)));
     RG_CHECK_LAUNCH();
     return RG_OK;
 }
@@ -470,7 +470,7 @@ int rg_ws_avgpool_bwd(const rg_act* dout, const rg_act* in, const rg_act* dskip,
     RG_REQUIRE(!dskip || (dskip->d == din->d && skip_off + din->c <= dskip->c), "rg_ws_avgpool_bwd: skip shape");
     const Act di = act(din);
     const Act ds = dskip ? act(dskip) : Act{nullptr, 0, 0, 0, 0, 0};
-    k_avgpool_bwd<<<grid_elems(di.positions() * di.c), 256, 0, stream()>>>(act(dout), act(in), ds, skip_off, di);
+    RG_TIMED(T_WS_OPS, (k_avgpool_bwd<<<grid_elems(di.positions() * di.c), 256, 0, stream()>>>(act(dout), act(in), ds, skip_off, di)));
     RG_CHECK_LAUNCH();
     return RG_OK;
 }
@@ -482,7 +482,7 @@ int rg_ws_upcat(const rg_act* a, const rg_act* b, rg_act* out)
     RG_ACT_OK(out, "rg_ws_upcat");
     RG_REQUIRE(a->d * 2 == out->d && b->d == out->d && out->c == a->c + b->c, "rg_ws_upcat: shape mismatch");
     const Act o = act(out);
-    k_upcat<<<grid_elems(o.positions() * o.c), 256, 0, stream()>>>(act(a), act(b), o);
+    RG_TIMED(T_WS_OPS, (k_upcat<<<grid_elems(o.positions() * o.c), 256, 0, stream()>>>(act(a), act(b), o)));
     RG_CHECK_LAUNCH();
     return RG_OK;
 }
@@ -498,7 +498,7 @@ int rg_ws_upcat_bwd(const rg_act* dcat, const rg_act* a, rg_act* da)
                "rg_ws_upcat_bwd: mask shape must equal da's");
     const Act d = act(da);
     const Act am = a ? act(a) : Act{nullptr, 0, 0, 0, 0, 0};
-    k_upcat_bwd<<<grid_elems(d.positions() * d.c), 256, 0, stream()>>>(act(dcat), am, d);
+    RG_TIMED(T_WS_OPS, (k_upcat_bwd<<<grid_elems(d.positions() * d.c), 256, 0, stream()>>>(act(dcat), am, d)));
     RG_CHECK_LAUNCH();
     return RG_OK;
 }
@@ -508,7 +508,7 @@ int rg_ws_head(const rg_act* x, const float* w, const float* b, float* out)
     RG_ACT_OK(x, "rg_ws_head");
     RG_REQUIRE(w && b && out, "rg_ws_head: NULL argument");
     const Act xa = act(x);
-    k_head<<<grid_elems(xa.positions()), 256, 0, stream()>>>(xa, w, b, out);
+    RG_TIMED(T_WS_OPS, (k_head<<<grid_elems(xa.positions()), 256, 0, stream()>>>(xa, w, b, out)));
     RG_CHECK_LAUNCH();
     return RG_OK;
 }
@@ -523,11 +523,11 @@ int rg_ws_colsum(const rg_act* v, const float* dout, float* out, float* work, in
     const int blocks = kNumSMs * 4, threads = 64;
     const size_t sm = sizeof(float) * threads * v->c;
     if (dout)
-        k_colsum<true><<<blocks, threads, sm, stream()>>>(va, dout, work, v->c);
+        RG_TIMED(T_WS_OPS, (k_colsum<true><<<blocks, threads, sm, stream()>>>(va, dout, work, v->c)));
     else
-        k_colsum<false><<<blocks, threads, sm, stream()>>>(va, nullptr, work, v->c);
+        RG_TIMED(T_WS_OPS, (k_colsum<false><<<blocks, threads, sm, stream()>>>(va, nullptr, work, v->c)));
     RG_CHECK_LAUNCH();
-    k_colsum_finish<<<1, 128, 0, stream()>>>(work, blocks, v->c, out, accumulate);
+    RG_TIMED(T_WS_OPS, (k_colsum_finish<<<1, 128, 0, stream()>>>(work, blocks, v->c, out, accumulate)));
     RG_CHECK_LAUNCH();
     return RG_OK;
 }
@@ -538,7 +538,7 @@ int rg_ws_head_bwd_x(const rg_act* x, const float* w, const float* dout, rg_act*
     RG_ACT_OK(dx, "rg_ws_head_bwd_x");
     RG_REQUIRE(w && dout && dx->c == x->c, "rg_ws_head_bwd_x: invalid argument");
     const Act xa = act(x);
-    k_head_bwd_x<<<grid_elems(xa.positions() * xa.c), 256, 0, stream()>>>(xa, w, dout, act(dx));
+    RG_TIMED(T_WS_OPS, (k_head_bwd_x<<<grid_elems(xa.positions() * xa.c), 256, 0, stream()>>>(xa, w, dout, act(dx))));
     RG_CHECK_LAUNCH();
     return RG_OK;
 }
@@ -550,9 +550,9 @@ int rg_ws_mse(const float* out, const float* target, int64_t count, float* dout,
 {
     RG_REQUIRE(out && target && dout && loss_dev && work && count > 0, "rg_ws_mse: invalid argument");
     const int blocks = kNumSMs * 4;
-    k_mse<<<blocks, 256, 0, stream()>>>(out, target, (size_t)count, dout, work);
+    RG_TIMED(T_WS_OPS, (k_mse<<<blocks, 256, 0, stream()>>>(out, target, (size_t)count, dout, work)));
     RG_CHECK_LAUNCH();
-    k_mse_finish<<<1, 32, 0, stream()>>>(work, blocks, (size_t)count, loss_dev, dsum_dev);
+    RG_TIMED(T_WS_OPS, (k_mse_finish<<<1, 32, 0, stream()>>>(work, blocks, (size_t)count, loss_dev, dsum_dev)));
     RG_CHECK_LAUNCH();
     return RG_OK;
 }
@@ -564,9 +564,9 @@ int rg_ws_h1_loss(const float* out, const float* target, int n, int d, int h, in
                "rg_ws_h1_loss: invalid argument");
     const int blocks = kNumSMs * 4;
     const size_t count = (size_t)n * d * h * w;
-    k_h1_loss<<<blocks, 256, 0, stream()>>>(out, target, n, d, h, w, lambda, dout, work);
+    RG_TIMED(T_WS_OPS, (k_h1_loss<<<blocks, 256, 0, stream()>>>(out, target, n, d, h, w, lambda, dout, work)));
     RG_CHECK_LAUNCH();
-    k_mse_finish<<<1, 32, 0, stream()>>>(work, blocks, count, loss_dev, dsum_dev);
+    RG_TIMED(T_WS_OPS, (k_mse_finish<<<1, 32, 0, stream()>>>(work, blocks, count, loss_dev, dsum_dev)));
     RG_CHECK_LAUNCH();
     return RG_OK;
 }
@@ -576,7 +576,7 @@ int rg_ws_adam(float* w, const float* g, float* m, float* v, int64_t count, floa
 {
     RG_REQUIRE(w && g && m && v && count > 0 && step > 0, "rg_ws_adam: invalid argument");
     const float c1 = 1.f - powf(beta1, (float)step), c2 = 1.f - powf(beta2, (float)step);
-    k_adam<<<grid_elems((size_t)count), 256, 0, stream()>>>(w, g, m, v, (size_t)count, lr, beta1, beta2, eps, c1, c2);
+    RG_TIMED(T_WS_OPS, (k_adam<<<grid_elems((size_t)count), 256, 0, stream()>>>(w, g, m, v, (size_t)count, lr, beta1, beta2, eps, c1, c2)));
     RG_CHECK_LAUNCH();
     return RG_OK;
 }
@@ -584,8 +584,8 @@ int rg_ws_adam(float* w, const float* g, float* m, float* v, int64_t count, floa
 int rg_ws_weights_bf16(const float* w, void* w_fwd, void* w_dgrad, int cout, int cin)
 {
     RG_REQUIRE(w && (w_fwd || w_dgrad) && cout > 0 && cin > 0, "rg_ws_weights_bf16: invalid argument");
-    k_weights_bf16<<<grid_elems((size_t)27 * cout * cin), 256, 0, stream()>>>(
-        w, static_cast<__nv_bfloat16*>(w_fwd), static_cast<__nv_bfloat16*>(w_dgrad), cout, cin);
+    RG_TIMED(T_WS_OPS, (k_weights_bf16<<<grid_elems((size_t)27 * cout * cin), 256, 0, stream()>>>(
+        w, static_cast<__nv_bfloat16*>(w_fwd), static_cast<__nv_bfloat16*>(w_dgrad), cout, cin)));
     RG_CHECK_LAUNCH();
     return RG_OK;
 }
@@ -597,10 +597,10 @@ int rg_ws_field_stats(const float* kappa, const float* y, int nsamples, int64_t 
 {
     RG_REQUIRE(kappa && y && stats && work && nsamples > 0 && per_sample > 0 && h_net > 0,
                "rg_ws_field_stats: invalid argument");
-    k_field_stats<<<dim3(kStatBlocks, nsamples), 256, 0, stream()>>>(kappa, y, (size_t)per_sample, work);
+    RG_TIMED(T_WS_OPS, (k_field_stats<<<dim3(kStatBlocks, nsamples), 256, 0, stream()>>>(kappa, y, (size_t)per_sample, work)));
     RG_CHECK_LAUNCH();
-    k_field_stats_finish<<<(nsamples + 63) / 64, 64, 0, stream()>>>(work, kStatBlocks, (size_t)per_sample, nsamples,
-                                                                     h_net, stats);
+    RG_TIMED(T_WS_OPS, (k_field_stats_finish<<<(nsamples + 63) / 64, 64, 0, stream()>>>(work, kStatBlocks, (size_t)per_sample, nsamples,
+                                                                     h_net, stats)));
     RG_CHECK_LAUNCH();
     return RG_OK;
 }
@@ -610,7 +610,7 @@ int rg_ws_pack_input(const float* kappa, const float* y, int factor, rg_act* x, 
     RG_ACT_OK(x, "rg_ws_pack_input");
     RG_REQUIRE(kappa && y && stats && x->c >= 5 && factor >= 1, "rg_ws_pack_input: invalid argument");
     const Act xa = act(x);
-    k_pack_input<<<grid_elems(xa.positions()), 256, 0, stream()>>>(kappa, y, factor, xa, stats);
+    RG_TIMED(T_WS_OPS, (k_pack_input<<<grid_elems(xa.positions()), 256, 0, stream()>>>(kappa, y, factor, xa, stats)));
     RG_CHECK_LAUNCH();
     return RG_OK;
 }
@@ -620,8 +620,8 @@ int rg_ws_nodes_to_cells(const double* u, int factor, int nsamples, int d, int h
 {
     RG_REQUIRE(u && stats && target && factor >= 1 && nsamples > 0 && d > 0 && h > 0 && w > 0,
                "rg_ws_nodes_to_cells: invalid argument");
-    k_nodes_to_cells<<<grid_elems((size_t)nsamples * d * h * w), 256, 0, stream()>>>(u, factor, nsamples, d, h, w,
-                                                                                   stats, target);
+    RG_TIMED(T_WS_OPS, (k_nodes_to_cells<<<grid_elems((size_t)nsamples * d * h * w), 256, 0, stream()>>>(u, factor, nsamples, d, h, w,
+                                                                                   stats, target)));
     RG_CHECK_LAUNCH();
     return RG_OK;
 }
@@ -631,8 +631,8 @@ int rg_ws_cells_to_nodes(const float* cells, int nsamples, int d, int h, int w, 
 {
     RG_REQUIRE(cells && stats && u && nsamples > 0 && d > 0 && h > 0 && w > 0 && nd > 1 && nh > 1 && nw > 1,
                "rg_ws_cells_to_nodes: invalid argument");
-    k_cells_to_nodes<<<grid_elems((size_t)nsamples * nd * nh * nw), 256, 0, stream()>>>(cells, nsamples, d, h, w,
-                                                                                      stats, nd, nh, nw, q, u);
+    RG_TIMED(T_WS_OPS, (k_cells_to_nodes<<<grid_elems((size_t)nsamples * nd * nh * nw), 256, 0, stream()>>>(cells, nsamples, d, h, w,
+                                                                                      stats, nd, nh, nw, q, u)));
     RG_CHECK_LAUNCH();
     return RG_OK;
 }

@@ -166,8 +166,9 @@ typedef struct {
                                    between FP64 residual replacements (default 1e-2)      */
     const double* initial_guess;/* STANDARD mode only: device x0 (unbalanced units) or NULL;
                                    dropped for zero when ||B(b - A x0)|| > ||B b||          */
-    int guess_sweeps;           /* damped Jacobi sweeps (omega 0.6) applied to initial_guess
-                                   before that test; default 0                            */
+    int guess_sweeps;           /* Chebyshev smoothing steps (Jacobi-preconditioned, on the
+                                   upper 29/30 of the Gershgorin range) applied to
+                                   initial_guess before that test; default 0               */
 } rg_solver_opts;
 
 typedef struct {
