@@ -104,3 +104,39 @@ def make_batch(nsys, nrhs, edges=(32, 48, 64, 80, 96), corr_cells=8.0, width_cel
         systems.append(prob)
         rhs.append(b)
     return systems, rhs
+
+
+def main(argv=None):
+    """python -m esys_b200.batch [--systems 64] [--nrhs 8] [--seed 0] [--tol 1e-8]: builds a
+    seeded batch (make_batch), tunes, solves it twice and prints one JSON line."""
+    import argparse
+    import json
+    import time
+    ap = argparse.ArgumentParser(description="batched Brick solves")
+    ap.add_argument("--systems", type=int, default=64)
+    ap.add_argument("--nrhs", type=int, default=8)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--tol", type=float, default=1e-8)
+    a = ap.parse_args(argv)
+    torch.cuda.set_device(0)
+    t0 = time.time()
+    systems, rhs = make_batch(a.systems, a.nrhs, seed=a.seed)
+    xs = [torch.zeros_like(b) for b in rhs]
+    with BatchSolver([s.mat for s in systems], a.nrhs) as bs:
+        info = bs.tune()
+        bs.solve(rhs, xs, tol=a.tol)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        d = bs.solve(rhs, xs, tol=a.tol)
+        e1.record()
+        torch.cuda.synchronize()
+    its = [x.num_iter for x in d]
+    print(json.dumps({"systems": a.systems, "nrhs": a.nrhs, "ms": e0.elapsed_time(e1),
+                      "setup_s": time.time() - t0, "all_converged": all(x.converged for x in d),
+                      "iterations": [min(its), float(np.mean(its)), max(its)], **info}))
+    for s in systems:
+        s.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -183,8 +183,16 @@ def main(argv=None):
     ap.add_argument("--gen-time-limit", type=float, default=None)
     ap.add_argument("--train-time-limit", type=float, default=None)
     ap.add_argument("--out", default=W.WEIGHTS_FILE)
+    ap.add_argument("--evaluate", metavar="WEIGHTS", default=None,
+                    help="only evaluate trained weights: A/B against the zero guess at 64^3 and 128^3")
     a = ap.parse_args(argv)
     torch.cuda.set_device(0)
+    if a.evaluate:
+        net = W.UNet.load(a.evaluate)
+        for ne, npb in ((64, 6), (128, 3)):
+            agg, _ = evaluate(net, ne, npb, 99 + ne, log=None, sweeps=(0, 4, 8, 16))
+            print(json.dumps({"ne": ne, **agg}), flush=True)
+        return
     xs, ts, info = generate(a.samples, a.rhs_per_kappa, a.seed, time_limit=a.gen_time_limit)
     print(json.dumps({"data": info}), flush=True)
     net = W.UNet(seed=a.seed)
