@@ -15,6 +15,27 @@
 
 namespace rg {
 
+// the 1-point rule of assemblePDESingleReduced (DefaultAssembler3D.cpp:2891-3271,
+// DefaultAssembler2D.cpp:842-1010): element centre, weight = element volume; N = 2^-dim,
+// dN_k/dx_d = +-(1/dx_d) 2^-(dim-1)
+void build_q1_reduced_tables(int dim, const double dx[3], Q1Tables* t)
+{
+    build_q1_tables(dim, dx, t);  // face weights and zeroed tables
+    double vol = 1.0;
+    for (int d = 0; d < dim; ++d) vol *= dx[d];
+    t->W = vol;
+    const int nk = 1 << dim;
+    for (int k = 0; k < nk; ++k) {
+        t->N[0][k] = 1.0 / nk;
+        for (int d = 0; d < dim; ++d) {
+            double g = (((k >> d) & 1) ? 1.0 : -1.0) / dx[d];
+            for (int e = 0; e < dim; ++e)
+                if (e != d) g *= 0.5;
+            t->G[0][k][d] = g;
+        }
+    }
+}
+
 void build_q1_tables(int dim, const double dx[3], Q1Tables* t)
 {
     const double g[2] = {0.5 - std::sqrt(3.0) / 6.0, 0.5 + std::sqrt(3.0) / 6.0};
@@ -146,11 +167,11 @@ __device__ __forceinline__ const double* coef_ptr(const CoefArg& c, int64_t e, i
 // Row R of the element matrix and vector of element e:
 //   em[c] = sum_q W (A_ij G_Ri G_cj + B_i G_Ri N_c + C_j N_R G_cj + D N_R N_c)
 //   f     = sum_q W (X_i G_Ri + Y N_R)
-template <int DIM, int R>
+template <int DIM, int NQ, int R>
 __device__ __forceinline__ void element_row(const AsmArgs& a, int64_t e, double (&em)[1 << DIM],
                                             double& f)
 {
-    constexpr int NK = 1 << DIM, NQ = 1 << DIM, D2 = DIM * DIM;
+    constexpr int NK = 1 << DIM, D2 = DIM * DIM;
     const CoefArg& A = a.c[0];
     const CoefArg& B = a.c[1];
     const CoefArg& C = a.c[2];
@@ -212,7 +233,7 @@ __host__ __device__ constexpr int band_of(int sx, int sy, int sz, int c)
                     : (sx + (c & 1)) + 3 * (sy + ((c >> 1) & 1));
 }
 
-template <int DIM, int SX, int SY, int SZ>
+template <int DIM, int NQ, int SX, int SY, int SZ>
 __device__ __forceinline__ void add_element(const AsmArgs& a, int64_t x, int64_t y, int64_t z,
                                             double (&acc)[DIM == 3 ? 27 : 9], double& facc)
 {
@@ -223,13 +244,15 @@ __device__ __forceinline__ void add_element(const AsmArgs& a, int64_t x, int64_t
     const int64_t e = ex + a.NE0 * ey + (DIM == 3 ? a.NE0 * a.NE1 * ez : 0);
     constexpr int R = (1 - SX) + 2 * (1 - SY) + (DIM == 3 ? 4 * (1 - SZ) : 0);
     double em[NK], f;
-    element_row<DIM, R>(a, e, em, f);
+    element_row<DIM, NQ, R>(a, e, em, f);
 #pragma unroll
     for (int c = 0; c < NK; ++c) acc[band_of<DIM>(SX, SY, SZ, c)] += em[c];
     facc += f;
 }
 
-template <int DIM>
+// NQ = 2^DIM Gauss points (assemblePDESingle) or 1, the element centre
+// (assemblePDESingleReduced); the tables in `a.t` hold the matching rule
+template <int DIM, int NQ>
 __global__ void __launch_bounds__(kRowsPerCta) k_assemble(const __grid_constant__ AsmArgs a)
 {
     constexpr int NB = DIM == 3 ? 27 : 9;
@@ -246,15 +269,15 @@ __global__ void __launch_bounds__(kRowsPerCta) k_assemble(const __grid_constant_
         x = i % a.NN0;
         y = (i / a.NN0) % a.NN1;
         z = DIM == 3 ? i / (a.NN0 * a.NN1) : 0;
-        add_element<DIM, 0, 0, 0>(a, x, y, z, acc, facc);
-        add_element<DIM, 1, 0, 0>(a, x, y, z, acc, facc);
-        add_element<DIM, 0, 1, 0>(a, x, y, z, acc, facc);
-        add_element<DIM, 1, 1, 0>(a, x, y, z, acc, facc);
+        add_element<DIM, NQ, 0, 0, 0>(a, x, y, z, acc, facc);
+        add_element<DIM, NQ, 1, 0, 0>(a, x, y, z, acc, facc);
+        add_element<DIM, NQ, 0, 1, 0>(a, x, y, z, acc, facc);
+        add_element<DIM, NQ, 1, 1, 0>(a, x, y, z, acc, facc);
         if (DIM == 3) {
-            add_element<DIM, 0, 0, 1>(a, x, y, z, acc, facc);
-            add_element<DIM, 1, 0, 1>(a, x, y, z, acc, facc);
-            add_element<DIM, 0, 1, 1>(a, x, y, z, acc, facc);
-            add_element<DIM, 1, 1, 1>(a, x, y, z, acc, facc);
+            add_element<DIM, NQ, 0, 0, 1>(a, x, y, z, acc, facc);
+            add_element<DIM, NQ, 1, 0, 1>(a, x, y, z, acc, facc);
+            add_element<DIM, NQ, 0, 1, 1>(a, x, y, z, acc, facc);
+            add_element<DIM, NQ, 1, 1, 1>(a, x, y, z, acc, facc);
         }
         if (a.rhs) a.rhs[i] += facc;
     }
@@ -430,7 +453,7 @@ int launch_pattern(Domain* d)
     return RG_OK;
 }
 
-int assemble_single_impl(const Domain* d, double* val, double* rhs, const rg_coef* c[6])
+int assemble_single_impl(const Domain* d, double* val, double* rhs, const rg_coef* c[6], bool reduced)
 {
     AsmArgs a;
     bool addS = false, addF = false;
@@ -439,7 +462,7 @@ int assemble_single_impl(const Domain* d, double* val, double* rhs, const rg_coe
         a.c[j].kind = (c[j] && c[j]->ptr) ? c[j]->kind : RG_COEF_EMPTY;
         if (a.c[j].kind) (j < 4 ? addS : addF) = true;
     }
-    a.t = d->q1;
+    a.t = reduced ? d->q1r : d->q1;
     a.NE0 = d->ne[0];
     a.NE1 = d->ne[1];
     a.NE2 = d->ne[2];
@@ -452,10 +475,14 @@ int assemble_single_impl(const Domain* d, double* val, double* rhs, const rg_coe
     a.rhs = addF ? rhs : nullptr;
     if (!a.val && !a.rhs) return RG_OK;
     const int grid = (int)((d->n + kRowsPerCta - 1) / kRowsPerCta);
-    if (d->dim == 3)
-        RG_TIMED(T_ASSEMBLE, (k_assemble<3><<<grid, kRowsPerCta, 0, stream()>>>(a)));
+    if (d->dim == 3 && !reduced)
+        RG_TIMED(T_ASSEMBLE, (k_assemble<3, 8><<<grid, kRowsPerCta, 0, stream()>>>(a)));
+    else if (d->dim == 3)
+        RG_TIMED(T_ASSEMBLE, (k_assemble<3, 1><<<grid, kRowsPerCta, 0, stream()>>>(a)));
+    else if (!reduced)
+        RG_TIMED(T_ASSEMBLE, (k_assemble<2, 4><<<grid, kRowsPerCta, 0, stream()>>>(a)));
     else
-        RG_TIMED(T_ASSEMBLE, (k_assemble<2><<<grid, kRowsPerCta, 0, stream()>>>(a)));
+        RG_TIMED(T_ASSEMBLE, (k_assemble<2, 1><<<grid, kRowsPerCta, 0, stream()>>>(a)));
     RG_CHECK_LAUNCH();
     return RG_OK;
 }

@@ -144,6 +144,7 @@ int rg_domain_create(int dim, const int64_t ne[3], const double x0[3], const dou
         d.band_off[b] = bx + d.nn[0] * by + d.nn[0] * d.nn[1] * bz;
     }
     build_q1_tables(dim, d.dx, &d.q1);
+    build_q1_reduced_tables(dim, d.dx, &d.q1r);
     cudaError_t e1 = cudaMalloc((void**)&d.ptr, sizeof(int32_t) * (n + 1));
     cudaError_t e2 = e1 == cudaSuccess ? cudaMalloc((void**)&d.idx, sizeof(int32_t) * nnz) : e1;
     if (e2 != cudaSuccess) {
@@ -296,7 +297,22 @@ int rg_assemble_single(rg_matrix* mat, double* rhs, const rg_coef* A, const rg_c
         if (rc) return rc;
         mat->m.solver_ready = false;
     }
-    return assemble_single_impl(mat->m.dom, mat->m.val, rhs, c);
+    return assemble_single_impl(mat->m.dom, mat->m.val, rhs, c, false);
+}
+
+int rg_assemble_single_reduced(rg_matrix* mat, double* rhs, const rg_coef* A, const rg_coef* B,
+                               const rg_coef* C, const rg_coef* D, const rg_coef* X, const rg_coef* Y)
+{
+    RG_REQUIRE(mat, "rg_assemble_single_reduced: a matrix handle is required (it names the domain)");
+    const rg_coef* c[6] = {A, B, C, D, X, Y};
+    for (int j = 0; j < 6; ++j) RG_REQUIRE(coef_ok(c[j]), "rg_assemble_single_reduced: invalid coefficient");
+    const bool addS = (A && A->kind) || (B && B->kind) || (C && C->kind) || (D && D->kind);
+    if (addS) {
+        int rc = require_unbalanced(&mat->m, "rg_assemble_single_reduced");
+        if (rc) return rc;
+        mat->m.solver_ready = false;
+    }
+    return assemble_single_impl(mat->m.dom, mat->m.val, rhs, c, true);
 }
 
 int rg_assemble_boundary(rg_matrix* mat, double* rhs, const rg_coef* d, const rg_coef* y)

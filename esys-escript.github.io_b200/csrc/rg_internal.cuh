@@ -49,6 +49,7 @@ struct Q1Tables {
     double Wf[3];  // face quadrature weight for faces normal to axis d
 };
 void build_q1_tables(int dim, const double dx[3], Q1Tables* t);
+void build_q1_reduced_tables(int dim, const double dx[3], Q1Tables* t);
 
 // ---------------------------------------------------------------- handles
 struct Domain {
@@ -62,6 +63,7 @@ struct Domain {
     int64_t npad;            // band stride: n rounded up to a multiple of 256
     int64_t band_off[27];    // column offset of band b: dx + NN0*dy + NN0*NN1*dz
     Q1Tables q1;
+    Q1Tables q1r;            // 1-point rule of the reduced-order assembly
 };
 
 struct Workspace;        // solver vectors, allocated lazily (rg_solver.cu)
@@ -204,7 +206,7 @@ void timers_add(const long long delta[T_COUNT], long long times);
 
 // ---------------------------------------------------------------- entry points between units
 int launch_pattern(Domain* d);
-int assemble_single_impl(const Domain* d, double* val, double* rhs, const rg_coef* c[6]);
+int assemble_single_impl(const Domain* d, double* val, double* rhs, const rg_coef* c[6], bool reduced);
 int assemble_boundary_impl(const Domain* d, double* val, double* rhs, const rg_coef* dc,
                            const rg_coef* yc);
 int launch_interpolate(const Domain* d, const double* nodal, int ncomp, double* out, int reduced);

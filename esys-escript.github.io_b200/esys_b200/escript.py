@@ -802,10 +802,10 @@ def _tensor_from_ptr(ptr, count, dtype):
 # ---------------------------------------------------------------------------------------------
 
 _INTERIOR = ("A", "B", "C", "D", "X", "Y")
+_REDUCED = ("A_reduced", "B_reduced", "C_reduced", "D_reduced", "X_reduced", "Y_reduced")
 _BOUNDARY = ("d", "y")
 _CONSTRAINT = ("q", "r")
-_UNSUPPORTED = ("A_reduced", "B_reduced", "C_reduced", "D_reduced", "X_reduced", "Y_reduced",
-                "d_reduced", "y_reduced", "d_contact", "y_contact", "d_contact_reduced",
+_UNSUPPORTED = ("d_reduced", "y_reduced", "d_contact", "y_contact", "d_contact_reduced",
                 "y_contact_reduced", "d_dirac", "y_dirac")
 
 
@@ -867,6 +867,8 @@ class LinearPDE:
     def getFunctionSpaceForCoefficient(self, name):
         if name in _INTERIOR:
             return Function(self._domain)
+        if name in _REDUCED:
+            return ReducedFunction(self._domain)
         if name in _BOUNDARY:
             return FunctionOnBoundary(self._domain)
         if name in _CONSTRAINT:
@@ -876,7 +878,7 @@ class LinearPDE:
     def _shape_of(self, name):
         d = self.getDim()
         return {"A": (d, d), "B": (d,), "C": (d,), "D": (), "X": (d,), "Y": (), "d": (),
-                "y": (), "q": (), "r": ()}[name]
+                "y": (), "q": (), "r": ()}[name[:-len("_reduced")] if name.endswith("_reduced") else name]
 
     def createSolution(self):
         return Scalar(0.0, Solution(self._domain), expanded=True)
@@ -887,7 +889,7 @@ class LinearPDE:
     def getCoefficient(self, name):
         if name in self._coef:
             return self._coef[name]
-        if name in _INTERIOR + _BOUNDARY + _CONSTRAINT + _UNSUPPORTED:
+        if name in _INTERIOR + _REDUCED + _BOUNDARY + _CONSTRAINT + _UNSUPPORTED:
             return Data()
         raise ValueError(f"unknown coefficient {name}")
 
@@ -898,7 +900,7 @@ class LinearPDE:
                 if value is None or (isinstance(value, Data) and value.isEmpty()):
                     continue
                 raise NotImplementedError(f"coefficient {name} is not part of the GPU path")
-            if name not in _INTERIOR + _BOUNDARY + _CONSTRAINT:
+            if name not in _INTERIOR + _REDUCED + _BOUNDARY + _CONSTRAINT:
                 raise ValueError(f"illegal coefficient {name} requested for general PDE.")
             if value is None or (isinstance(value, Data) and value.isEmpty()):
                 self._coef.pop(name, None)
@@ -916,9 +918,9 @@ class LinearPDE:
                         raise ValueError(f"coefficient {name}: expected shape {shape}")
                     dat = Data(a, shape, fs)
                 self._coef[name] = dat
-            if name in ("A", "B", "C", "D", "d"):
+            if name in ("A", "B", "C", "D", "d", "A_reduced", "B_reduced", "C_reduced", "D_reduced"):
                 self._operator_valid = False
-            if name in ("X", "Y", "y", "r"):
+            if name in ("X", "Y", "y", "r", "X_reduced", "Y_reduced"):
                 self._rhs_valid = False
             if name == "q":
                 self._operator_valid = False
@@ -948,6 +950,11 @@ class LinearPDE:
             cs = [self._coef_c(n, keep) for n in _INTERIOR]
             L.check(lib.rg_assemble_single(self._operator._handle, C.c_void_p(self._rhs._t.data_ptr()),
                                            *[C.byref(c) for c in cs]))
+            if any(n in self._coef for n in _REDUCED):
+                cr = [self._coef_c(n, keep) for n in _REDUCED]
+                L.check(lib.rg_assemble_single_reduced(self._operator._handle,
+                                                       C.c_void_p(self._rhs._t.data_ptr()),
+                                                       *[C.byref(c) for c in cr]))
             bd = [self._coef_c(n, keep) for n in _BOUNDARY]
             L.check(lib.rg_assemble_boundary(self._operator._handle, C.c_void_p(self._rhs._t.data_ptr()),
                                              C.byref(bd[0]), C.byref(bd[1])))
@@ -959,6 +966,11 @@ class LinearPDE:
             cs = [empty, empty, empty, empty, self._coef_c("X", keep), self._coef_c("Y", keep)]
             L.check(lib.rg_assemble_single(self._operator._handle, C.c_void_p(self._rhs._t.data_ptr()),
                                            *[C.byref(c) for c in cs]))
+            if "X_reduced" in self._coef or "Y_reduced" in self._coef:
+                cr = [empty, empty, empty, empty, self._coef_c("X_reduced", keep), self._coef_c("Y_reduced", keep)]
+                L.check(lib.rg_assemble_single_reduced(self._operator._handle,
+                                                       C.c_void_p(self._rhs._t.data_ptr()),
+                                                       *[C.byref(c) for c in cr]))
             yc = self._coef_c("y", keep)
             L.check(lib.rg_assemble_boundary(self._operator._handle, C.c_void_p(self._rhs._t.data_ptr()),
                                              C.byref(empty), C.byref(yc)))

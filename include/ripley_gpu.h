@@ -100,6 +100,12 @@ int rg_matrix_balance_vector(rg_matrix* mat, const double** bv);
    or RG_COEF_EMPTY. */
 int rg_assemble_single(rg_matrix* mat, double* rhs, const rg_coef* A, const rg_coef* B,
                        const rg_coef* C, const rg_coef* D, const rg_coef* X, const rg_coef* Y);
+/* assemblePDESingleReduced (ripley/src/DefaultAssembler3D.cpp:2891-3271,
+   DefaultAssembler2D.cpp:842-1010): the same terms for coefficients on ReducedFunction
+   (A_reduced ... Y_reduced), integrated with the 1-point rule at the element centre.
+   Coefficients are CONSTANT, or EXPANDED / PER_ELEMENT with one value set per element. */
+int rg_assemble_single_reduced(rg_matrix* mat, double* rhs, const rg_coef* A, const rg_coef* B,
+                               const rg_coef* C, const rg_coef* D, const rg_coef* X, const rg_coef* Y);
 /* assemblePDEBoundarySingle: adds the face terms d (matrix) and y (rhs).  d/y are on
    FunctionOnBoundary: faces left,right,bottom,top(,front,back), face elements lower
    in-face axis fastest, 2^(dim-1) Gauss points per face element. */

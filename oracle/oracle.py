@@ -127,9 +127,11 @@ def pattern(dim: int, ne) -> Pattern:
 
 
 def assemble(dim, ne, dx, pat: Pattern, A=None, B=None, C_=None, D=None, X=None, Y=None,
-             use_ref=False):
+             use_ref=False, reduced=False):
     """Interior assembly.  Coefficients are (kind, array) pairs or None.  Returns
-    (val, rhs).  ``use_ref`` runs the reference's own DefaultAssembler source."""
+    (val, rhs).  ``use_ref`` runs the reference's own DefaultAssembler source; ``reduced``
+    selects the reduced-order (1-point) assembly of coefficients on ReducedFunction, whose
+    expanded data has one value set per element."""
     val = np.zeros(pat.nnz)
     rhs = np.zeros(pat.n)
     coefs = [_coef(c) for c in (A, B, C_, D, X, Y)]
@@ -139,13 +141,13 @@ def assemble(dim, ne, dx, pat: Pattern, A=None, B=None, C_=None, D=None, X=None,
         ptrs = (C.POINTER(C.c_double) * 6)(*[c[0].p for c in coefs])
         if any(k == PER_ELEMENT for k in kinds):
             raise ValueError("the reference assembler takes constant or expanded data")
-        rc = R.ref_assemble(dim, _i64x3(ne), _dx3(dx), _ip(pat.ptr), _ip(pat.idx), _dp(val),
-                            _dp(rhs), kinds, ptrs)
+        fn = R.ref_assemble_reduced if reduced else R.ref_assemble
+        rc = fn(dim, _i64x3(ne), _dx3(dx), _ip(pat.ptr), _ip(pat.idx), _dp(val), _dp(rhs), kinds, ptrs)
         if rc:
             raise RuntimeError(R.ref_last_error().decode())
     else:
-        lib().ro_assemble_single(dim, _i64x3(ne), _dx3(dx), _ip(pat.ptr), _ip(pat.idx), _dp(val),
-                                 _dp(rhs), *[c[0] for c in coefs])
+        fn = lib().ro_assemble_single_reduced if reduced else lib().ro_assemble_single
+        fn(dim, _i64x3(ne), _dx3(dx), _ip(pat.ptr), _ip(pat.idx), _dp(val), _dp(rhs), *[c[0] for c in coefs])
     return val, rhs
 
 

@@ -1,5 +1,5 @@
 // Driver that links the reference's own hot-path sources, compiled in place from
-// the esys-escript tree by oracle/build_ref.sh, into oracle/_ref/libripley_ref.so:
+// the esys-escript tree by oracle/Makefile (target ref), into oracle/_ref/libripley_ref.so:
 //
 //   ripley/src/DefaultAssembler2D.cpp, ripley/src/DefaultAssembler3D.cpp
 //   paso/src/Solver.cpp, paso/src/PCG.cpp, paso/src/SparseMatrix_MatrixVector.cpp
@@ -237,6 +237,40 @@ int ref_assemble(int dim, const int64_t ne[3], const double dx[3], const int32_t
         } else {
             ripley::DefaultAssembler2D<double> a(&g.dom, g.dx, g.NE, g.NN);
             a.assemblePDESingle(val ? &S : nullptr, rhsD, A, B, C, D, X, Y);
+        }
+    } catch (const std::exception& e) {
+        snprintf(g_err, sizeof(g_err), "%s", e.what());
+        return 1;
+    }
+    return 0;
+}
+
+// the reduced-order interior terms (coefficients on ReducedFunction: one data point per
+// element), DefaultAssembler{2,3}D::assemblePDESingleReduced
+int ref_assemble_reduced(int dim, const int64_t ne[3], const double dx[3], const int32_t* ptr,
+                         const int32_t* idx, double* val, double* rhs, const int* kinds,
+                         const double* const* coefs)
+{
+    try {
+        Geometry g;
+        make_geometry(g, dim, ne, dx);
+        escript::AbstractSystemMatrix S;
+        S.ptr = ptr;
+        S.idx = idx;
+        S.val = val;
+        escript::Data rhsD(rhs, 1, 1, true);
+        escript::Data A = make_coef(coefs[0], kinds[0], dim * dim, 1);
+        escript::Data B = make_coef(coefs[1], kinds[1], dim, 1);
+        escript::Data C = make_coef(coefs[2], kinds[2], dim, 1);
+        escript::Data D = make_coef(coefs[3], kinds[3], 1, 1);
+        escript::Data X = make_coef(coefs[4], kinds[4], dim, 1);
+        escript::Data Y = make_coef(coefs[5], kinds[5], 1, 1);
+        if (dim == 3) {
+            ripley::DefaultAssembler3D<double> a(&g.dom, g.dx, g.NE, g.NN);
+            a.assemblePDESingleReduced(val ? &S : nullptr, rhsD, A, B, C, D, X, Y);
+        } else {
+            ripley::DefaultAssembler2D<double> a(&g.dom, g.dx, g.NE, g.NN);
+            a.assemblePDESingleReduced(val ? &S : nullptr, rhsD, A, B, C, D, X, Y);
         }
     } catch (const std::exception& e) {
         snprintf(g_err, sizeof(g_err), "%s", e.what());

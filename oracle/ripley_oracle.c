@@ -102,6 +102,28 @@ static void q1_build(int dim, const double dx[3], q1_tab* t)
     }
 }
 
+/* The 1-point rule of the reduced-order assembly (assemblePDESingleReduced,
+   DefaultAssembler3D.cpp:2891-3271, DefaultAssembler2D.cpp:842-1010): the element centre
+   with weight = element volume. */
+static void q1_build_reduced(int dim, const double dx[3], q1_tab* t)
+{
+    t->dim = dim;
+    t->nk = 1 << dim;
+    t->nq = 1;
+    double vol = 1.0;
+    for (int d = 0; d < dim; ++d) vol *= dx[d];
+    t->W = vol;
+    for (int k = 0; k < t->nk; ++k) {
+        t->N[0][k] = 1.0 / t->nk;
+        for (int d = 0; d < dim; ++d) {
+            double gd = (((k >> d) & 1) ? 1.0 : -1.0) / dx[d];
+            for (int e = 0; e < dim; ++e)
+                if (e != d) gd *= 0.5;
+            t->G[0][k][d] = gd;
+        }
+    }
+}
+
 /* value of component c of a coefficient at quadrature point q of element e */
 static inline double coef_at(ro_coef a, int size, int nq, int64_t e, int c, int q)
 {
@@ -180,12 +202,37 @@ static void scatter(int nk, const int64_t* nodes, const int32_t* ptr, const int3
    analogue (DefaultAssembler2D.cpp:151-597): two colours of z-slabs (y-rows in 2D),
    elements in k2,k1,k0 order inside a colour; element node order as in
    Brick::addToMatrixAndRHS (Brick.cpp:3238-3265). */
+static void assemble_with(const q1_tab* tp, int dim, const int64_t ne[3], const int32_t* ptr,
+                          const int32_t* idx, double* val, double* rhs, ro_coef A, ro_coef B,
+                          ro_coef C, ro_coef D, ro_coef X, ro_coef Y);
+
 void ro_assemble_single(int dim, const int64_t ne[3], const double dx[3],
                         const int32_t* ptr, const int32_t* idx, double* val, double* rhs,
                         ro_coef A, ro_coef B, ro_coef C, ro_coef D, ro_coef X, ro_coef Y)
 {
     q1_tab t;
     q1_build(dim, dx, &t);
+    assemble_with(&t, dim, ne, ptr, idx, val, rhs, A, B, C, D, X, Y);
+}
+
+/* DefaultAssembler3D::assemblePDESingleReduced (DefaultAssembler3D.cpp:2891-3271) and
+   DefaultAssembler2D::assemblePDESingleReduced (DefaultAssembler2D.cpp:842-1010): the same
+   element formula with the 1-point rule; coefficients on ReducedFunction (one value set
+   per element, or constant). */
+void ro_assemble_single_reduced(int dim, const int64_t ne[3], const double dx[3],
+                                const int32_t* ptr, const int32_t* idx, double* val, double* rhs,
+                                ro_coef A, ro_coef B, ro_coef C, ro_coef D, ro_coef X, ro_coef Y)
+{
+    q1_tab t;
+    q1_build_reduced(dim, dx, &t);
+    assemble_with(&t, dim, ne, ptr, idx, val, rhs, A, B, C, D, X, Y);
+}
+
+static void assemble_with(const q1_tab* tp, int dim, const int64_t ne[3], const int32_t* ptr,
+                          const int32_t* idx, double* val, double* rhs, ro_coef A, ro_coef B,
+                          ro_coef C, ro_coef D, ro_coef X, ro_coef Y)
+{
+    const q1_tab t = *tp;
     const int addS = A.kind || B.kind || C.kind || D.kind;
     const int addF = X.kind || Y.kind;
     if (!addS && !addF) return;

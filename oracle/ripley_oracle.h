@@ -58,6 +58,12 @@ void ro_assemble_single(int dim, const int64_t ne[3], const double dx[3],
                         const int32_t* ptr, const int32_t* idx, double* val, double* rhs,
                         ro_coef A, ro_coef B, ro_coef C, ro_coef D, ro_coef X, ro_coef Y);
 
+/* DefaultAssembler{2,3}D::assemblePDESingleReduced: the same terms with the 1-point
+   (element centre) rule; coefficients constant or one value set per element. */
+void ro_assemble_single_reduced(int dim, const int64_t ne[3], const double dx[3],
+                                const int32_t* ptr, const int32_t* idx, double* val, double* rhs,
+                                ro_coef A, ro_coef B, ro_coef C, ro_coef D, ro_coef X, ro_coef Y);
+
 /* DefaultAssembler{2,3}D::assemblePDEBoundarySingle (face terms d, y), 2x2 (2) Gauss
    per face.  d, y are given per face element in ripley face order. */
 void ro_assemble_boundary(int dim, const int64_t ne[3], const double dx[3],

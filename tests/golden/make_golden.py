@@ -114,6 +114,27 @@ def main():
     g["r200_iter"] = np.array(res.num_iter)
 
     out = os.path.join(HERE, "golden.npz")
+    # reduced-order interior assembly (coefficients on ReducedFunction, one value set per
+    # element), from its own generator so that the cases above keep their values.  (The
+    # solution vectors of the solve cases depend on the reference's OpenMP thread count at
+    # the 1e-13 level; the committed file keeps those of its first generation.)
+    rr = np.random.default_rng(20261204)
+    for dim, ne in ((2, (5, 7)), (3, (3, 4, 5))):
+        dx = tuple(0.3 + 0.2 * k for k in range(dim))
+        tag = f"{dim}d"
+        pat = O.pattern(dim, ne)
+        nel = int(np.prod(ne))
+        for kname, kind in (("const", O.CONSTANT), ("exp", O.EXPANDED)):
+            cs = {}
+            for name, size in (("A", dim * dim), ("B", dim), ("C", dim), ("D", 1), ("X", dim), ("Y", 1)):
+                cs[name] = rr.standard_normal(size if kind == O.CONSTANT else size * nel)
+            val, rhs = O.assemble(dim, ne, dx, pat, use_ref=True, reduced=True,
+                                  **{("C_" if k == "C" else k): (kind, v) for k, v in cs.items()})
+            for k, v in cs.items():
+                g[f"red{tag}_{kname}_{k}"] = v
+            g[f"red{tag}_{kname}_val"] = val
+            g[f"red{tag}_{kname}_rhs"] = rhs
+
     np.savez_compressed(out, **g)
     print(f"wrote {out}: {len(g)} arrays, {os.path.getsize(out) / 1024:.0f} KiB; "
           f"iterations r200={int(g['r200_iter'])} solve2d={int(g['solve2d_iter'])} "

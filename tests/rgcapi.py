@@ -90,6 +90,13 @@ def assemble(mat, rhs_t, keep, **coefs):
     L.check(lib().rg_assemble_single(mat.h if mat else None, ptr(rhs_t), *[C.byref(c) for c in cs]))
 
 
+def assemble_reduced(mat, rhs_t, keep, **coefs):
+    """coefs: name -> (array, kind) for A,B,C,D,X,Y on ReducedFunction."""
+    cs = [coef(*coefs[k], keep) if k in coefs else L.rg_coef(None, 0) for k in "ABCDXY"]
+    L.set_stream_from_torch()
+    L.check(lib().rg_assemble_single_reduced(mat.h if mat else None, ptr(rhs_t), *[C.byref(c) for c in cs]))
+
+
 def assemble_boundary(mat, rhs_t, keep, d=None, y=None):
     dc = coef(*d, keep) if d else L.rg_coef(None, 0)
     yc = coef(*y, keep) if y else L.rg_coef(None, 0)

@@ -41,6 +41,19 @@ def test_pcg_jacobi(domain, precision):
     assert so.getDiagnostics("converged")
 
 
+def test_pcg_jacobi_reduced_coefficients(domain):
+    """test_PCG_JACOBI with the coefficients on ReducedFunction (the 1-point rule of
+    assemblePDESingleReduced): A_reduced = I, D_reduced = 1, Y_reduced = 1 gives u = 1; mixed
+    with full-order coefficients the systems add up."""
+    pde = LinearPDE(domain)
+    pde.setValue(A_reduced=kronecker(domain), D_reduced=1.0, Y_reduced=1.0)
+    u = pde.getSolution()
+    assert check(u, 1.0)
+    pde2 = LinearPDE(domain)
+    pde2.setValue(A=kronecker(domain), D_reduced=1.0, Y=0.5, Y_reduced=0.5)
+    assert check(pde2.getSolution(), 1.0)
+
+
 def test_poisson_quadratic(domain):
     d = domain.getDim()
     cf = ContinuousFunction(domain)
@@ -99,7 +112,7 @@ def test_unsupported_features_raise(cuda):
         LinearPDE(dom, numEquations=2)
     pde = LinearPDE(dom)
     with pytest.raises(NotImplementedError):
-        pde.setValue(A_reduced=kronecker(2))
+        pde.setValue(y_reduced=1.0)
     with pytest.raises(ValueError):
         pde.setValue(Z=1.0)
     pde.setValue(A=kronecker(2), Y=1.0)

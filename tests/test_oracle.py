@@ -58,6 +58,37 @@ def test_assembly_matches_reference(golden, dim, kname, kind):
 
 @pytest.mark.parametrize("dim", [2, 3])
 @pytest.mark.parametrize("kname,kind", [("const", O.CONSTANT), ("exp", O.EXPANDED)])
+def test_reduced_assembly_matches_reference(golden, dim, kname, kind):
+    """assemblePDESingleReduced (1-point rule) against the reference's own output."""
+    tag = f"{dim}d"
+    ne = tuple(golden[f"asm{tag}_ne"])
+    dx = tuple(golden[f"asm{tag}_dx"])
+    pat = O.pattern(dim, ne)
+    cs = {("C_" if k == "C" else k): (kind, golden[f"red{tag}_{kname}_{k}"]) for k in "ABCDXY"}
+    val, rhs = O.assemble(dim, ne, dx, pat, reduced=True, **cs)
+    assert row_scaled_err(pat, val, golden[f"red{tag}_{kname}_val"]) < ASM_TOL
+    ref_rhs = golden[f"red{tag}_{kname}_rhs"]
+    assert np.abs(rhs - ref_rhs).max() <= ASM_TOL * np.abs(ref_rhs).max()
+
+
+@pytest.mark.parametrize("dim,ne", [(2, (4, 6)), (3, (3, 4, 2))])
+def test_reduced_known_answers(dim, ne):
+    """Reduced rule: A = I gives zero row sums; D = 1 gives the element volume spread
+    evenly (sum of all entries = domain volume); Y = 1 integrates to the volume."""
+    dx = tuple(0.5 + 0.25 * k for k in range(dim))
+    pat = O.pattern(dim, ne)
+    vol = float(np.prod([dx[k] * ne[k] for k in range(dim)]))
+    val, rhs = O.assemble(dim, ne, dx, pat, reduced=True, A=(O.CONSTANT, np.eye(dim).reshape(-1)),
+                          Y=(O.CONSTANT, np.ones(1)))
+    for i in range(pat.n):
+        assert abs(val[pat.ptr[i]:pat.ptr[i + 1]].sum()) < 1e-13
+    assert abs(rhs.sum() - vol) < 1e-12 * vol
+    val, _ = O.assemble(dim, ne, dx, pat, reduced=True, D=(O.CONSTANT, np.ones(1)))
+    assert abs(val.sum() - vol) < 1e-12 * vol
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+@pytest.mark.parametrize("kname,kind", [("const", O.CONSTANT), ("exp", O.EXPANDED)])
 def test_boundary_assembly_matches_reference(golden, dim, kname, kind):
     tag = f"{dim}d"
     ne = tuple(golden[f"asm{tag}_ne"])
