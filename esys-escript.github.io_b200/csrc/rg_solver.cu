@@ -75,6 +75,7 @@ struct Workspace {
     cudaGraphExec_t graph[3] = {nullptr, nullptr, nullptr};
     int graph_chunk[3] = {0, 0, 0};
     long long graph_launches[3][T_COUNT] = {};
+    int spmv_cfg = -1;   // FP32 band SpMV pipeline: 0 = 3 stages x 1 CTA/SM, 1 = 2 stages x 2 CTAs/SM
 };
 
 namespace {
@@ -264,6 +265,11 @@ __global__ void __launch_bounds__(kThreads) k_gershgorin(int64_t n, const int32_
     }
     double t[1];
     if (grid_reduce<1, 1u>(v, rb, t) && threadIdx.x == 0) *out = t[0];
+}
+
+__global__ void k_fill32(int64_t n, float* __restrict__ a, float v)
+{
+    for (int64_t i = gtid(); i < n; i += gstride()) a[i] = v;
 }
 
 __global__ void k_mul(int64_t n, const double* __restrict__ a, const double* __restrict__ b,
@@ -578,7 +584,6 @@ __global__ void __launch_bounds__(kThreads) k_std_pupdate(int64_t n, const doubl
 // z = dinv r and the FP64 reductions r.z and r.r.  p alternates between two buffers by
 // the parity counter s->pk.
 constexpr int kTile = 256;
-constexpr int kStages = 3;
 constexpr int kPWin = kTile + 8;
 constexpr int kConsumerWarps = kTile / 32;
 enum { ST_TIMEOUT = 6 };
@@ -698,7 +703,7 @@ __global__ void __launch_bounds__(kThreads) k_f32_init(int64_t n, const double* 
 // thread from shared memory and release the stage through an `empty` mbarrier.  Tiles near
 // the two ends read z and p_old with clamped loads.  All waits are bounded: on timeout the
 // kernel records ST_TIMEOUT and returns.
-template <int NB>
+template <int NB, int kStages>
 __global__ void __launch_bounds__(kTile + 32, 1) k_f32_spmv_tma(const float* __restrict__ band,
                                                                 const __grid_constant__ TmaBandArgs ta,
                                                                 const float* __restrict__ z,
@@ -1082,13 +1087,21 @@ int sm_count()
     return count;
 }
 
+template <int NB, int STAGES>
+size_t tma_smem()
+{
+    return sizeof(float) * STAGES * (NB * kTile + 2 * (NB / 3) * kPWin);
+}
+
+// configurations of the FP32 band SpMV pipeline: (stages, CTAs per SM)
+constexpr int kSpmvCfg[2][2] = {{3, 1}, {2, 2}};
+
 template <int NB>
-int launch_f32_spmv_tma(Matrix* m)
+int launch_f32_spmv_tma(Matrix* m, int cfg)
 {
     Workspace* w = m->ws;
     const Domain* d = m->dom;
     constexpr int NG = NB / 3;
-    const size_t smem = sizeof(float) * kStages * (NB * kTile + 2 * NG * kPWin);
     TmaBandArgs ta;
     int64_t h = 0;
     for (int b = 0; b < NB; ++b) {
@@ -1099,9 +1112,13 @@ int launch_f32_spmv_tma(Matrix* m)
     ta.n = d->n;
     ta.halo = h;
     const int64_t ntiles = (d->n + kTile - 1) / kTile;
-    const int grid = (int)std::min<int64_t>(ntiles, sm_count());
-    RG_TIMED(T_F32_SPMV, (k_f32_spmv_tma<NB><<<grid, kTile + 32, smem, stream()>>>(
-                             m->band32, ta, w->z32, w->p32[0], w->p32[1], w->q32, rbuf(w), w->s)));
+    const int grid = (int)std::min<int64_t>(ntiles, (int64_t)sm_count() * kSpmvCfg[cfg][1]);
+    if (cfg == 0)
+        RG_TIMED(T_F32_SPMV, (k_f32_spmv_tma<NB, 3><<<grid, kTile + 32, tma_smem<NB, 3>(), stream()>>>(
+                                 m->band32, ta, w->z32, w->p32[0], w->p32[1], w->q32, rbuf(w), w->s)));
+    else
+        RG_TIMED(T_F32_SPMV, (k_f32_spmv_tma<NB, 2><<<grid, kTile + 32, tma_smem<NB, 2>(), stream()>>>(
+                                 m->band32, ta, w->z32, w->p32[0], w->p32[1], w->q32, rbuf(w), w->s)));
     RG_CHECK_LAUNCH();
     return RG_OK;
 }
@@ -1110,12 +1127,66 @@ int tma_attributes()
 {
     static bool done = false;
     if (!done) {
-        RG_CHECK_CUDA(cudaFuncSetAttribute(k_f32_spmv_tma<27>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)(sizeof(float) * kStages * (27 * kTile + 2 * 9 * kPWin))));
-        RG_CHECK_CUDA(cudaFuncSetAttribute(k_f32_spmv_tma<9>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)(sizeof(float) * kStages * (9 * kTile + 2 * 3 * kPWin))));
+        RG_CHECK_CUDA(cudaFuncSetAttribute(k_f32_spmv_tma<27, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)tma_smem<27, 3>()));
+        RG_CHECK_CUDA(cudaFuncSetAttribute(k_f32_spmv_tma<27, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)tma_smem<27, 2>()));
+        RG_CHECK_CUDA(cudaFuncSetAttribute(k_f32_spmv_tma<9, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)tma_smem<9, 3>()));
+        RG_CHECK_CUDA(cudaFuncSetAttribute(k_f32_spmv_tma<9, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)tma_smem<9, 2>()));
         done = true;
     }
+    return RG_OK;
+}
+
+int launch_spmv_cfg(Matrix* m, int cfg)
+{
+    return m->dom->nbands == 27 ? launch_f32_spmv_tma<27>(m, cfg) : launch_f32_spmv_tma<9>(m, cfg);
+}
+
+// Picks the faster SpMV pipeline for this matrix once per workspace: a few timed launches of
+// each configuration before the first FP32 segment seeds the recursion (their outputs are
+// overwritten by that seed).
+int tune_spmv(Matrix* m)
+{
+    Workspace* w = m->ws;
+    if (w->spmv_cfg >= 0) return RG_OK;
+    if (timers_on()) {  // keep the timed launch counts clean: default configuration
+        w->spmv_cfg = 0;
+        return RG_OK;
+    }
+    // every timed launch does the full work: z = 1, p = 0, beta = 0 (q = A 1, p.q > 0)
+    k_fill32<<<w->grid_vec, kThreads, 0, stream()>>>(w->n, w->z32, 1.0f);
+    RG_CHECK_LAUNCH();
+    RG_CHECK_CUDA(cudaMemsetAsync(w->p32[0], 0, sizeof(float) * w->n, stream()));
+    RG_CHECK_CUDA(cudaMemsetAsync(w->p32[1], 0, sizeof(float) * w->n, stream()));
+    w->hs->beta = 0.0;
+    w->hs->pk = 0;
+    int rc = RG_OK;
+    cudaEvent_t e0, e1;
+    RG_CHECK_CUDA(cudaEventCreate(&e0));
+    RG_CHECK_CUDA(cudaEventCreate(&e1));
+    float best = 1e30f;
+    int best_cfg = 0;
+    for (int cfg = 0; cfg < 2; ++cfg) {
+        if ((rc = write_scal_fields(w, 0.0, 1, 0))) break;  // done = 0
+        for (int k = 0; k < 2 && rc == RG_OK; ++k) rc = launch_spmv_cfg(m, cfg);
+        RG_CHECK_CUDA(cudaEventRecord(e0, stream()));
+        for (int k = 0; k < 8 && rc == RG_OK; ++k) rc = launch_spmv_cfg(m, cfg);
+        RG_CHECK_CUDA(cudaEventRecord(e1, stream()));
+        RG_CHECK_CUDA(cudaEventSynchronize(e1));
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (rc == RG_OK && ms < best) {
+            best = ms;
+            best_cfg = cfg;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+    w->spmv_cfg = best_cfg;
     return RG_OK;
 }
 
@@ -1123,7 +1194,7 @@ int f32_step(Matrix* m)
 {
     Workspace* w = m->ws;
     const Domain* d = m->dom;
-    int rc = d->nbands == 27 ? launch_f32_spmv_tma<27>(m) : launch_f32_spmv_tma<9>(m);
+    int rc = launch_spmv_cfg(m, w->spmv_cfg < 0 ? 0 : w->spmv_cfg);
     if (rc) return rc;
     RG_TIMED(T_F32_UPDATE, (k_f32_update<<<w->grid_vec, kThreads, 0, stream()>>>(
                                d->n, w->d32, w->r32, w->q32, w->p32[0], w->p32[1], m->dinv32, w->z32, rbuf(w),
@@ -1284,6 +1355,7 @@ int solve_f32(Matrix* m, const rg_solver_opts* o, OuterState& st, rg_diag& dg)
     double n2r = 0, nmr = 0;
     int rc = outer_residual(m, o, st, dg, &conv, &n2r, &nmr, true);
     if (rc || conv) return rc;
+    if ((rc = tune_spmv(m))) return rc;
     bool first = true;
     long long done_iters = 0;
     for (;;) {
