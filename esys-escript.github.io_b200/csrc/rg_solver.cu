@@ -76,6 +76,7 @@ struct Workspace {
     int graph_chunk[3] = {0, 0, 0};
     long long graph_launches[3][T_COUNT] = {};
     int spmv_cfg = -1;   // FP32 band SpMV pipeline: 0 = 3 stages x 1 CTA/SM, 1 = 2 stages x 2 CTAs/SM
+    int grid_upd32 = 0;  // CTAs of k_f32_update (tuned with the SpMV; 0 = grid_vec)
 };
 
 namespace {
@@ -1161,8 +1162,14 @@ int tune_spmv(Matrix* m)
     RG_CHECK_LAUNCH();
     RG_CHECK_CUDA(cudaMemsetAsync(w->p32[0], 0, sizeof(float) * w->n, stream()));
     RG_CHECK_CUDA(cudaMemsetAsync(w->p32[1], 0, sizeof(float) * w->n, stream()));
+    // and for the update kernel: r = 1, d = 0, finite scalars
+    k_fill32<<<w->grid_vec, kThreads, 0, stream()>>>(w->n, w->r32, 1.0f);
+    RG_CHECK_LAUNCH();
+    RG_CHECK_CUDA(cudaMemsetAsync(w->d32, 0, sizeof(float) * w->n, stream()));
     w->hs->beta = 0.0;
     w->hs->pk = 0;
+    w->hs->rho = 1.0;
+    w->hs->norm = 1.0;
     int rc = RG_OK;
     cudaEvent_t e0, e1;
     RG_CHECK_CUDA(cudaEventCreate(&e0));
@@ -1183,10 +1190,38 @@ int tune_spmv(Matrix* m)
             best_cfg = cfg;
         }
     }
+    // the update kernel's grid: fewer CTAs shorten its reduction tail, more hide latency
+    w->spmv_cfg = best_cfg;
+    const int64_t nv = (w->n + 3) / 4;
+    float best_u = 1e30f;
+    int best_grid = w->grid_vec;
+    for (int per_sm : {2, 4, 8}) {
+        const int g = grid_for(nv, kThreads, per_sm);
+        if ((rc = write_scal_fields(w, 0.0, 1LL << 40, 0))) break;  // done = 0, no iteration cap
+        w->grid_upd32 = g;
+        RG_CHECK_CUDA(cudaEventRecord(e0, stream()));
+        for (int k = 0; k < 8 && rc == RG_OK; ++k) {
+            RG_TIMED(T_F32_UPDATE, (k_f32_update<<<g, kThreads, 0, stream()>>>(
+                                       w->n, w->d32, w->r32, w->q32, w->p32[0], w->p32[1], m->dinv32, w->z32,
+                                       rbuf(w), w->s)));
+            rc = cudaGetLastError() == cudaSuccess ? RG_OK : RG_CUDA_ERROR;
+        }
+        RG_CHECK_CUDA(cudaEventRecord(e1, stream()));
+        RG_CHECK_CUDA(cudaEventSynchronize(e1));
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (rc == RG_OK && ms < best_u) {
+            best_u = ms;
+            best_grid = g;
+        }
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    if (rc) return rc;
-    w->spmv_cfg = best_cfg;
+    if (rc) {
+        set_error("FP32 update tuning launch failed");
+        return rc;
+    }
+    w->grid_upd32 = best_grid;
     return RG_OK;
 }
 
@@ -1196,7 +1231,7 @@ int f32_step(Matrix* m)
     const Domain* d = m->dom;
     int rc = launch_spmv_cfg(m, w->spmv_cfg < 0 ? 0 : w->spmv_cfg);
     if (rc) return rc;
-    RG_TIMED(T_F32_UPDATE, (k_f32_update<<<w->grid_vec, kThreads, 0, stream()>>>(
+    RG_TIMED(T_F32_UPDATE, (k_f32_update<<<w->grid_upd32 > 0 ? w->grid_upd32 : w->grid_vec, kThreads, 0, stream()>>>(
                                d->n, w->d32, w->r32, w->q32, w->p32[0], w->p32[1], m->dinv32, w->z32, rbuf(w),
                                w->s)));
     RG_CHECK_LAUNCH();
