@@ -191,6 +191,16 @@ def cpu_full_reference_iterations(inp, threads):
 F32_SPMV_BYTES_PER_ROW = 27 * 4 + 4 * 4
 
 
+def max_over_ranks_of(v, dist=None, device="cpu"):
+    """The largest of every rank's v (the whole job's time); v itself on one process."""
+    if dist is None:
+        return v
+    import torch
+    t = torch.tensor([float(v)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def run_ours(args):
     import ctypes as C
     import torch
@@ -292,11 +302,7 @@ def run_ours(args):
         torch.cuda.synchronize()
 
     def max_over_ranks(v):
-        if dist is None:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return max_over_ranks_of(v, dist, dev)
 
     if args.only == "plain":
         for _ in range(args.warmup + args.steps):
