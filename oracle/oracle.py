@@ -240,3 +240,65 @@ def solve_cg(pat: Pattern, val, b, rtol=1e-10, iter_max=100000, x0=None) -> Solv
 def set_threads(n: int) -> None:
     if have_ref():
         ref().ref_set_threads(n)
+
+
+# ---- PDE systems (block size nb = numEq = numComp, 1..3) -----------------------------------
+# Block CSR values on the node pattern: val[k nb^2 + ir + nb ic]; vectors u[node nb + comp];
+# coefficient data points A (nb, dim, nb, dim), B (nb, dim, nb), C (nb, nb, dim), D (nb, nb),
+# X (nb, dim), Y (nb), first index fastest (escript's layout).
+
+def assemble_system(dim, ne, dx, pat: Pattern, nb, A=None, B=None, C_=None, D=None, X=None, Y=None,
+                    use_ref=False):
+    """assemblePDESystem.  Returns (val (nnz nb^2), rhs (n nb))."""
+    val = np.zeros(pat.nnz * nb * nb)
+    rhs = np.zeros(pat.n * nb)
+    coefs = [_coef(c) for c in (A, B, C_, D, X, Y)]
+    if use_ref:
+        R = ref()
+        kinds = (C.c_int * 6)(*[c[0].kind for c in coefs])
+        ptrs = (C.POINTER(C.c_double) * 6)(*[c[0].p for c in coefs])
+        rc = R.ref_assemble_system(dim, _i64x3(ne), _dx3(dx), int(nb), _ip(pat.ptr), _ip(pat.idx), _dp(val),
+                                   _dp(rhs), kinds, ptrs)
+        if rc:
+            raise RuntimeError(R.ref_last_error().decode())
+    else:
+        lib().ro_assemble_system(dim, _i64x3(ne), _dx3(dx), int(nb), _ip(pat.ptr), _ip(pat.idx), _dp(val),
+                                 _dp(rhs), *[c[0] for c in coefs])
+    return val, rhs
+
+
+def spmv_block(pat: Pattern, nb, val, x, alpha=1.0, beta=0.0, y=None):
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    y = np.zeros(pat.n * nb) if y is None else np.array(y, dtype=np.float64)
+    lib().ro_spmv_block(C.c_int64(pat.n), int(nb), _ip(pat.ptr), _ip(pat.idx), _dp(val), C.c_double(alpha),
+                        _dp(x), C.c_double(beta), _dp(y))
+    return y
+
+
+def insert_constraint_block(pat: Pattern, nb, val, rhs, q, r=None):
+    q = np.ascontiguousarray(q, dtype=np.float64)
+    rr = None if r is None else np.ascontiguousarray(r, dtype=np.float64)
+    lib().ro_insert_constraint_block(C.c_int64(pat.n), int(nb), _ip(pat.ptr), _ip(pat.idx), _dp(val), _dp(rhs),
+                                     _dp(q), _dp(rr) if rr is not None else None)
+
+
+def solve_paso_block(pat: Pattern, nb, val, b, tol=1e-8, iter_max=100000, use_ref=False) -> SolveResult:
+    """paso::Solver PCG + block Jacobi on a block CSR matrix; ``val`` is balanced IN PLACE."""
+    b = np.ascontiguousarray(b, dtype=np.float64).copy()
+    x = np.zeros(pat.n * nb)
+    if use_ref:
+        R = ref()
+        it = C.c_int64(0)
+        rn = C.c_double(0)
+        conv = C.c_int(0)
+        st = R.ref_solve_block(C.c_int64(pat.n), int(nb), _ip(pat.ptr), _ip(pat.idx), _dp(val), _dp(b), _dp(x),
+                               C.c_double(tol), C.c_int64(iter_max), C.byref(it), C.byref(rn), C.byref(conv))
+        if st < 0:
+            raise RuntimeError(R.ref_last_error().decode())
+        return SolveResult(x, st, it.value, rn.value, bool(conv.value))
+    bv = np.zeros(pat.n * nb)
+    d = _Diag()
+    o = _Opts(tol, iter_max, 1, 0)
+    st = lib().ro_solve_paso_block(C.c_int64(pat.n), int(nb), _ip(pat.ptr), _ip(pat.idx), _dp(val), _dp(b),
+                                   _dp(x), _dp(bv), C.byref(o), C.byref(d))
+    return SolveResult(x, st, d.num_iter, d.residual_norm, bool(d.converged), bv)

@@ -35,8 +35,10 @@ template <>
 void ShimDomain::addToMatrixAndRHS<double>(escript::AbstractSystemMatrix* S, escript::Data& F,
                                            const std::vector<double>& EM_S,
                                            const std::vector<double>& EM_F, bool addS,
-                                           bool addF, index_t firstNode, int, int) const
+                                           bool addF, index_t firstNode, int nEq, int nComp) const
 {
+    // element arrays EM_S[INDEX4(ieq, icomp, r, c, nEq, nComp, nk)], EM_F[INDEX2(ieq, r, nEq)];
+    // block entries val[k nEq^2 + ieq + nEq icomp] (RipleyDomain.cpp:1508-1518)
     const int nk = dim == 3 ? 8 : 4;
     index_t rows[8];
     for (int k = 0; k < nk; ++k)
@@ -45,7 +47,8 @@ void ShimDomain::addToMatrixAndRHS<double>(escript::AbstractSystemMatrix* S, esc
     if (addF) {
         double* F_p = F.getSampleDataRW(0, 0.0);
         for (int k = 0; k < nk; ++k)
-            if (rows[k] < numDOF) F_p[rows[k]] += EM_F[k];
+            if (rows[k] < numDOF)
+                for (int e = 0; e < nEq; ++e) F_p[rows[k] * nEq + e] += EM_F[e + nEq * k];
     }
     if (addS && S && S->val) {
         for (int r = 0; r < nk; ++r) {
@@ -53,7 +56,13 @@ void ShimDomain::addToMatrixAndRHS<double>(escript::AbstractSystemMatrix* S, esc
             for (int c = 0; c < nk; ++c) {
                 const index_t col = rows[c];
                 for (index_t k = S->ptr[row]; k < S->ptr[row + 1]; ++k)
-                    if (S->idx[k] == col) { S->val[k] += EM_S[r + nk * c]; break; }
+                    if (S->idx[k] == col) {
+                        for (int ic = 0; ic < nComp; ++ic)
+                            for (int ie = 0; ie < nEq; ++ie)
+                                S->val[k * nEq * nComp + ie + nEq * ic] +=
+                                    EM_S[ie + nEq * (ic + nComp * (r + nk * c))];
+                        break;
+                    }
             }
         }
     }
@@ -75,22 +84,29 @@ namespace paso {
 template <>
 void SystemMatrix<double>::balance()
 {
+    // SystemMatrix::balance (SystemMatrix.cpp:263-312) with SparseMatrix::maxAbsRow and
+    // applyDiagonal (SparseMatrix.cpp:266-282, 361-385): one factor per scalar row
     if (is_balanced) return;
-    const dim_t n = getTotalNumRows();
+    const dim_t nodes = mainBlock->numRows;
+    const dim_t nb = row_block_size;
     const index_t* ptr = mainBlock->pattern->ptr;
     const index_t* idx = mainBlock->pattern->index;
     double* val = mainBlock->val;
-    balance_vector.assign(n, 0.0);
+    balance_vector.assign(nodes * nb, 0.0);
 #pragma omp parallel for
-    for (dim_t i = 0; i < n; ++i) {
-        double fac = 0.;
-        for (index_t k = ptr[i]; k < ptr[i + 1]; ++k) fac = std::max(fac, std::abs(val[k]));
-        balance_vector[i] = fac > 0 ? std::sqrt(1. / fac) : 1.;
-    }
+    for (dim_t i = 0; i < nodes; ++i)
+        for (dim_t ir = 0; ir < nb; ++ir) {
+            double fac = 0.;
+            for (index_t k = ptr[i]; k < ptr[i + 1]; ++k)
+                for (dim_t ic = 0; ic < nb; ++ic) fac = std::max(fac, std::abs(val[k * nb * nb + ir + nb * ic]));
+            balance_vector[i * nb + ir] = fac > 0 ? std::sqrt(1. / fac) : 1.;
+        }
 #pragma omp parallel for
-    for (dim_t i = 0; i < n; ++i)
-        for (index_t k = ptr[i]; k < ptr[i + 1]; ++k)
-            val[k] *= balance_vector[i] * balance_vector[idx[k]];
+    for (dim_t i = 0; i < nodes; ++i)
+        for (dim_t ir = 0; ir < nb; ++ir)
+            for (index_t k = ptr[i]; k < ptr[i + 1]; ++k)
+                for (dim_t ic = 0; ic < nb; ++ic)
+                    val[k * nb * nb + ir + nb * ic] *= balance_vector[i * nb + ir] * balance_vector[idx[k] * nb + ic];
     is_balanced = true;
 }
 
@@ -112,24 +128,62 @@ void SystemMatrix<double>::applyBalanceInPlace(double* x, bool) const
     for (dim_t i = 0; i < n; ++i) x[i] *= balance_vector[i];
 }
 
+namespace {
+// BlockOps_invM_2 / _3 (BlockOps.h:99-160): inverse of a column-major block
+bool invert_block(dim_t nb, const double* A, double* inv)
+{
+    if (nb == 1) {
+        if (!(std::abs(A[0]) > 0.)) return false;
+        inv[0] = 1. / A[0];
+        return true;
+    }
+    if (nb == 2) {
+        double D = A[0] * A[3] - A[2] * A[1];
+        if (!(std::abs(D) > 0)) return false;
+        D = 1. / D;
+        inv[0] = A[3] * D;
+        inv[1] = -A[1] * D;
+        inv[2] = -A[2] * D;
+        inv[3] = A[0] * D;
+        return true;
+    }
+    const double A11 = A[0], A21 = A[1], A31 = A[2], A12 = A[3], A22 = A[4], A32 = A[5];
+    const double A13 = A[6], A23 = A[7], A33 = A[8];
+    double D = A11 * (A22 * A33 - A23 * A32) + A12 * (A31 * A23 - A21 * A33) + A13 * (A21 * A32 - A31 * A22);
+    if (!(std::abs(D) > 0)) return false;
+    D = 1. / D;
+    inv[0] = (A22 * A33 - A23 * A32) * D;
+    inv[1] = (A31 * A23 - A21 * A33) * D;
+    inv[2] = (A21 * A32 - A31 * A22) * D;
+    inv[3] = (A13 * A32 - A12 * A33) * D;
+    inv[4] = (A11 * A33 - A31 * A13) * D;
+    inv[5] = (A12 * A31 - A11 * A32) * D;
+    inv[6] = (A12 * A23 - A13 * A22) * D;
+    inv[7] = (A13 * A21 - A11 * A23) * D;
+    inv[8] = (A11 * A22 - A12 * A21) * D;
+    return true;
+}
+}  // namespace
+
 template <>
 void SystemMatrix<double>::setPreconditioner(Options* options)
 {
+    // SparseMatrix::invMain (SparseMatrix.cpp:387-435) via the diagonal pointer
+    // (Pattern.cpp:139-164): inverses of the main diagonal blocks
     sweeps = options->sweeps;
     if (!dinv.empty()) return;
-    const dim_t n = getTotalNumRows();
+    const dim_t nodes = mainBlock->numRows;
+    const dim_t nb = row_block_size;
     const index_t* ptr = mainBlock->pattern->ptr;
     const index_t* idx = mainBlock->pattern->index;
-    dinv.assign(n, 0.0);
+    dinv.assign(nodes * nb * nb, 0.0);
     bool failed = false;
-    for (dim_t i = 0; i < n; ++i) {
+    for (dim_t i = 0; i < nodes; ++i) {
         const index_t* lo = idx + ptr[i];
         const index_t* hi = idx + ptr[i + 1];
         const index_t* w = std::lower_bound(lo, hi, i);
         if (w == hi || *w != i) { failed = true; continue; }
-        const double a = mainBlock->val[w - idx];
-        if (std::abs(a) > 0.) dinv[i] = 1. / a;
-        else failed = true;
+        if (!invert_block(nb, mainBlock->val + (w - idx) * nb * nb, &dinv[i * nb * nb])) failed = true;
     }
     if (failed) throw PasoException("SparseMatrix::invMain: non-regular main diagonal block.");
 }
@@ -137,13 +191,25 @@ void SystemMatrix<double>::setPreconditioner(Options* options)
 template <>
 void SystemMatrix<double>::solvePreconditioner(double* x, double* b)
 {
-    const dim_t n = getTotalNumRows();
-    for (dim_t i = 0; i < n; ++i) x[i] = b[i] * dinv[i];
+    // Preconditioner_Smoother_solve (Smoother.cpp:100-128): x = D^-1 b, then sweeps-1
+    // corrections x += D^-1 (b - A x) (BlockOps_solveAll: block products)
+    const dim_t nodes = mainBlock->numRows;
+    const dim_t nb = row_block_size;
+    const dim_t n = nodes * nb;
+    auto apply = [&](const double* in, double* out, bool add) {
+        for (dim_t i = 0; i < nodes; ++i)
+            for (dim_t ir = 0; ir < nb; ++ir) {
+                double s = 0.0;
+                for (dim_t ic = 0; ic < nb; ++ic) s += dinv[i * nb * nb + ir + nb * ic] * in[i * nb + ic];
+                out[i * nb + ir] = add ? out[i * nb + ir] + s : s;
+            }
+    };
+    apply(b, x, false);
     std::vector<double> bn;
     for (int s = 1; s < sweeps; ++s) {
         bn.assign(b, b + n);
         SparseMatrix_MatrixVector_CSR_OFFSET0(-1., mainBlock, x, 1., bn.data());
-        for (dim_t i = 0; i < n; ++i) x[i] += bn[i] * dinv[i];
+        apply(bn.data(), x, true);
     }
 }
 
@@ -279,6 +345,42 @@ int ref_assemble_reduced(int dim, const int64_t ne[3], const double dx[3], const
     return 0;
 }
 
+// PDE systems: DefaultAssembler{2,3}D::assemblePDESystem with block size nb; coefficient data
+// point sizes A nb^2 dim^2, B/C nb^2 dim, D nb^2, X nb dim, Y nb
+int ref_assemble_system(int dim, const int64_t ne[3], const double dx[3], int nb, const int32_t* ptr,
+                        const int32_t* idx, double* val, double* rhs, const int* kinds,
+                        const double* const* coefs)
+{
+    try {
+        Geometry g;
+        make_geometry(g, dim, ne, dx);
+        const int nq = 1 << dim;
+        escript::AbstractSystemMatrix S;
+        S.ptr = ptr;
+        S.idx = idx;
+        S.val = val;
+        S.nb = nb;
+        escript::Data rhsD(rhs, nb, 1, true);
+        escript::Data A = make_coef(coefs[0], kinds[0], nb * nb * dim * dim, nq);
+        escript::Data B = make_coef(coefs[1], kinds[1], nb * nb * dim, nq);
+        escript::Data C = make_coef(coefs[2], kinds[2], nb * nb * dim, nq);
+        escript::Data D = make_coef(coefs[3], kinds[3], nb * nb, nq);
+        escript::Data X = make_coef(coefs[4], kinds[4], nb * dim, nq);
+        escript::Data Y = make_coef(coefs[5], kinds[5], nb, nq);
+        if (dim == 3) {
+            ripley::DefaultAssembler3D<double> a(&g.dom, g.dx, g.NE, g.NN);
+            a.assemblePDESystem(val ? &S : nullptr, rhsD, A, B, C, D, X, Y);
+        } else {
+            ripley::DefaultAssembler2D<double> a(&g.dom, g.dx, g.NE, g.NN);
+            a.assemblePDESystem(val ? &S : nullptr, rhsD, A, B, C, D, X, Y);
+        }
+    } catch (const std::exception& e) {
+        snprintf(g_err, sizeof(g_err), "%s", e.what());
+        return 1;
+    }
+    return 0;
+}
+
 // boundary terms d, y on the faces (FunctionOnBoundary layout)
 int ref_assemble_boundary(int dim, const int64_t ne[3], const double dx[3], const int32_t* ptr,
                           const int32_t* idx, double* val, double* rhs, int dkind,
@@ -333,6 +435,37 @@ int ref_solve(int64_t n, int32_t* ptr, int32_t* idx, double* val, double* b, dou
         const double t0 = escript::gettime();
         paso::SolverResult res = paso::Solver(A, x, b, &o, &pp);
         if (seconds) *seconds = escript::gettime() - t0;
+        *num_iter = o.num_iter;
+        *residual_norm = o.residual_norm;
+        *converged = o.converged ? 1 : 0;
+        return (int)res;
+    } catch (const std::exception& e) {
+        snprintf(g_err, sizeof(g_err), "%s", e.what());
+        return -1;
+    }
+}
+
+// paso::Solver with PCG + (block) Jacobi on a block CSR matrix with block size nb
+int ref_solve_block(int64_t nodes, int nb, int32_t* ptr, int32_t* idx, double* val, double* b, double* x,
+                    double tol, int64_t iter_max, int64_t* num_iter, double* residual_norm, int* converged)
+{
+    try {
+        auto A = std::make_shared<paso::SystemMatrix<double>>();
+        A->row_block_size = A->col_block_size = nb;
+        A->mainBlock = std::make_shared<paso::SparseMatrix<double>>();
+        A->mainBlock->numRows = A->mainBlock->numCols = (paso::dim_t)nodes;
+        A->mainBlock->row_block_size = A->mainBlock->col_block_size = nb;
+        A->mainBlock->block_size = nb * nb;
+        A->mainBlock->pattern = std::make_shared<paso::Pattern>();
+        A->mainBlock->pattern->ptr = ptr;
+        A->mainBlock->pattern->index = idx;
+        A->mainBlock->pattern->numOutput = A->mainBlock->pattern->numInput = (paso::dim_t)nodes;
+        A->mainBlock->val = val;
+        paso::Options o;
+        o.tolerance = tol;
+        o.iter_max = (paso::dim_t)iter_max;
+        paso::Performance pp;
+        paso::SolverResult res = paso::Solver(A, x, b, &o, &pp);
         *num_iter = o.num_iter;
         *residual_norm = o.residual_norm;
         *converged = o.converged ? 1 : 0;

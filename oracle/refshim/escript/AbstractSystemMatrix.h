@@ -5,8 +5,9 @@ namespace escript {
 class AbstractSystemMatrix {
 public:
     virtual ~AbstractSystemMatrix() {}
-    int getRowBlockSize() const { return 1; }
-    int getColumnBlockSize() const { return 1; }
+    int getRowBlockSize() const { return nb; }
+    int getColumnBlockSize() const { return nb; }
+    int nb = 1;  // block size (numEq = numComp) of a PDE system
     const int* ptr = nullptr;
     const int* idx = nullptr;
     double* val = nullptr;

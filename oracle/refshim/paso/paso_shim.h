@@ -101,10 +101,10 @@ public:
     std::vector<double> dinv;
     bool is_balanced = false;
     int sweeps = 1;
-    dim_t getTotalNumRows() const { return mainBlock->numRows; }
-    dim_t getTotalNumCols() const { return mainBlock->numCols; }
-    dim_t getGlobalNumRows() const { return mainBlock->numRows; }
-    dim_t getGlobalNumCols() const { return mainBlock->numCols; }
+    dim_t getTotalNumRows() const { return mainBlock->numRows * row_block_size; }
+    dim_t getTotalNumCols() const { return mainBlock->numCols * col_block_size; }
+    dim_t getGlobalNumRows() const { return mainBlock->numRows * row_block_size; }
+    dim_t getGlobalNumCols() const { return mainBlock->numCols * col_block_size; }
     void balance();
     void applyBalance(T* x_out, const T* x, bool RHS) const;
     void applyBalanceInPlace(T* x, bool RHS) const;

@@ -689,3 +689,352 @@ int ro_solve_cg(int64_t n, const int32_t* ptr, const int32_t* idx, const double*
     free(r); free(z); free(p); free(q); free(dinv);
     return st;
 }
+
+/* ------------------------------------------------------------------------- */
+/* PDE systems: block size nb = numEq = numComp (paso block CSR, MATRIX_FORMAT  */
+/* DEFAULT, blocks up to 3 without LAPACK: SystemMatrix.h:403-492).  A block   */
+/* of pattern entry k is val[k nb^2 + ir + nb ic] (column-major, SparseMatrix  */
+/* layout used by addToPasoMatrix, RipleyDomain.cpp:1508-1518); vectors hold   */
+/* the nb components of a node together: u[node nb + comp].                   */
+/* ------------------------------------------------------------------------- */
+
+/* DefaultAssembler3D::assemblePDESystem (DefaultAssembler3D.cpp:3630-5751) and the 2D
+   analogue: per equation k and component m
+     EM_S[k + nb (m + nb (r + nk c))] = sum_q W (A_kimj G_ri G_cj + B_kim G_ri N_c
+                                                 + C_kmj N_r G_cj + D_km N_r N_c)
+     EM_F[k + nb r] = sum_q W (X_ki G_ri + Y_k N_r)
+   with A[k + nb (i + dim (m + nb j))], B[k + nb (i + dim m)], C[k + nb (m + nb j)],
+   D[k + nb m], X[k + nb i], Y[k] per data point (DefaultAssembler3D.cpp:3748-3777, ...). */
+static void element_system(const q1_tab* t, int nb, int64_t e, ro_coef A, ro_coef B, ro_coef C,
+                           ro_coef D, ro_coef X, ro_coef Y, double* EM_S, double* EM_F)
+{
+    const int dim = t->dim, nk = t->nk, nq = t->nq;
+    const int sA = nb * dim * nb * dim, sB = nb * dim * nb, sC = nb * nb * dim, sD = nb * nb;
+    const int sX = nb * dim, sY = nb;
+    memset(EM_S, 0, sizeof(double) * (size_t)(nb * nb * nk * nk));
+    memset(EM_F, 0, sizeof(double) * (size_t)(nb * nk));
+    for (int q = 0; q < nq; ++q)
+        for (int k = 0; k < nb; ++k) {
+            for (int m = 0; m < nb; ++m) {
+                double a[9] = {0}, b[3] = {0}, c[3] = {0}, dq = 0.0;
+                for (int i = 0; i < dim; ++i)
+                    for (int j = 0; j < dim; ++j)
+                        if (A.kind) a[i + dim * j] = coef_at(A, sA, nq, e, k + nb * (i + dim * (m + nb * j)), q);
+                for (int i = 0; i < dim; ++i) {
+                    if (B.kind) b[i] = coef_at(B, sB, nq, e, k + nb * (i + dim * m), q);
+                    if (C.kind) c[i] = coef_at(C, sC, nq, e, k + nb * (m + nb * i), q);
+                }
+                if (D.kind) dq = coef_at(D, sD, nq, e, k + nb * m, q);
+                for (int r = 0; r < nk; ++r) {
+                    const double* Gr = t->G[q][r];
+                    const double Nr = t->N[q][r];
+                    double s[3] = {0, 0, 0};
+                    double bg = 0.0;
+                    for (int j = 0; j < dim; ++j)
+                        for (int i = 0; i < dim; ++i) s[j] += a[i + dim * j] * Gr[i];
+                    for (int i = 0; i < dim; ++i) bg += b[i] * Gr[i];
+                    for (int cc = 0; cc < nk; ++cc) {
+                        const double* Gc = t->G[q][cc];
+                        const double Nc = t->N[q][cc];
+                        double v = 0.0;
+                        for (int j = 0; j < dim; ++j) v += (s[j] + Nr * c[j]) * Gc[j];
+                        v += bg * Nc + dq * Nr * Nc;
+                        EM_S[k + nb * (m + nb * (r + nk * cc))] += t->W * v;
+                    }
+                }
+            }
+            double xq[3] = {0}, yq = 0.0;
+            for (int i = 0; i < dim; ++i)
+                if (X.kind) xq[i] = coef_at(X, sX, nq, e, k + nb * i, q);
+            if (Y.kind) yq = coef_at(Y, sY, nq, e, k, q);
+            for (int r = 0; r < nk; ++r) {
+                double f = yq * t->N[q][r];
+                for (int i = 0; i < dim; ++i) f += xq[i] * t->G[q][r][i];
+                EM_F[k + nb * r] += t->W * f;
+            }
+        }
+}
+
+void ro_assemble_system(int dim, const int64_t ne[3], const double dx[3], int nb,
+                        const int32_t* ptr, const int32_t* idx, double* val, double* rhs,
+                        ro_coef A, ro_coef B, ro_coef C, ro_coef D, ro_coef X, ro_coef Y)
+{
+    q1_tab t;
+    q1_build(dim, dx, &t);
+    const int addS = A.kind || B.kind || C.kind || D.kind;
+    const int addF = X.kind || Y.kind;
+    if (!addS && !addF) return;
+    const int64_t NE0 = ne[0], NE1 = ne[1], NE2 = dim == 3 ? ne[2] : 1;
+    const int64_t NN0 = NE0 + 1, NN1 = NE1 + 1;
+    const int nk = t.nk, bs = nb * nb;
+    const int64_t outer = dim == 3 ? NE2 : NE1;
+    for (int colour = 0; colour < 2; ++colour) {
+#pragma omp parallel for schedule(static)
+        for (int64_t ko = colour; ko < outer; ko += 2) {
+            double EM_S[9 * 64], EM_F[3 * 8];
+            int64_t nodes[8];
+            const int64_t k1lo = dim == 3 ? 0 : ko, k1hi = dim == 3 ? NE1 : ko + 1;
+            const int64_t k2 = dim == 3 ? ko : 0;
+            for (int64_t k1 = k1lo; k1 < k1hi; ++k1)
+                for (int64_t k0 = 0; k0 < NE0; ++k0) {
+                    const int64_t e = k0 + NE0 * k1 + NE0 * NE1 * k2;
+                    element_system(&t, nb, e, A, B, C, D, X, Y, EM_S, EM_F);
+                    const int64_t first = k0 + NN0 * k1 + NN0 * NN1 * k2;
+                    for (int k = 0; k < nk; ++k)
+                        nodes[k] = first + (k & 1) + ((k >> 1) & 1) * NN0 + ((k >> 2) & 1) * NN0 * NN1;
+                    if (addF && rhs)
+                        for (int r = 0; r < nk; ++r)
+                            for (int ir = 0; ir < nb; ++ir) rhs[nodes[r] * nb + ir] += EM_F[ir + nb * r];
+                    if (addS && val)
+                        for (int r = 0; r < nk; ++r)
+                            for (int c = 0; c < nk; ++c)
+                                for (int64_t kk = ptr[nodes[r]]; kk < ptr[nodes[r] + 1]; ++kk)
+                                    if (idx[kk] == nodes[c]) {
+                                        for (int ic = 0; ic < nb; ++ic)
+                                            for (int ir = 0; ir < nb; ++ir)
+                                                val[kk * bs + ir + nb * ic] +=
+                                                    EM_S[ir + nb * (ic + nb * (r + nk * c))];
+                                        break;
+                                    }
+                }
+        }
+    }
+}
+
+/* y = alpha A x + beta y for a block CSR matrix (SparseMatrix_MatrixVector.cpp, blocked
+   branches) */
+void ro_spmv_block(int64_t nodes, int nb, const int32_t* ptr, const int32_t* idx, const double* val,
+                   double alpha, const double* x, double beta, double* y)
+{
+    const int bs = nb * nb;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < nodes; ++i)
+        for (int ir = 0; ir < nb; ++ir) {
+            double s = 0.0;
+            for (int64_t k = ptr[i]; k < ptr[i + 1]; ++k)
+                for (int ic = 0; ic < nb; ++ic) s += val[k * bs + ir + nb * ic] * x[(int64_t)idx[k] * nb + ic];
+            y[i * nb + ir] = (beta == 0.0 ? 0.0 : beta * y[i * nb + ir]) + alpha * s;
+        }
+}
+
+/* insertConstraint for systems (linearPDEs.py:2084-2112 with
+   SparseMatrix::nullifyRowsAndCols_CSR, SparseMatrix.h:513-535): q, r per component */
+void ro_insert_constraint_block(int64_t nodes, int nb, const int32_t* ptr, const int32_t* idx,
+                                double* val, double* rhs, const double* q, const double* r)
+{
+    const int64_t n = nodes * nb;
+    const int bs = nb * nb;
+    double* u = (double*)calloc((size_t)n, sizeof(double));
+    if (r)
+        for (int64_t i = 0; i < n; ++i) u[i] = q[i] > 0 ? r[i] : 0.0;
+    ro_spmv_block(nodes, nb, ptr, idx, val, -1.0, u, 1.0, rhs);
+    for (int64_t i = 0; i < nodes; ++i)
+        for (int64_t k = ptr[i]; k < ptr[i + 1]; ++k)
+            for (int ir = 0; ir < nb; ++ir)
+                for (int ic = 0; ic < nb; ++ic) {
+                    const int64_t irow = i * nb + ir, icol = (int64_t)idx[k] * nb + ic;
+                    if (q[icol] > 0. || q[irow] > 0.) val[k * bs + ir + nb * ic] = irow == icol ? 1.0 : 0.0;
+                }
+    for (int64_t i = 0; i < n; ++i)
+        if (q[i] > 0) rhs[i] = r ? r[i] : 0.0;
+    free(u);
+}
+
+/* block Jacobi: x = D^-1 b with the inverses of the main diagonal blocks (SparseMatrix::
+   invMain with BlockOps_invM_2/3, BlockOps_solveAll; Smoother.cpp:100-128) */
+static void jacobi_block(int64_t nodes, int nb, const double* dinv, const double* b, double* x)
+{
+    const int bs = nb * nb;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < nodes; ++i)
+        for (int ir = 0; ir < nb; ++ir) {
+            double s = 0.0;
+            for (int ic = 0; ic < nb; ++ic) s += dinv[i * bs + ir + nb * ic] * b[i * nb + ic];
+            x[i * nb + ir] = s;
+        }
+}
+
+static int invert_block(int nb, const double* A, double* inv)
+{
+    if (nb == 1) {
+        if (!(fabs(A[0]) > 0.)) return 1;
+        inv[0] = 1. / A[0];
+        return 0;
+    }
+    if (nb == 2) {
+        const double A11 = A[0], A21 = A[1], A12 = A[2], A22 = A[3];
+        double D = A11 * A22 - A12 * A21;
+        if (!(fabs(D) > 0)) return 1;
+        D = 1. / D;
+        inv[0] = A22 * D;
+        inv[1] = -A21 * D;
+        inv[2] = -A12 * D;
+        inv[3] = A11 * D;
+        return 0;
+    }
+    const double A11 = A[0], A21 = A[1], A31 = A[2], A12 = A[3], A22 = A[4], A32 = A[5];
+    const double A13 = A[6], A23 = A[7], A33 = A[8];
+    double D = A11 * (A22 * A33 - A23 * A32) + A12 * (A31 * A23 - A21 * A33) + A13 * (A21 * A32 - A31 * A22);
+    if (!(fabs(D) > 0)) return 1;
+    D = 1. / D;
+    inv[0] = (A22 * A33 - A23 * A32) * D;
+    inv[1] = (A31 * A23 - A21 * A33) * D;
+    inv[2] = (A21 * A32 - A31 * A22) * D;
+    inv[3] = (A13 * A32 - A12 * A33) * D;
+    inv[4] = (A11 * A33 - A31 * A13) * D;
+    inv[5] = (A12 * A31 - A11 * A32) * D;
+    inv[6] = (A12 * A23 - A13 * A22) * D;
+    inv[7] = (A13 * A21 - A11 * A23) * D;
+    inv[8] = (A11 * A22 - A12 * A21) * D;
+    return 0;
+}
+
+/* Solver_PCG (PCG.cpp:62-367) on a block matrix */
+static int pcg_block(int64_t nodes, int nb, const int32_t* ptr, const int32_t* idx, const double* val,
+                     const double* dinv, double* r, double* x, int64_t* iter, double* tol)
+{
+    const int64_t n = nodes * nb;
+    double* rs = (double*)malloc(sizeof(double) * (size_t)n);
+    double* p = (double*)malloc(sizeof(double) * (size_t)n);
+    double* v = (double*)malloc(sizeof(double) * (size_t)n);
+    double* x2 = (double*)malloc(sizeof(double) * (size_t)n);
+    const int64_t maxit = *iter;
+    const double tolv = *tol;
+    for (int64_t i = 0; i < n; ++i) { rs[i] = r[i]; x2[i] = x[i]; p[i] = 0; v[i] = 0; }
+    int64_t num_iter = 0;
+    double tau = 0.0, tau_old, norm_of_residual = 0.0;
+    int converge = 0, maxflag = 0, brk = 0;
+    while (!(converge || maxflag || brk)) {
+        ++num_iter;
+        jacobi_block(nodes, nb, dinv, r, v);
+        const double sum1 = dot(n, v, r);
+        tau_old = tau;
+        tau = sum1;
+        if (num_iter == 1) {
+            for (int64_t i = 0; i < n; ++i) p[i] = v[i];
+        } else {
+            const double beta = tau / tau_old;
+            for (int64_t i = 0; i < n; ++i) p[i] = v[i] + beta * p[i];
+        }
+        ro_spmv_block(nodes, nb, ptr, idx, val, 1.0, p, 0.0, v);
+        const double delta = dot(n, v, p);
+        const double alpha = tau / delta;
+        brk = fabs(delta) <= 0.0;
+        if (!brk) {
+            double s3 = 0.0, s4 = 0.0;
+            for (int64_t i = 0; i < n; ++i) {
+                r[i] -= alpha * v[i];
+                const double d = r[i] - rs[i];
+                s3 += d * d;
+                s4 += d * rs[i];
+            }
+            const double gamma_1 = (fabs(s3) <= 0.0) ? 0.0 : -s4 / s3;
+            const double gamma_2 = 1.0 - gamma_1;
+            double s5 = 0.0;
+            for (int64_t i = 0; i < n; ++i) {
+                rs[i] = gamma_2 * rs[i] + gamma_1 * r[i];
+                x2[i] += alpha * p[i];
+                x[i] = gamma_2 * x[i] + gamma_1 * x2[i];
+                s5 += rs[i] * rs[i];
+            }
+            norm_of_residual = sqrt(s5);
+            converge = norm_of_residual <= tolv;
+            maxflag = num_iter > maxit;
+            brk = fabs(tau) <= 0.0;
+        }
+    }
+    free(rs); free(p); free(v); free(x2);
+    *iter = num_iter;
+    *tol = norm_of_residual;
+    if (maxflag) return RO_MAXITER;
+    if (brk) return RO_BREAKDOWN;
+    return RO_OK;
+}
+
+/* paso::Solver (Solver.cpp:46-330), PCG + block Jacobi (sweeps = 1), block matrix balanced
+   in place per scalar row (SparseMatrix::maxAbsRow_CSR_OFFSET0 and applyDiagonal). */
+int ro_solve_paso_block(int64_t nodes, int nb, const int32_t* ptr, const int32_t* idx, double* val,
+                        const double* b, double* x, double* bv, const ro_opts* opts, ro_diag* diag)
+{
+    const double EPS = 2.220446049250313e-16;
+    const double tolerance = opts->tolerance;
+    const int64_t n = nodes * nb;
+    const int bs = nb * nb;
+    memset(diag, 0, sizeof(*diag));
+    if (tolerance < 100. * EPS || tolerance > 1.) return RO_INPUT_ERROR;
+    if (nb < 1 || nb > 3) return RO_INPUT_ERROR;
+    for (int64_t i = 0; i < nodes; ++i)
+        for (int ir = 0; ir < nb; ++ir) {
+            double fac = 0.0;
+            for (int64_t k = ptr[i]; k < ptr[i + 1]; ++k)
+                for (int ic = 0; ic < nb; ++ic) fac = fmax(fac, fabs(val[k * bs + ir + nb * ic]));
+            bv[i * nb + ir] = fac > 0 ? sqrt(1. / fac) : 1.0;
+        }
+    for (int64_t i = 0; i < nodes; ++i)
+        for (int ir = 0; ir < nb; ++ir)
+            for (int64_t k = ptr[i]; k < ptr[i + 1]; ++k)
+                for (int ic = 0; ic < nb; ++ic)
+                    val[k * bs + ir + nb * ic] *= bv[i * nb + ir] * bv[(int64_t)idx[k] * nb + ic];
+    double* r = (double*)malloc(sizeof(double) * (size_t)n);
+    double* dinv = (double*)malloc(sizeof(double) * (size_t)(nodes * bs));
+    for (int64_t i = 0; i < n; ++i) r[i] = b[i] * bv[i];
+    double n2b, nmb;
+    norms(n, r, &n2b, &nmb);
+    n2b = sqrt(n2b);
+    int err = RO_OK;
+    if (isnan(n2b) || isnan(nmb)) {
+        err = RO_NAN;
+    } else if (n2b <= 0.) {
+        for (int64_t i = 0; i < n; ++i) x[i] = 0.0;
+    } else {
+        for (int64_t i = 0; i < nodes && err == RO_OK; ++i) {
+            int64_t kd = -1;
+            for (int64_t k = ptr[i]; k < ptr[i + 1]; ++k)
+                if (idx[k] == i) { kd = k; break; }
+            if (kd < 0 || invert_block(nb, val + kd * bs, dinv + i * bs)) err = RO_INPUT_ERROR;
+        }
+        if (err == RO_OK) {
+            jacobi_block(nodes, nb, dinv, r, x);
+            int64_t totIter = 1;
+            int fin = 0;
+            double last2 = n2b, lastm = nmb;
+            while (!fin) {
+                int64_t cnt = opts->iter_max - totIter;
+                fin = 1;
+                if (totIter > 1)
+                    for (int64_t i = 0; i < n; ++i) r[i] = b[i] * bv[i];
+                ro_spmv_block(nodes, nb, ptr, idx, val, -1., x, 1., r);
+                double n2r, nmr;
+                norms(n, r, &n2r, &nmr);
+                n2r = sqrt(n2r);
+                diag->residual_norm = n2r;
+                diag->num_outer++;
+                if (totIter > 1 && n2r >= last2 && nmr >= lastm) {
+                    err = RO_DIVERGENCE;
+                    break;
+                }
+                if (n2r > tolerance * n2b || nmr > tolerance * nmb) {
+                    double tol = tolerance * fmin(n2b, 0.1 * n2r / nmr * nmb);
+                    last2 = n2r;
+                    lastm = nmr;
+                    int st = pcg_block(nodes, nb, ptr, idx, val, dinv, r, x, &cnt, &tol);
+                    totIter += cnt;
+                    if (st == RO_OK) {
+                        fin = 0;
+                    } else if (st == RO_BREAKDOWN && cnt > 1) {
+                        fin = 0;
+                    } else {
+                        err = st;
+                        break;
+                    }
+                } else {
+                    diag->converged = 1;
+                }
+            }
+            diag->num_iter = totIter;
+            for (int64_t i = 0; i < n; ++i) x[i] *= bv[i];
+        }
+    }
+    free(r); free(dinv);
+    return err;
+}

@@ -93,6 +93,19 @@ int ro_solve_paso(int64_t n, const int32_t* ptr, const int32_t* idx, double* val
 int ro_solve_cg(int64_t n, const int32_t* ptr, const int32_t* idx, const double* val,
                 const double* b, double* x, double rtol, int64_t iter_max, ro_diag* diag);
 
+/* PDE systems with block size nb (1..3): block CSR values val[k nb^2 + ir + nb ic] on the
+   node pattern, vectors u[node nb + comp].  Coefficient data points: A (nb, dim, nb, dim),
+   B (nb, dim, nb), C (nb, nb, dim), D (nb, nb), X (nb, dim), Y (nb), first index fastest. */
+void ro_assemble_system(int dim, const int64_t ne[3], const double dx[3], int nb,
+                        const int32_t* ptr, const int32_t* idx, double* val, double* rhs,
+                        ro_coef A, ro_coef B, ro_coef C, ro_coef D, ro_coef X, ro_coef Y);
+void ro_spmv_block(int64_t nodes, int nb, const int32_t* ptr, const int32_t* idx, const double* val,
+                   double alpha, const double* x, double beta, double* y);
+void ro_insert_constraint_block(int64_t nodes, int nb, const int32_t* ptr, const int32_t* idx,
+                                double* val, double* rhs, const double* q, const double* r);
+int ro_solve_paso_block(int64_t nodes, int nb, const int32_t* ptr, const int32_t* idx, double* val,
+                        const double* b, double* x, double* bv, const ro_opts* opts, ro_diag* diag);
+
 #ifdef __cplusplus
 }
 #endif

@@ -135,6 +135,53 @@ def main():
             g[f"red{tag}_{kname}_val"] = val
             g[f"red{tag}_{kname}_rhs"] = rhs
 
+    # PDE systems (block size nb = numEq = numComp): assemblePDESystem for every coefficient
+    # with random data, and a Lame elasticity solve clamped on the bottom face
+    rs = np.random.default_rng(20261205)
+    for dim, ne, nb in ((2, (5, 7), 2), (3, (3, 4, 5), 3)):
+        dx = tuple(0.3 + 0.2 * k for k in range(dim))
+        tag = f"{dim}d"
+        pat = O.pattern(dim, ne)
+        nel = int(np.prod(ne))
+        nq = 1 << dim
+        sizes = {"A": nb * nb * dim * dim, "B": nb * nb * dim, "C": nb * nb * dim, "D": nb * nb, "X": nb * dim,
+                 "Y": nb}
+        for kname, kind in (("const", O.CONSTANT), ("exp", O.EXPANDED)):
+            cs = {k: rs.standard_normal(v if kind == O.CONSTANT else v * nq * nel) for k, v in sizes.items()}
+            val, rhs = O.assemble_system(dim, ne, dx, pat, nb, use_ref=True,
+                                         **{("C_" if k == "C" else k): (kind, v) for k, v in cs.items()})
+            for k, v in cs.items():
+                g[f"sys{tag}_{kname}_{k}"] = v
+            g[f"sys{tag}_{kname}_val"] = val
+            g[f"sys{tag}_{kname}_rhs"] = rhs
+        g[f"sys{tag}_nb"] = np.array(nb)
+    for dim, ne in ((2, (16, 12)), (3, (5, 4, 6))):
+        nb = dim
+        tag = f"{dim}d"
+        dx = tuple(1.0 / e for e in ne)
+        pat = O.pattern(dim, ne)
+        nel = int(np.prod(ne))
+        nq = 1 << dim
+        lam, mu = 1.0, 0.5
+        A = np.zeros((dim, dim, dim, dim))
+        for k in range(dim):
+            for i in range(dim):
+                for m in range(dim):
+                    for j in range(dim):
+                        A[k, i, m, j] = lam * (k == i) * (m == j) + mu * ((k == m) * (i == j) + (k == j) * (i == m))
+        A = A.reshape(-1, order="F")
+        Y = rs.standard_normal(nb * nq * nel)
+        val, rhs = O.assemble_system(dim, ne, dx, pat, nb, A=(O.CONSTANT, A), Y=(O.EXPANDED, Y), use_ref=True)
+        nn = [e + 1 for e in ne]
+        n = int(np.prod(nn))
+        layer = int(np.prod(nn[: dim - 1]))
+        q = np.repeat(((np.arange(n) // layer) == 0).astype(np.float64), nb)
+        O.insert_constraint_block(pat, nb, val, rhs, q)
+        res = O.solve_paso_block(pat, nb, val.copy(), rhs, tol=1e-10, use_ref=True)
+        g[f"lame{tag}_ne"] = np.array(ne)
+        g[f"lame{tag}_A"], g[f"lame{tag}_Y"], g[f"lame{tag}_q"] = A, Y, q
+        g[f"lame{tag}_x"], g[f"lame{tag}_iter"] = res.x, np.array(res.num_iter)
+
     np.savez_compressed(out, **g)
     print(f"wrote {out}: {len(g)} arrays, {os.path.getsize(out) / 1024:.0f} KiB; "
           f"iterations r200={int(g['r200_iter'])} solve2d={int(g['solve2d_iter'])} "
