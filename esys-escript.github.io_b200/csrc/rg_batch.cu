@@ -1077,6 +1077,10 @@ int rg_batch_create(rg_matrix* const* mats, int ninst, int nrhs, rg_batch** out)
         }
         Matrix* m = &mats[i]->m;
         const Domain* d = m->dom;
+        if (m->nb != 1) {
+            set_error("rg_batch_create: PDE systems (block size > 1) are not supported in batches");
+            return fail(RG_NOT_SUPPORTED);
+        }
         if (i == 0) b->dim = d->dim;
         if (d->dim != b->dim) {
             set_error("rg_batch_create: all systems must have the same dimension");

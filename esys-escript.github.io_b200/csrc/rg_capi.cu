@@ -61,6 +61,7 @@ void free_matrix(Matrix* m)
 {
     free_workspace(m);
     free_residual_scratch(m);
+    free_system_workspace(m);
     if (m->val) cudaFree(m->val);
     if (m->bv) cudaFree(m->bv);
     if (m->dinv) cudaFree(m->dinv);
@@ -243,6 +244,43 @@ int rg_matrix_create(rg_domain* dom, rg_matrix** out)
     RG_GUARD_END
 }
 
+int rg_matrix_create_system(rg_domain* dom, int block_size, rg_matrix** out)
+{
+    RG_REQUIRE(out, "rg_matrix_create_system: out is NULL");
+    *out = nullptr;
+    RG_REQUIRE(dom, "rg_matrix_create_system: NULL domain");
+    if (block_size == 1) return rg_matrix_create(dom, out);
+    if (block_size != 2 && block_size != 3) {
+        set_error("rg_matrix_create_system: block sizes 1, 2 and 3 are supported");
+        return RG_NOT_SUPPORTED;
+    }
+    RG_GUARD_BEGIN
+    rg_matrix* h = new rg_matrix();
+    Matrix& m = h->m;
+    m.dom = &dom->d;
+    m.nb = block_size;
+    const size_t nv = (size_t)dom->d.nnz * block_size * block_size;
+    cudaError_t e = cudaMalloc((void**)&m.val, sizeof(double) * nv);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&m.bv, sizeof(double) * dom->d.n * block_size);
+    if (e == cudaSuccess) e = cudaMemsetAsync(m.val, 0, sizeof(double) * nv, stream());
+    if (e != cudaSuccess) {
+        free_matrix(&m);
+        delete h;
+        set_error(std::string("rg_matrix_create_system: ") + cudaGetErrorString(e));
+        return RG_CUDA_ERROR;
+    }
+    *out = h;
+    return RG_OK;
+    RG_GUARD_END
+}
+
+int rg_matrix_block_size(const rg_matrix* mat, int* block_size)
+{
+    RG_REQUIRE(mat && block_size, "rg_matrix_block_size: NULL argument");
+    *block_size = mat->m.nb;
+    return RG_OK;
+}
+
 int rg_matrix_destroy(rg_matrix* mat)
 {
     if (!mat) return RG_OK;
@@ -256,7 +294,7 @@ int rg_matrix_reset(rg_matrix* mat)
 {
     RG_REQUIRE(mat, "rg_matrix_reset: NULL matrix");
     Matrix& m = mat->m;
-    RG_CHECK_CUDA(cudaMemsetAsync(m.val, 0, sizeof(double) * m.dom->nnz, stream()));
+    RG_CHECK_CUDA(cudaMemsetAsync(m.val, 0, sizeof(double) * m.dom->nnz * m.nb * m.nb, stream()));
     m.balanced = false;
     m.solver_ready = false;
     return RG_OK;
@@ -289,6 +327,10 @@ int rg_assemble_single(rg_matrix* mat, double* rhs, const rg_coef* A, const rg_c
                        const rg_coef* C, const rg_coef* D, const rg_coef* X, const rg_coef* Y)
 {
     RG_REQUIRE(mat, "rg_assemble_single: a matrix handle is required (it names the domain)");
+    if (mat->m.nb != 1) {
+        set_error("rg_assemble_single: the matrix is a PDE system; use rg_assemble_system");
+        return RG_INVALID_ARG;
+    }
     const rg_coef* c[6] = {A, B, C, D, X, Y};
     for (int j = 0; j < 6; ++j) RG_REQUIRE(coef_ok(c[j]), "rg_assemble_single: invalid coefficient");
     const bool addS = (A && A->kind) || (B && B->kind) || (C && C->kind) || (D && D->kind);
@@ -304,6 +346,10 @@ int rg_assemble_single_reduced(rg_matrix* mat, double* rhs, const rg_coef* A, co
                                const rg_coef* C, const rg_coef* D, const rg_coef* X, const rg_coef* Y)
 {
     RG_REQUIRE(mat, "rg_assemble_single_reduced: a matrix handle is required (it names the domain)");
+    if (mat->m.nb != 1) {
+        set_error("rg_assemble_single_reduced: reduced-order terms of PDE systems are not implemented");
+        return RG_NOT_SUPPORTED;
+    }
     const rg_coef* c[6] = {A, B, C, D, X, Y};
     for (int j = 0; j < 6; ++j) RG_REQUIRE(coef_ok(c[j]), "rg_assemble_single_reduced: invalid coefficient");
     const bool addS = (A && A->kind) || (B && B->kind) || (C && C->kind) || (D && D->kind);
@@ -315,9 +361,29 @@ int rg_assemble_single_reduced(rg_matrix* mat, double* rhs, const rg_coef* A, co
     return assemble_single_impl(mat->m.dom, mat->m.val, rhs, c, true);
 }
 
+int rg_assemble_system(rg_matrix* mat, double* rhs, const rg_coef* A, const rg_coef* B,
+                       const rg_coef* C, const rg_coef* D, const rg_coef* X, const rg_coef* Y)
+{
+    RG_REQUIRE(mat, "rg_assemble_system: a matrix handle is required (it names the domain and block size)");
+    const rg_coef* c[6] = {A, B, C, D, X, Y};
+    for (int j = 0; j < 6; ++j) RG_REQUIRE(coef_ok(c[j]), "rg_assemble_system: invalid coefficient");
+    const bool addS = (A && A->kind) || (B && B->kind) || (C && C->kind) || (D && D->kind);
+    if (addS) {
+        int rc = require_unbalanced(&mat->m, "rg_assemble_system");
+        if (rc) return rc;
+        mat->m.solver_ready = false;
+    }
+    if (mat->m.nb == 1) return assemble_single_impl(mat->m.dom, mat->m.val, rhs, c, false);
+    return assemble_system_impl(mat->m.dom, mat->m.nb, mat->m.val, rhs, c);
+}
+
 int rg_assemble_boundary(rg_matrix* mat, double* rhs, const rg_coef* d, const rg_coef* y)
 {
     RG_REQUIRE(mat, "rg_assemble_boundary: a matrix handle is required");
+    if (mat->m.nb != 1) {
+        set_error("rg_assemble_boundary: boundary terms of PDE systems are not implemented");
+        return RG_NOT_SUPPORTED;
+    }
     RG_REQUIRE(coef_ok(d) && coef_ok(y), "rg_assemble_boundary: invalid coefficient");
     if (d && d->kind) {
         int rc = require_unbalanced(&mat->m, "rg_assemble_boundary");
@@ -335,6 +401,7 @@ int rg_insert_constraint(rg_matrix* mat, double* rhs, const double* q, const dou
         if (rc) return rc;
         mat->m.solver_ready = false;
     }
+    if (mat->m.nb != 1) return launch_system_constraint(&mat->m, rhs, q, r, rhs_only);
     return launch_insert_constraint(&mat->m, rhs, q, r, rhs_only);
 }
 
@@ -345,6 +412,7 @@ int rg_nullify_rows_and_cols(rg_matrix* mat, const double* mask_row, const doubl
     int rc = require_unbalanced(&mat->m, "rg_nullify_rows_and_cols");
     if (rc) return rc;
     mat->m.solver_ready = false;
+    if (mat->m.nb != 1) return launch_system_nullify(&mat->m, mask_row, mask_col, main_diagonal_value);
     return launch_nullify(&mat->m, mask_row, mask_col, main_diagonal_value);
 }
 
@@ -352,6 +420,7 @@ int rg_spmv(rg_matrix* mat, double alpha, const double* x, double beta, double* 
 {
     RG_REQUIRE(mat && x && y, "rg_spmv: NULL argument");
     RG_REQUIRE(!mat->m.balanced, "MatrixVector: balanced matrix is not supported.");
+    if (mat->m.nb != 1) return launch_system_spmv(&mat->m, alpha, x, beta, y);
     return launch_spmv64(mat->m.dom, mat->m.val, alpha, x, beta, y);
 }
 
@@ -366,22 +435,27 @@ int rg_save_mm(rg_matrix* mat, const char* path)
     RG_REQUIRE(mat && path, "rg_save_mm: NULL argument");
     RG_GUARD_BEGIN
     const Domain& d = *mat->m.dom;
+    const int nb = mat->m.nb;
     std::vector<int32_t> ptr(d.n + 1), idx(d.nnz);
-    std::vector<double> val(d.nnz);
+    std::vector<double> val((size_t)d.nnz * nb * nb);
     RG_CHECK_CUDA(cudaMemcpyAsync(ptr.data(), d.ptr, sizeof(int32_t) * (d.n + 1), cudaMemcpyDeviceToHost, stream()));
     RG_CHECK_CUDA(cudaMemcpyAsync(idx.data(), d.idx, sizeof(int32_t) * d.nnz, cudaMemcpyDeviceToHost, stream()));
-    RG_CHECK_CUDA(cudaMemcpyAsync(val.data(), mat->m.val, sizeof(double) * d.nnz, cudaMemcpyDeviceToHost, stream()));
+    RG_CHECK_CUDA(cudaMemcpyAsync(val.data(), mat->m.val, sizeof(double) * val.size(), cudaMemcpyDeviceToHost, stream()));
     RG_CHECK_CUDA(cudaStreamSynchronize(stream()));
     FILE* f = fopen(path, "w");
     if (!f) {
         set_error(std::string("rg_save_mm: cannot open ") + path);
         return RG_INVALID_ARG;
     }
+    // scalar coordinates: block entry (ir, ic) of node pair (i, j) is row i nb + ir, column j nb + ic
     fprintf(f, "%%%%MatrixMarket matrix coordinate real general\n");
-    fprintf(f, "%lld %lld %lld\n", (long long)d.n, (long long)d.n, (long long)d.nnz);
+    fprintf(f, "%lld %lld %lld\n", (long long)d.n * nb, (long long)d.n * nb, (long long)d.nnz * nb * nb);
     for (int64_t i = 0; i < d.n; ++i)
-        for (int32_t k = ptr[i]; k < ptr[i + 1]; ++k)
-            fprintf(f, "%lld %d %.17g\n", (long long)(i + 1), idx[k] + 1, val[k]);
+        for (int ir = 0; ir < nb; ++ir)
+            for (int32_t k = ptr[i]; k < ptr[i + 1]; ++k)
+                for (int ic = 0; ic < nb; ++ic)
+                    fprintf(f, "%lld %lld %.17g\n", (long long)(i * nb + ir + 1), (long long)idx[k] * nb + ic + 1,
+                            val[(size_t)k * nb * nb + ir + nb * ic]);
     fclose(f);
     return RG_OK;
     RG_GUARD_END
@@ -412,6 +486,7 @@ int rg_solve(rg_matrix* mat, const double* rhs, double* x, const rg_solver_opts*
     else
         rg_solver_opts_default(&o);
     RG_GUARD_BEGIN
+    if (mat->m.nb != 1) return rg::solve_system(&mat->m, rhs, x, &o, diag);
     return rg::solve(&mat->m, rhs, x, &o, diag);
     RG_GUARD_END
 }

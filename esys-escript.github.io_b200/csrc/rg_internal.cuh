@@ -67,11 +67,14 @@ struct Domain {
 };
 
 struct Workspace;        // solver vectors, allocated lazily (rg_solver.cu)
+struct SysWorkspace;     // vectors of the block (PDE system) solver (rg_system.cu)
 struct ResidualScratch;  // reduction scratch of rg_residual_norms (rg_residual.cu)
 
 struct Matrix {
     Domain* dom;
-    double* val = nullptr;     // nnz FP64 CSR values (paso mainBlock->val)
+    int nb = 1;                // block size (numEq = numComp of a PDE system; 1 = scalar)
+    double* val = nullptr;     // nnz * nb^2 FP64 CSR values (paso mainBlock->val), blocks
+                               // column-major: val[k nb^2 + ir + nb ic]
     double* bv = nullptr;      // balance vector
     bool balanced = false;
     // solver data derived from the balanced values (paso's preconditioner data)
@@ -81,6 +84,7 @@ struct Matrix {
     float* dinv32 = nullptr;
     Workspace* ws = nullptr;
     ResidualScratch* rs = nullptr;
+    SysWorkspace* sws = nullptr;
 };
 
 // ---------------------------------------------------------------- deterministic reductions
@@ -222,6 +226,14 @@ int solve(Matrix* m, const double* rhs, double* x, const rg_solver_opts* o, rg_d
 // included when `band` (what rg_solve does before iterating)
 int solver_prepare(Matrix* m, bool band);
 void free_workspace(Matrix* m);
+// PDE systems (rg_system.cu): block size m->nb in {2, 3}
+int assemble_system_impl(const Domain* d, int nb, double* val, double* rhs, const rg_coef* c[6]);
+int launch_system_constraint(Matrix* m, double* rhs, const double* q, const double* r, int rhs_only);
+int launch_system_nullify(Matrix* m, const double* mr, const double* mc, double diag);
+int launch_system_spmv(const Matrix* m, double alpha, const double* x, double beta, double* y);
+int solve_system(Matrix* m, const double* rhs, double* x, const rg_solver_opts* o, rg_diag* diag);
+int residual_norms_system(Matrix* m, const double* b, const double* x, double* l2, double* linf);
+void free_system_workspace(Matrix* m);
 void free_residual_scratch(Matrix* m);
 // l2 norm of b - A x with the matrix's values as they are (unbalance: undo an in-place
 // balancing on the fly); synchronises the stream

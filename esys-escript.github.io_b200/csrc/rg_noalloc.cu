@@ -67,6 +67,10 @@ extern "C" int rg_residual_norms_noalloc(rg_matrix* mat, const double* rhs, cons
                                          double* linf_host)
 {
     RG_REQUIRE(mat && rhs && x, "rg_residual_norms_noalloc: NULL argument");
+    if (mat->m.nb != 1) {
+        set_error("rg_residual_norms_noalloc: PDE systems are not supported (use rg_residual_norms)");
+        return RG_NOT_SUPPORTED;
+    }
     Matrix* m = &mat->m;
     const Domain* d = m->dom;
     const int grid = residual::grid(d->n);

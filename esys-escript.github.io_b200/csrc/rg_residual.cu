@@ -60,6 +60,7 @@ extern "C" int rg_residual_norms(rg_matrix* mat, const double* rhs, const double
 {
     RG_REQUIRE(mat && rhs && x, "rg_residual_norms: NULL argument");
     Matrix* m = &mat->m;
+    if (m->nb != 1) return residual_norms_system(m, rhs, x, l2_host, linf_host);
     const Domain* d = m->dom;
     int rc = ensure_residual_scratch(m);
     if (rc) return rc;

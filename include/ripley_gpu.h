@@ -85,6 +85,12 @@ typedef struct {
 /* ---- system matrix: paso::SystemMatrix<double>, block size 1 -------------------------- */
 int rg_matrix_create(rg_domain* dom, rg_matrix** out); /* values zeroed */
 int rg_matrix_destroy(rg_matrix* mat);
+/* A PDE system's matrix (numEq = numComp = block_size, 1..3; paso block CSR on the node
+   pattern, SystemMatrix.h:403-492): values val[k bs^2 + ir + bs ic] for pattern entry k,
+   equation ir, component ic (column-major blocks); vectors hold a node's components
+   together, u[node bs + comp].  Solved by the paso algorithm in FP64 with block Jacobi. */
+int rg_matrix_create_system(rg_domain* dom, int block_size, rg_matrix** out);
+int rg_matrix_block_size(const rg_matrix* mat, int* block_size);
 /* AbstractSystemMatrix::resetValues: zero the values, drop balancing and solver data */
 int rg_matrix_reset(rg_matrix* mat);
 /* device pointer to the nnz CSR values (FP64), in the domain's pattern order */
@@ -106,6 +112,12 @@ int rg_assemble_single(rg_matrix* mat, double* rhs, const rg_coef* A, const rg_c
    Coefficients are CONSTANT, or EXPANDED / PER_ELEMENT with one value set per element. */
 int rg_assemble_single_reduced(rg_matrix* mat, double* rhs, const rg_coef* A, const rg_coef* B,
                                const rg_coef* C, const rg_coef* D, const rg_coef* X, const rg_coef* Y);
+/* assemblePDESystem (ripley/src/DefaultAssembler3D.cpp:3630-5751, DefaultAssembler2D.cpp:
+   1186-1980): the interior terms of a PDE system into a matrix of rg_matrix_create_system.
+   Coefficient data points, first index fastest: A (bs, dim, bs, dim), B (bs, dim, bs),
+   C (bs, bs, dim), D (bs, bs), X (bs, dim), Y (bs); rhs has n bs entries. */
+int rg_assemble_system(rg_matrix* mat, double* rhs, const rg_coef* A, const rg_coef* B,
+                       const rg_coef* C, const rg_coef* D, const rg_coef* X, const rg_coef* Y);
 /* assemblePDEBoundarySingle: adds the face terms d (matrix) and y (rhs).  d/y are on
    FunctionOnBoundary: faces left,right,bottom,top(,front,back), face elements lower
    in-face axis fastest, 2^(dim-1) Gauss points per face element. */

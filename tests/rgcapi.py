@@ -48,16 +48,20 @@ class Domain:
 
 
 class Matrix:
-    def __init__(self, dom):
+    def __init__(self, dom, block_size=1):
         self.dom = dom
+        self.nb = block_size
         self.h = C.c_void_p()
-        L.check(lib().rg_matrix_create(dom.h, C.byref(self.h)))
+        if block_size == 1:
+            L.check(lib().rg_matrix_create(dom.h, C.byref(self.h)))
+        else:
+            L.check(lib().rg_matrix_create_system(dom.h, block_size, C.byref(self.h)))
 
     def values(self):
         p = C.c_void_p()
         L.check(lib().rg_matrix_values(self.h, C.byref(p)))
         torch.cuda.synchronize()
-        return _raw(p.value, self.dom.nnz).clone().cpu().numpy()
+        return _raw(p.value, self.dom.nnz * self.nb * self.nb).clone().cpu().numpy()
 
     def __del__(self):
         if getattr(self, "h", None):
@@ -88,6 +92,13 @@ def assemble(mat, rhs_t, keep, **coefs):
     cs = [coef(*coefs[k], keep) if k in coefs else L.rg_coef(None, 0) for k in "ABCDXY"]
     L.set_stream_from_torch()
     L.check(lib().rg_assemble_single(mat.h if mat else None, ptr(rhs_t), *[C.byref(c) for c in cs]))
+
+
+def assemble_system(mat, rhs_t, keep, **coefs):
+    """coefs: name -> (array, kind) for A,B,C,D,X,Y of a PDE system."""
+    cs = [coef(*coefs[k], keep) if k in coefs else L.rg_coef(None, 0) for k in "ABCDXY"]
+    L.set_stream_from_torch()
+    L.check(lib().rg_assemble_system(mat.h, ptr(rhs_t), *[C.byref(c) for c in cs]))
 
 
 def assemble_reduced(mat, rhs_t, keep, **coefs):

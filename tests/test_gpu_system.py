@@ -1,0 +1,122 @@
+"""PDE systems (block size 2 and 3) on the GPU against the reference's own outputs
+(assemblePDESystem golden vectors; the Lame solve with paso's Solver/PCG and block Jacobi)
+and against the CPU oracle (block SpMV, constraint)."""
+import numpy as np
+import pytest
+import torch
+
+import rgcapi as R
+from oracle import oracle as O
+from esys_b200 import _lib as L
+
+pytestmark = pytest.mark.gpu
+ASM_TOL = 1e-12
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+@pytest.mark.parametrize("kname", ["const", "exp"])
+def test_system_assembly_matches_reference(cuda, golden, dim, kname):
+    tag = f"{dim}d"
+    ne = tuple(int(v) for v in golden[f"asm{tag}_ne"])
+    dx = golden[f"asm{tag}_dx"]
+    nb = int(golden[f"sys{tag}_nb"])
+    d = R.Domain(dim, ne, x1=[dx[k] * ne[k] for k in range(dim)])
+    m = R.Matrix(d, nb)
+    rhs = torch.zeros(d.n * nb, dtype=torch.float64, device="cuda")
+    keep = []
+    R.assemble_system(m, rhs, keep, **{k: (golden[f"sys{tag}_{kname}_{k}"], R.KINDS[kname]) for k in "ABCDXY"})
+    ref = golden[f"sys{tag}_{kname}_val"]
+    assert np.abs(m.values() - ref).max() <= ASM_TOL * np.abs(ref).max()
+    ref_rhs = golden[f"sys{tag}_{kname}_rhs"]
+    assert np.abs(rhs.cpu().numpy() - ref_rhs).max() <= ASM_TOL * np.abs(ref_rhs).max()
+
+
+def _lame(golden, dim):
+    tag = f"{dim}d"
+    ne = tuple(int(v) for v in golden[f"lame{tag}_ne"])
+    d = R.Domain(dim, ne)
+    m = R.Matrix(d, dim)
+    rhs = torch.zeros(d.n * dim, dtype=torch.float64, device="cuda")
+    keep = []
+    R.assemble_system(m, rhs, keep, A=(golden[f"lame{tag}_A"], R.KINDS["const"]),
+                      Y=(golden[f"lame{tag}_Y"], R.KINDS["exp"]))
+    q = R.dev(golden[f"lame{tag}_q"])
+    R.insert_constraint(m, rhs, q)
+    return d, m, rhs
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_lame_solve_matches_reference(cuda, golden, dim):
+    """paso Solver + PCG with block Jacobi, tol 1e-10: iterations within 1 of the reference's,
+    solution within 1e-8."""
+    d, m, rhs = _lame(golden, dim)
+    x = torch.zeros(d.n * dim, dtype=torch.float64, device="cuda")
+    st, dg = R.solve(m, rhs, x, R.opts(tolerance=1e-10))
+    assert st == 0 and dg.converged
+    assert abs(int(dg.num_iter) - int(golden[f"lame{dim}d_iter"])) <= 1
+    ref = golden[f"lame{dim}d_x"]
+    assert np.linalg.norm(x.cpu().numpy() - ref) / np.linalg.norm(ref) < 1e-8
+    # the residual of the assembled (unbalanced) system
+    l2, lm = C_norms(m, rhs, x)
+    assert l2 <= 1e-8 * float(rhs.norm())
+
+
+def C_norms(m, rhs, x):
+    import ctypes as C
+    l2, lm = C.c_double(), C.c_double()
+    L.check(R.lib().rg_residual_norms(m.h, R.ptr(rhs), R.ptr(x), C.byref(l2), C.byref(lm)))
+    return l2.value, lm.value
+
+
+@pytest.mark.parametrize("dim,nb", [(2, 2), (3, 3), (3, 2), (2, 3)])
+def test_block_spmv_and_constraint_match_oracle(cuda, dim, nb):
+    rng = np.random.default_rng(7 + nb)
+    ne = (5, 4) if dim == 2 else (3, 4, 2)
+    dx = tuple(1.0 / e for e in ne)
+    pat = O.pattern(dim, ne)
+    nel = int(np.prod(ne))
+    nq = 1 << dim
+    A = rng.standard_normal(nb * nb * dim * dim * nq * nel)
+    D = rng.standard_normal(nb * nb)
+    Y = rng.standard_normal(nb)
+    val, rhs = O.assemble_system(dim, ne, dx, pat, nb, A=(O.EXPANDED, A), D=(O.CONSTANT, D), Y=(O.CONSTANT, Y))
+    d = R.Domain(dim, ne)
+    m = R.Matrix(d, nb)
+    r_t = torch.zeros(d.n * nb, dtype=torch.float64, device="cuda")
+    keep = []
+    R.assemble_system(m, r_t, keep, A=(A, R.KINDS["exp"]), D=(D, R.KINDS["const"]), Y=(Y, R.KINDS["const"]))
+    xv = rng.standard_normal(d.n * nb)
+    y = torch.zeros(d.n * nb, dtype=torch.float64, device="cuda")
+    L.check(R.lib().rg_spmv(m.h, 1.0, R.ptr(R.dev(xv)), 0.0, R.ptr(y)))
+    ref = O.spmv_block(pat, nb, val, xv)
+    assert np.abs(y.cpu().numpy() - ref).max() <= 1e-12 * np.abs(ref).max()
+    # constraint with r on a random half of the components
+    q = (rng.random(d.n * nb) < 0.3).astype(np.float64)
+    rr = rng.standard_normal(d.n * nb)
+    O.insert_constraint_block(pat, nb, val, rhs, q, rr)
+    R.insert_constraint(m, r_t, R.dev(q), R.dev(rr))
+    assert np.abs(m.values() - val).max() <= 1e-12 * np.abs(val).max()
+    assert np.abs(r_t.cpu().numpy() - rhs).max() <= 1e-12 * np.abs(rhs).max()
+
+
+def test_system_known_answer_and_unsupported_paths(cuda):
+    """A = I per component, coupled D, Y = row sums of D: u = 1.  FP32 refinement and the
+    batched solver refuse PDE systems."""
+    dim, nb, ne = 3, 3, (4, 3, 5)
+    d = R.Domain(dim, ne)
+    m = R.Matrix(d, nb)
+    A = np.zeros((nb, dim, nb, dim))
+    for k in range(nb):
+        for i in range(dim):
+            A[k, i, k, i] = 1.0
+    D = np.array([[2.0, -1.0, 0.0], [-1.0, 2.0, -1.0], [0.0, -1.0, 2.0]])
+    rhs = torch.zeros(d.n * nb, dtype=torch.float64, device="cuda")
+    keep = []
+    R.assemble_system(m, rhs, keep, A=(A.reshape(-1, order="F"), R.KINDS["const"]),
+                      D=(D.reshape(-1, order="F"), R.KINDS["const"]), Y=(D.sum(axis=1), R.KINDS["const"]))
+    x = torch.zeros(d.n * nb, dtype=torch.float64, device="cuda")
+    st, dg = R.solve(m, rhs, x, R.opts(tolerance=1e-10))
+    assert st == 0
+    assert float((x - 1.0).abs().max()) < 1e-8
+    st, _ = R.solve(m, rhs, x, R.opts(precision=L.RG_PREC_FP32_REFINE))
+    assert st == L.RG_NOT_SUPPORTED
