@@ -692,12 +692,27 @@ class SolverBuddy:
 class SystemMatrix:
     """Operator returned by LinearPDE.getSystem(): a paso CSR matrix on the GPU."""
 
-    def __init__(self, domain):
+    def __init__(self, domain, block_size=1):
         self._domain = domain
+        self._nb = int(block_size)
         h = C.c_void_p()
         L.set_stream_from_torch()
-        L.check(L.lib().rg_matrix_create(domain._handle, C.byref(h)))
+        if self._nb == 1:
+            L.check(L.lib().rg_matrix_create(domain._handle, C.byref(h)))
+        else:
+            L.check(L.lib().rg_matrix_create_system(domain._handle, self._nb, C.byref(h)))
         self._handle = h
+
+    def _new_vector(self):
+        if self._nb == 1:
+            return Scalar(0.0, Solution(self._domain), expanded=True)
+        return Data(0.0, (self._nb,), Solution(self._domain), expanded=True)
+
+    def getRowBlockSize(self):
+        return self._nb
+
+    def getColumnBlockSize(self):
+        return self._nb
 
     def __del__(self):
         h = getattr(self, "_handle", None)
@@ -720,7 +735,7 @@ class SystemMatrix:
         """The nnz CSR values as a CUDA tensor view (device memory owned by the matrix)."""
         p = C.c_void_p()
         L.check(L.lib().rg_matrix_values(self._handle, C.byref(p)))
-        return _tensor_from_ptr(p.value, self._domain._nnz, torch.float64)
+        return _tensor_from_ptr(p.value, self._domain._nnz * self._nb * self._nb, torch.float64)
 
     def nullifyRowsAndCols(self, row_q, col_q, mdv):
         r = row_q.interpolate(Solution(self._domain)) if row_q._fs._storage() != "nodes" else row_q
@@ -732,7 +747,7 @@ class SystemMatrix:
 
     def __mul__(self, u):
         """AbstractSystemMatrix.__mul__ -> vectorMultiply: y = A u."""
-        out = Scalar(0.0, Solution(self._domain), expanded=True)
+        out = self._new_vector()
         x = u._dev(self._domain._n) if u._fs._storage() == "nodes" else None
         if x is None:
             raise ValueError("matrix vector product: function space of input does not match")
@@ -748,7 +763,7 @@ class SystemMatrix:
 
     def solve(self, rhs, options=None):
         options = SolverBuddy() if options is None else options
-        out = Scalar(0.0, Solution(self._domain), expanded=True)
+        out = self._new_vector()
         self.setToSolution(out, rhs, options)
         return out
 
@@ -814,10 +829,17 @@ class LinearPDE:
     + d u = n_i X_i + y on the boundary and u = r where q > 0 (single equation)."""
 
     def __init__(self, domain, numEquations=None, numSolutions=None, isComplex=False, debug=False):
-        if numEquations not in (None, 1) or numSolutions not in (None, 1):
-            raise NotImplementedError("PDE systems are not part of the GPU path")
+        ne = numEquations if numEquations is not None else numSolutions
+        ns = numSolutions if numSolutions is not None else ne
+        ne = 1 if ne is None else int(ne)
+        ns = 1 if ns is None else int(ns)
+        if ne != ns:
+            raise ValueError("number of equations and number of solutions don't match")
+        if ne > 3:
+            raise NotImplementedError("PDE systems of more than 3 equations are not part of the GPU path")
         if isComplex:
             raise NotImplementedError("complex PDEs are not part of the GPU path")
+        self._nb = ne
         self._domain = domain
         self._coef = {}
         self._options = SolverBuddy()
@@ -837,10 +859,10 @@ class LinearPDE:
         return self._domain.getDim()
 
     def getNumEquations(self):
-        return 1
+        return self._nb
 
     def getNumSolutions(self):
-        return 1
+        return self._nb
 
     def getSolverOptions(self):
         return self._options
@@ -876,15 +898,22 @@ class LinearPDE:
         raise ValueError(f"unknown coefficient {name}")
 
     def _shape_of(self, name):
-        d = self.getDim()
-        return {"A": (d, d), "B": (d,), "C": (d,), "D": (), "X": (d,), "Y": (), "d": (),
-                "y": (), "q": (), "r": ()}[name[:-len("_reduced")] if name.endswith("_reduced") else name]
+        d, n = self.getDim(), self._nb
+        base = name[:-len("_reduced")] if name.endswith("_reduced") else name
+        if n == 1:
+            return {"A": (d, d), "B": (d,), "C": (d,), "D": (), "X": (d,), "Y": (), "d": (),
+                    "y": (), "q": (), "r": ()}[base]
+        # LinearPDE coefficient shapes of a system (linearPDEs.py: A (n, d, n, d), ...)
+        return {"A": (n, d, n, d), "B": (n, d, n), "C": (n, n, d), "D": (n, n), "X": (n, d), "Y": (n,),
+                "d": (n, n), "y": (n,), "q": (n,), "r": (n,)}[base]
 
     def createSolution(self):
-        return Scalar(0.0, Solution(self._domain), expanded=True)
+        if self._nb == 1:
+            return Scalar(0.0, Solution(self._domain), expanded=True)
+        return Data(0.0, (self._nb,), Solution(self._domain), expanded=True)
 
     def createRightHandSide(self):
-        return Scalar(0.0, Solution(self._domain), expanded=True)
+        return self.createSolution()
 
     def getCoefficient(self, name):
         if name in self._coef:
@@ -902,6 +931,9 @@ class LinearPDE:
                 raise NotImplementedError(f"coefficient {name} is not part of the GPU path")
             if name not in _INTERIOR + _REDUCED + _BOUNDARY + _CONSTRAINT:
                 raise ValueError(f"illegal coefficient {name} requested for general PDE.")
+            if self._nb > 1 and name in _REDUCED + _BOUNDARY and not (
+                    value is None or (isinstance(value, Data) and value.isEmpty())):
+                raise NotImplementedError(f"coefficient {name} of a PDE system is not part of the GPU path")
             if value is None or (isinstance(value, Data) and value.isEmpty()):
                 self._coef.pop(name, None)
             else:
@@ -943,7 +975,24 @@ class LinearPDE:
             return self._operator, self._rhs
         keep = []
         lib = L.lib()
-        if not self._operator_valid:
+        if not self._operator_valid and self._nb > 1:
+            # PDE system: interior terms (assemblePDESystem) and the constraint
+            self._operator = SystemMatrix(self._domain, self._nb)
+            self._rhs = self.createRightHandSide()
+            L.set_stream_from_torch()
+            cs = [self._coef_c(n, keep) for n in _INTERIOR]
+            L.check(lib.rg_assemble_system(self._operator._handle, C.c_void_p(self._rhs._t.data_ptr()),
+                                           *[C.byref(c) for c in cs]))
+            self._insert_constraint(rhs_only=False)
+        elif self._nb > 1:
+            self._rhs = self.createRightHandSide()
+            L.set_stream_from_torch()
+            empty = L.rg_coef(None, L.RG_COEF_EMPTY)
+            cs = [empty, empty, empty, empty, self._coef_c("X", keep), self._coef_c("Y", keep)]
+            L.check(lib.rg_assemble_system(self._operator._handle, C.c_void_p(self._rhs._t.data_ptr()),
+                                           *[C.byref(c) for c in cs]))
+            self._insert_constraint(rhs_only=True)
+        elif not self._operator_valid:
             self._operator = SystemMatrix(self._domain)
             self._rhs = self.createRightHandSide()
             L.set_stream_from_torch()

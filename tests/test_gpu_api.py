@@ -109,7 +109,9 @@ def test_rhs_only_change_reuses_operator(cuda):
 def test_unsupported_features_raise(cuda):
     dom = ripley.Rectangle(4, 4)
     with pytest.raises(NotImplementedError):
-        LinearPDE(dom, numEquations=2)
+        LinearPDE(dom, numEquations=4)
+    with pytest.raises(ValueError):
+        LinearPDE(dom, numEquations=2, numSolutions=3)
     pde = LinearPDE(dom)
     with pytest.raises(NotImplementedError):
         pde.setValue(y_reduced=1.0)
@@ -144,3 +146,42 @@ def test_function_space_coordinates(cuda):
     # interpolation of a linear field to the Gauss points is exact
     lin = Data(Solution(dom).getX()[0] * 2.0 + Solution(dom).getX()[2], Function(dom))
     assert np.allclose(lin.toNumpy(), 2 * xq[:, 0] + xq[:, 2])
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_lame_system_through_linear_pde(cuda, golden, dim):
+    """LinearPDE(numEquations=dim) with A = Lame tensor, Y on Function, u = 0 on the bottom
+    face: the reference's solution (paso PCG + block Jacobi) to 1e-8."""
+    import torch
+    from esys_b200.escript import Vector, Function
+    tag = f"{dim}d"
+    ne = tuple(int(v) for v in golden[f"lame{tag}_ne"])
+    dom = ripley.Rectangle(*ne) if dim == 2 else ripley.Brick(*ne)
+    pde = LinearPDE(dom, numEquations=dim)
+    assert pde.getNumEquations() == dim and pde.getNumSolutions() == dim
+    A = golden[f"lame{tag}_A"].reshape((dim,) * 4, order="F")
+    Y = Data._wrap(torch.as_tensor(golden[f"lame{tag}_Y"], device="cuda").reshape(-1, dim), (dim,), Function(dom))
+    x = ContinuousFunction(dom).getX()
+    q = whereZero(x[dim - 1]) * np.ones(dim)
+    pde.setValue(A=A, Y=Y, q=q)
+    pde.getSolverOptions().setTolerance(1e-10)
+    u = pde.getSolution()
+    ref = golden[f"lame{tag}_x"]
+    got = u._dev().reshape(-1).cpu().numpy()
+    assert np.linalg.norm(got - ref) / np.linalg.norm(ref) < 1e-8
+    assert abs(pde.getSolverOptions().getDiagnostics("num_iter") - int(golden[f"lame{tag}_iter"])) <= 1
+
+
+def test_system_coupled_known_answer(cuda):
+    dom = ripley.Brick(4, 3, 5)
+    pde = LinearPDE(dom, numEquations=3)
+    A = np.zeros((3, 3, 3, 3))
+    for k in range(3):
+        for i in range(3):
+            A[k, i, k, i] = 1.0
+    D = np.array([[2.0, -1.0, 0.0], [-1.0, 2.0, -1.0], [0.0, -1.0, 2.0]])
+    pde.setValue(A=A, D=D, Y=D.sum(axis=1))
+    u = pde.getSolution()
+    assert float((u._dev() - 1.0).abs().max()) < 1e-8
+    with pytest.raises(NotImplementedError):
+        pde.setValue(d=np.eye(3))
