@@ -846,8 +846,7 @@ __global__ void __launch_bounds__(kThreads) k_f32_update(int64_t n, float* __res
     const float* __restrict__ p = (s->pk & 1) ? P0 : P1;  // the direction just formed
     double v[2] = {0.0, 0.0};
     const int64_t nv = n >> 2;
-    for (int64_t k = gtid(); k < nv; k += gstride()) {
-        const float4 d0 = ld4(d, k), r0 = ld4(r, k), q0 = ld4(q, k), p0 = ld4(p, k), di = ld4(dinv, k);
+    auto body = [&](int64_t k, float4 d0, float4 r0, float4 q0, float4 p0, float4 di) {
         st4(d, k, make_float4(fmaf(alpha, p0.x, d0.x), fmaf(alpha, p0.y, d0.y), fmaf(alpha, p0.z, d0.z),
                               fmaf(alpha, p0.w, d0.w)));
         const float4 rn = make_float4(fmaf(-alpha, q0.x, r0.x), fmaf(-alpha, q0.y, r0.y),
@@ -857,7 +856,19 @@ __global__ void __launch_bounds__(kThreads) k_f32_update(int64_t n, float* __res
         st4(z, k, zn);
         v[0] += (double)zn.x * rn.x + (double)zn.y * rn.y + (double)zn.z * rn.z + (double)zn.w * rn.w;
         v[1] += (double)rn.x * rn.x + (double)rn.y * rn.y + (double)rn.z * rn.z + (double)rn.w * rn.w;
+    };
+    // two float4 groups per trip with all ten loads issued first: the inputs are mostly L2
+    // hits, and the kernel is bound by load latency rather than bandwidth
+    const int64_t st = gstride();
+    int64_t k = gtid();
+    for (; k + st < nv; k += 2 * st) {
+        const int64_t k2 = k + st;
+        const float4 d0 = ld4(d, k), r0 = ld4(r, k), q0 = ld4(q, k), p0 = ld4(p, k), di0 = ld4(dinv, k);
+        const float4 d1 = ld4(d, k2), r1 = ld4(r, k2), q1 = ld4(q, k2), p1 = ld4(p, k2), di1 = ld4(dinv, k2);
+        body(k, d0, r0, q0, p0, di0);
+        body(k2, d1, r1, q1, p1, di1);
     }
+    if (k < nv) body(k, ld4(d, k), ld4(r, k), ld4(q, k), ld4(p, k), ld4(dinv, k));
     if (gtid() < (n & 3)) {
         const int64_t i = (nv << 2) + gtid();
         d[i] = fmaf(alpha, p[i], d[i]);
