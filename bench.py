@@ -450,6 +450,13 @@ def run_ours(args):
 
     kernels = {k: {"launches_per_step": v[0] // n_prof, "ms_per_step": round(v[2] / n_prof, 3)}
                for k, v in tm.items() if v[0]}
+    cfg, ug = C.c_int(), C.c_int()
+    spmv_us = (C.c_double * 2)()
+    lib.rg_solver_config(mat, C.byref(cfg), C.byref(ug), spmv_us)
+    spmv_names = {0: "k_f32_spmv_tma<27, 3 stages>", 1: "k_f32_spmv_tma<27, 2 stages x 2 CTAs/SM>"}
+    roofline["kernel"] = spmv_names.get(cfg.value, roofline["kernel"])
+    roofline["tuned"] = {"spmv_config": cfg.value, "update_grid": ug.value,
+                         "spmv_us_per_config": [round(v, 2) for v in spmv_us]}
 
     # --- batched workload: 64 Bricks with edges from {32,48,64,80,96} per axis, 8 right hand
     # sides each, FP32-inner/FP64-refinement PCG to rtol 1e-8, one batch (timed separately)

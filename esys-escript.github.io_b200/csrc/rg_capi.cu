@@ -477,6 +477,18 @@ void rg_solver_opts_default(rg_solver_opts* o)
     o->inner_tolerance = 1e-2;
 }
 
+int rg_solver_config(const rg_matrix* mat, int* spmv_config, int* update_grid, double* spmv_us)
+{
+    RG_REQUIRE(mat, "rg_solver_config: NULL matrix");
+    return rg::solver_config(&mat->m, spmv_config, update_grid, spmv_us);
+}
+
+int rg_solver_set_config(rg_matrix* mat, int spmv_config)
+{
+    RG_REQUIRE(mat, "rg_solver_set_config: NULL matrix");
+    return rg::solver_set_config(&mat->m, spmv_config);
+}
+
 int rg_solve(rg_matrix* mat, const double* rhs, double* x, const rg_solver_opts* opts, rg_diag* diag)
 {
     RG_REQUIRE(mat && rhs && x, "rg_solve: NULL argument");

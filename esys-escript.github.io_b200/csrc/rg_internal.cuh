@@ -81,6 +81,7 @@ struct Matrix {
     bool solver_ready = false;
     double* dinv = nullptr;    // 1 / balanced diagonal
     float* band32 = nullptr;   // [nbands][npad] FP32 copy of the balanced matrix
+    int force_spmv = -1;       // FP32 SpMV configuration fixed by the caller (-1: tuned)
     float* dinv32 = nullptr;
     Workspace* ws = nullptr;
     ResidualScratch* rs = nullptr;
@@ -225,6 +226,10 @@ int solve(Matrix* m, const double* rhs, double* x, const rg_solver_opts* o, rg_d
 // balance the matrix in place (first time) and build its solver data, the FP32 band copy
 // included when `band` (what rg_solve does before iterating)
 int solver_prepare(Matrix* m, bool band);
+// the FP32 path's tuned configuration (see rg_solver_config)
+int solver_config(const Matrix* m, int* spmv_cfg, int* update_grid, double* spmv_us);
+// fixes the FP32 SpMV configuration (-1: tune at the next FP32 solve)
+int solver_set_config(Matrix* m, int spmv_cfg);
 void free_workspace(Matrix* m);
 // PDE systems (rg_system.cu): block size m->nb in {2, 3}
 int assemble_system_impl(const Domain* d, int nb, double* val, double* rhs, const rg_coef* c[6]);

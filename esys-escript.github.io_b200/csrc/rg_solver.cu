@@ -77,6 +77,7 @@ struct Workspace {
     long long graph_launches[3][T_COUNT] = {};
     int spmv_cfg = -1;   // FP32 band SpMV pipeline: 0 = 3 stages x 1 CTA/SM, 1 = 2 stages x 2 CTAs/SM
     int grid_upd32 = 0;  // CTAs of k_f32_update (tuned with the SpMV; 0 = grid_vec)
+    double spmv_us[2] = {0, 0};  // tuner's time per launch of each SpMV configuration
 };
 
 namespace {
@@ -1165,7 +1166,7 @@ int tune_spmv(Matrix* m)
     Workspace* w = m->ws;
     if (w->spmv_cfg >= 0) return RG_OK;
     if (timers_on()) {  // keep the timed launch counts clean: default configuration
-        w->spmv_cfg = 0;
+        w->spmv_cfg = m->force_spmv >= 0 ? m->force_spmv : 0;
         return RG_OK;
     }
     // every timed launch does the full work: z = 1, p = 0, beta = 0 (q = A 1, p.q > 0)
@@ -1196,6 +1197,7 @@ int tune_spmv(Matrix* m)
         RG_CHECK_CUDA(cudaEventSynchronize(e1));
         float ms = 0;
         cudaEventElapsedTime(&ms, e0, e1);
+        w->spmv_us[cfg] = 1e3 * ms / 8;
         if (rc == RG_OK && ms < best) {
             best = ms;
             best_cfg = cfg;
@@ -1203,6 +1205,7 @@ int tune_spmv(Matrix* m)
     }
     // the update kernel's grid: fewer CTAs shorten its reduction tail, more hide latency
     w->spmv_cfg = best_cfg;
+    if (m->force_spmv >= 0) w->spmv_cfg = m->force_spmv;
     const int64_t nv = (w->n + 3) / 4;
     float best_u = 1e30f;
     int best_grid = w->grid_vec;
@@ -1450,6 +1453,26 @@ int solve_f32(Matrix* m, const rg_solver_opts* o, OuterState& st, rg_diag& dg)
 }
 
 }  // namespace
+
+int solver_config(const Matrix* m, int* spmv_cfg, int* update_grid, double* spmv_us)
+{
+    if (spmv_us)
+        for (int c = 0; c < 2; ++c) spmv_us[c] = m->ws ? m->ws->spmv_us[c] : 0.0;
+    if (spmv_cfg) *spmv_cfg = m->ws ? m->ws->spmv_cfg : -1;
+    if (update_grid) *update_grid = m->ws ? m->ws->grid_upd32 : 0;
+    return RG_OK;
+}
+
+int solver_set_config(Matrix* m, int spmv_cfg)
+{
+    if (spmv_cfg < -1 || spmv_cfg > 1) {
+        set_error("rg_solver_set_config: spmv_config must be -1, 0 or 1");
+        return RG_INVALID_ARG;
+    }
+    m->force_spmv = spmv_cfg;
+    if (m->ws) m->ws->spmv_cfg = -1;  // re-tune (and apply) at the next FP32 solve
+    return RG_OK;
+}
 
 int solver_prepare(Matrix* m, bool band)
 {

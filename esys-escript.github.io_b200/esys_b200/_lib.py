@@ -97,9 +97,11 @@ _SIGNATURES = {
     "rg_save_mm": (C.c_int, [C.c_void_p, C.c_char_p]),
     "rg_residual_norms": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_double),
                                     C.POINTER(C.c_double)]),
+    "rg_solver_set_config": (C.c_int, [C.c_void_p, C.c_int]),
     "rg_residual_norms_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_double),
                                             C.POINTER(C.c_double)]),
     "rg_solver_opts_default": (None, [C.POINTER(rg_solver_opts)]),
+    "rg_solver_config": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_double)]),
     "rg_solve": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(rg_solver_opts),
                            C.POINTER(rg_diag)]),
     "rg_ws_conv3": (C.c_int, [C.POINTER(rg_act), C.c_void_p, C.c_void_p, C.POINTER(rg_act), C.c_int,

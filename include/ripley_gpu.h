@@ -213,6 +213,18 @@ int rg_solve(rg_matrix* mat, const double* rhs, double* x, const rg_solver_opts*
              rg_diag* diag);
 
 
+/* The FP32 path's configuration chosen at the matrix's first FP32_REFINE solve (no reference
+   counterpart; diagnostics and tests): spmv_config 0/1 = the band SpMV pipeline with 3 stages
+   x 1 CTA per SM / 2 stages x 2 CTAs per SM (-1: not tuned yet); update_grid: CTAs of the
+   vector update; spmv_us (NULL or 2 entries): the tuner's time per launch of each
+   configuration, 0 where not timed.  Any output pointer may be NULL. */
+int rg_solver_config(const rg_matrix* mat, int* spmv_config, int* update_grid, double* spmv_us);
+
+/* Fixes the FP32 SpMV configuration used from the next FP32_REFINE solve on (-1 restores the
+   tuner's choice).  The tuner still times both configurations, so rg_solver_config reports
+   them. */
+int rg_solver_set_config(rg_matrix* mat, int spmv_config);
+
 /* ---- batched solves (no reference counterpart: many independent systems at once) ------- */
 /* A batch holds assembled matrices of the same dimension (any sizes) that are solved
    together, each with nrhs right hand sides (1, 2, 4 or 8), by PCG + Jacobi with FP32 inner
