@@ -151,15 +151,25 @@ def assemble(dim, ne, dx, pat: Pattern, A=None, B=None, C_=None, D=None, X=None,
     return val, rhs
 
 
-def assemble_boundary(dim, ne, dx, pat: Pattern, val, rhs, d=None, y=None, use_ref=False):
+def assemble_boundary(dim, ne, dx, pat: Pattern, val, rhs, d=None, y=None, use_ref=False, nb=1, reduced=False):
+    """Face terms d, y added into val / rhs (block size nb; ``reduced``: one data point per
+    face element, ReducedFunctionOnBoundary)."""
     cd, _kd = _coef(d)
     cy, _ky = _coef(y)
+    general = nb != 1 or reduced
     if use_ref:
         R = ref()
-        rc = R.ref_assemble_boundary(dim, _i64x3(ne), _dx3(dx), _ip(pat.ptr), _ip(pat.idx),
-                                     _dp(val), _dp(rhs), cd.kind, cd.p, cy.kind, cy.p)
+        if general:
+            rc = R.ref_assemble_boundary_ex(dim, _i64x3(ne), _dx3(dx), int(nb), int(bool(reduced)), _ip(pat.ptr),
+                                            _ip(pat.idx), _dp(val), _dp(rhs), cd.kind, cd.p, cy.kind, cy.p)
+        else:
+            rc = R.ref_assemble_boundary(dim, _i64x3(ne), _dx3(dx), _ip(pat.ptr), _ip(pat.idx),
+                                         _dp(val), _dp(rhs), cd.kind, cd.p, cy.kind, cy.p)
         if rc:
             raise RuntimeError(R.ref_last_error().decode())
+    elif general:
+        lib().ro_assemble_boundary_ex(dim, _i64x3(ne), _dx3(dx), int(nb), int(bool(reduced)), _ip(pat.ptr),
+                                      _ip(pat.idx), _dp(val), _dp(rhs), cd, cy)
     else:
         lib().ro_assemble_boundary(dim, _i64x3(ne), _dx3(dx), _ip(pat.ptr), _ip(pat.idx),
                                    _dp(val), _dp(rhs), cd, cy)
@@ -248,8 +258,9 @@ def set_threads(n: int) -> None:
 # X (nb, dim), Y (nb), first index fastest (escript's layout).
 
 def assemble_system(dim, ne, dx, pat: Pattern, nb, A=None, B=None, C_=None, D=None, X=None, Y=None,
-                    use_ref=False):
-    """assemblePDESystem.  Returns (val (nnz nb^2), rhs (n nb))."""
+                    use_ref=False, reduced=False):
+    """assemblePDESystem (``reduced``: assemblePDESystemReduced, one data point per
+    element).  Returns (val (nnz nb^2), rhs (n nb))."""
     val = np.zeros(pat.nnz * nb * nb)
     rhs = np.zeros(pat.n * nb)
     coefs = [_coef(c) for c in (A, B, C_, D, X, Y)]
@@ -257,13 +268,14 @@ def assemble_system(dim, ne, dx, pat: Pattern, nb, A=None, B=None, C_=None, D=No
         R = ref()
         kinds = (C.c_int * 6)(*[c[0].kind for c in coefs])
         ptrs = (C.POINTER(C.c_double) * 6)(*[c[0].p for c in coefs])
-        rc = R.ref_assemble_system(dim, _i64x3(ne), _dx3(dx), int(nb), _ip(pat.ptr), _ip(pat.idx), _dp(val),
-                                   _dp(rhs), kinds, ptrs)
+        fn = R.ref_assemble_system_reduced if reduced else R.ref_assemble_system
+        rc = fn(dim, _i64x3(ne), _dx3(dx), int(nb), _ip(pat.ptr), _ip(pat.idx), _dp(val), _dp(rhs), kinds, ptrs)
         if rc:
             raise RuntimeError(R.ref_last_error().decode())
     else:
-        lib().ro_assemble_system(dim, _i64x3(ne), _dx3(dx), int(nb), _ip(pat.ptr), _ip(pat.idx), _dp(val),
-                                 _dp(rhs), *[c[0] for c in coefs])
+        fn = lib().ro_assemble_system_reduced if reduced else lib().ro_assemble_system
+        fn(dim, _i64x3(ne), _dx3(dx), int(nb), _ip(pat.ptr), _ip(pat.idx), _dp(val), _dp(rhs),
+           *[c[0] for c in coefs])
     return val, rhs
 
 

@@ -411,6 +411,80 @@ int ref_assemble_boundary(int dim, const int64_t ne[3], const double dx[3], cons
     return 0;
 }
 
+// face terms in general form: block size nb and, with `reduced`, ReducedFunctionOnBoundary
+// (one data point per face element): assemblePDEBoundarySingle / SingleReduced / System /
+// SystemReduced of DefaultAssembler{2,3}D
+int ref_assemble_boundary_ex(int dim, const int64_t ne[3], const double dx[3], int nb, int reduced,
+                             const int32_t* ptr, const int32_t* idx, double* val, double* rhs, int dkind,
+                             const double* d, int ykind, const double* y)
+{
+    try {
+        Geometry g;
+        make_geometry(g, dim, ne, dx);
+        const int nq = reduced ? 1 : 1 << (dim - 1);
+        escript::AbstractSystemMatrix S;
+        S.ptr = ptr;
+        S.idx = idx;
+        S.val = val;
+        S.nb = nb;
+        escript::Data rhsD(rhs, nb, 1, true);
+        escript::Data dD = make_coef(d, dkind, nb * nb, nq);
+        escript::Data yD = make_coef(y, ykind, nb, nq);
+        escript::AbstractSystemMatrix* M = val ? &S : nullptr;
+        if (dim == 3) {
+            ripley::DefaultAssembler3D<double> a(&g.dom, g.dx, g.NE, g.NN);
+            if (nb == 1 && !reduced) a.assemblePDEBoundarySingle(M, rhsD, dD, yD);
+            else if (nb == 1) a.assemblePDEBoundarySingleReduced(M, rhsD, dD, yD);
+            else if (!reduced) a.assemblePDEBoundarySystem(M, rhsD, dD, yD);
+            else a.assemblePDEBoundarySystemReduced(M, rhsD, dD, yD);
+        } else {
+            ripley::DefaultAssembler2D<double> a(&g.dom, g.dx, g.NE, g.NN);
+            if (nb == 1 && !reduced) a.assemblePDEBoundarySingle(M, rhsD, dD, yD);
+            else if (nb == 1) a.assemblePDEBoundarySingleReduced(M, rhsD, dD, yD);
+            else if (!reduced) a.assemblePDEBoundarySystem(M, rhsD, dD, yD);
+            else a.assemblePDEBoundarySystemReduced(M, rhsD, dD, yD);
+        }
+    } catch (const std::exception& e) {
+        snprintf(g_err, sizeof(g_err), "%s", e.what());
+        return 1;
+    }
+    return 0;
+}
+
+// assemblePDESystemReduced: the system terms on ReducedFunction (one data point per element)
+int ref_assemble_system_reduced(int dim, const int64_t ne[3], const double dx[3], int nb, const int32_t* ptr,
+                                const int32_t* idx, double* val, double* rhs, const int* kinds,
+                                const double* const* coefs)
+{
+    try {
+        Geometry g;
+        make_geometry(g, dim, ne, dx);
+        escript::AbstractSystemMatrix S;
+        S.ptr = ptr;
+        S.idx = idx;
+        S.val = val;
+        S.nb = nb;
+        escript::Data rhsD(rhs, nb, 1, true);
+        escript::Data A = make_coef(coefs[0], kinds[0], nb * nb * dim * dim, 1);
+        escript::Data B = make_coef(coefs[1], kinds[1], nb * nb * dim, 1);
+        escript::Data C = make_coef(coefs[2], kinds[2], nb * nb * dim, 1);
+        escript::Data D = make_coef(coefs[3], kinds[3], nb * nb, 1);
+        escript::Data X = make_coef(coefs[4], kinds[4], nb * dim, 1);
+        escript::Data Y = make_coef(coefs[5], kinds[5], nb, 1);
+        if (dim == 3) {
+            ripley::DefaultAssembler3D<double> a(&g.dom, g.dx, g.NE, g.NN);
+            a.assemblePDESystemReduced(val ? &S : nullptr, rhsD, A, B, C, D, X, Y);
+        } else {
+            ripley::DefaultAssembler2D<double> a(&g.dom, g.dx, g.NE, g.NN);
+            a.assemblePDESystemReduced(val ? &S : nullptr, rhsD, A, B, C, D, X, Y);
+        }
+    } catch (const std::exception& e) {
+        snprintf(g_err, sizeof(g_err), "%s", e.what());
+        return 1;
+    }
+    return 0;
+}
+
 // paso::Solver with PCG + Jacobi on a CSR matrix (balanced in place).
 // Returns the paso SolverResult, or -1 when a PasoException was thrown.
 int ref_solve(int64_t n, int32_t* ptr, int32_t* idx, double* val, double* b, double* x,

@@ -344,6 +344,101 @@ void ro_assemble_boundary(int dim, const int64_t ne[3], const double dx[3],
     }
 }
 
+/* The face terms in general form: block size nb (assemblePDEBoundarySystem,
+   DefaultAssembler3D.cpp:5753-6464; EM_S[k + nb (m + nb (r + nk c))] from
+   d[k + nb m] per data point, EM_F[k + nb r] from y[k]) and, with `reduced`, the 1-point
+   rule at the face centre with weight = face area (assemblePDEBoundarySingleReduced,
+   DefaultAssembler3D.cpp:3274-3628, assemblePDEBoundarySystemReduced, 6878-7255: d, y have
+   one data point per face element). */
+void ro_assemble_boundary_ex(int dim, const int64_t ne[3], const double dx[3], int nb, int reduced,
+                             const int32_t* ptr, const int32_t* idx, double* val, double* rhs,
+                             ro_coef d, ro_coef y)
+{
+    const int addS = d.kind != RO_EMPTY, addF = y.kind != RO_EMPTY;
+    if (!addS && !addF) return;
+    const double g2[2] = {0.5 - sqrt(3.0) / 6.0, 0.5 + sqrt(3.0) / 6.0};
+    const double g1[2] = {0.5, 0.5};
+    const double* g = reduced ? g1 : g2;
+    const int nk = 1 << dim;
+    const int nqf = reduced ? 1 : 1 << (dim - 1);
+    const int bs = nb * nb;
+    const int64_t NE[3] = {ne[0], ne[1], dim == 3 ? ne[2] : 1};
+    const int64_t NN0 = NE[0] + 1, NN1 = NE[1] + 1;
+    int64_t offset = 0;
+    for (int face = 0; face < 2 * dim; ++face) {
+        const int ax = face / 2, side = face % 2;
+        int fa[2] = {-1, -1}, nf = 0;
+        for (int a = 0; a < dim; ++a)
+            if (a != ax) fa[nf++] = a;
+        const int64_t n_a = NE[fa[0]], n_b = dim == 3 ? NE[fa[1]] : 1;
+        double area = 1.0;
+        for (int i = 0; i < nf; ++i) area *= dx[fa[i]];
+        const double W = area / nqf;
+        double Nf[4][8];
+        for (int q = 0; q < nqf; ++q)
+            for (int k = 0; k < nk; ++k) {
+                if (((k >> ax) & 1) != side) { Nf[q][k] = 0.0; continue; }
+                double v = 1.0;
+                for (int i = 0; i < nf; ++i) {
+                    const double xi = g[(q >> i) & 1];
+                    v *= ((k >> fa[i]) & 1) ? xi : 1.0 - xi;
+                }
+                Nf[q][k] = v;
+            }
+        for (int colour = 0; colour < 2; ++colour) {
+            const int64_t outer = dim == 3 ? n_b : n_a;
+#pragma omp parallel for schedule(static)
+            for (int64_t ko = colour; ko < outer; ko += 2) {
+                double EM_S[9 * 64], EM_F[3 * 8];
+                int64_t nodes[8];
+                const int64_t alo = dim == 3 ? 0 : ko, ahi = dim == 3 ? n_a : ko + 1;
+                const int64_t kb = dim == 3 ? ko : 0;
+                for (int64_t ka = alo; ka < ahi; ++ka) {
+                    const int64_t f = offset + ka + n_a * kb;
+                    int64_t k[3] = {0, 0, 0};
+                    k[ax] = side ? NE[ax] - 1 : 0;
+                    k[fa[0]] = ka;
+                    if (dim == 3) k[fa[1]] = kb;
+                    memset(EM_S, 0, sizeof(double) * (size_t)(bs * nk * nk));
+                    memset(EM_F, 0, sizeof(double) * (size_t)(nb * nk));
+                    for (int q = 0; q < nqf; ++q)
+                        for (int kk = 0; kk < nb; ++kk) {
+                            const double yq = addF ? coef_at(y, nb, nqf, f, kk, q) : 0.0;
+                            for (int r = 0; r < nk; ++r) {
+                                if (Nf[q][r] == 0.0) continue;
+                                EM_F[kk + nb * r] += W * yq * Nf[q][r];
+                                for (int m = 0; m < nb && addS; ++m) {
+                                    const double dq = coef_at(d, bs, nqf, f, kk + nb * m, q);
+                                    for (int c = 0; c < nk; ++c)
+                                        EM_S[kk + nb * (m + nb * (r + nk * c))] += W * dq * Nf[q][r] * Nf[q][c];
+                                }
+                            }
+                        }
+                    const int64_t first = k[0] + NN0 * k[1] + NN0 * NN1 * k[2];
+                    for (int m = 0; m < nk; ++m)
+                        nodes[m] = first + (m & 1) + ((m >> 1) & 1) * NN0 + ((m >> 2) & 1) * NN0 * NN1;
+                    if (addF && rhs)
+                        for (int r = 0; r < nk; ++r)
+                            for (int ir = 0; ir < nb; ++ir) rhs[nodes[r] * nb + ir] += EM_F[ir + nb * r];
+                    if (addS && val)
+                        for (int r = 0; r < nk; ++r)
+                            for (int c = 0; c < nk; ++c) {
+                                if (Nf[0][r] == 0.0 || Nf[0][c] == 0.0) continue;
+                                for (int64_t kk = ptr[nodes[r]]; kk < ptr[nodes[r] + 1]; ++kk)
+                                    if (idx[kk] == nodes[c]) {
+                                        for (int ic = 0; ic < nb; ++ic)
+                                            for (int ir = 0; ir < nb; ++ir)
+                                                val[kk * bs + ir + nb * ic] += EM_S[ir + nb * (ic + nb * (r + nk * c))];
+                                        break;
+                                    }
+                            }
+                }
+            }
+        }
+        offset += n_a * n_b;
+    }
+}
+
 /* ------------------------------------------------------------------------- */
 /* Brick::interpolateNodesOnElementsWorker (Brick.cpp:3355-3391) and the       */
 /* Rectangle analogue: trilinear (bilinear) interpolation to the Gauss points. */
@@ -755,12 +850,35 @@ static void element_system(const q1_tab* t, int nb, int64_t e, ro_coef A, ro_coe
         }
 }
 
+static void system_with(const q1_tab* tp, int dim, const int64_t ne[3], int nb, const int32_t* ptr,
+                        const int32_t* idx, double* val, double* rhs, ro_coef A, ro_coef B, ro_coef C,
+                        ro_coef D, ro_coef X, ro_coef Y);
+
 void ro_assemble_system(int dim, const int64_t ne[3], const double dx[3], int nb,
                         const int32_t* ptr, const int32_t* idx, double* val, double* rhs,
                         ro_coef A, ro_coef B, ro_coef C, ro_coef D, ro_coef X, ro_coef Y)
 {
     q1_tab t;
     q1_build(dim, dx, &t);
+    system_with(&t, dim, ne, nb, ptr, idx, val, rhs, A, B, C, D, X, Y);
+}
+
+/* DefaultAssembler3D::assemblePDESystemReduced (DefaultAssembler3D.cpp:6466-6876) and
+   DefaultAssembler2D::assemblePDESystemReduced: the system terms with the 1-point rule */
+void ro_assemble_system_reduced(int dim, const int64_t ne[3], const double dx[3], int nb,
+                                const int32_t* ptr, const int32_t* idx, double* val, double* rhs,
+                                ro_coef A, ro_coef B, ro_coef C, ro_coef D, ro_coef X, ro_coef Y)
+{
+    q1_tab t;
+    q1_build_reduced(dim, dx, &t);
+    system_with(&t, dim, ne, nb, ptr, idx, val, rhs, A, B, C, D, X, Y);
+}
+
+static void system_with(const q1_tab* tp, int dim, const int64_t ne[3], int nb, const int32_t* ptr,
+                        const int32_t* idx, double* val, double* rhs, ro_coef A, ro_coef B, ro_coef C,
+                        ro_coef D, ro_coef X, ro_coef Y)
+{
+    const q1_tab t = *tp;
     const int addS = A.kind || B.kind || C.kind || D.kind;
     const int addF = X.kind || Y.kind;
     if (!addS && !addF) return;

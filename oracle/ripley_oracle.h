@@ -70,6 +70,14 @@ void ro_assemble_boundary(int dim, const int64_t ne[3], const double dx[3],
                           const int32_t* ptr, const int32_t* idx, double* val, double* rhs,
                           ro_coef d, ro_coef y);
 
+/* The face terms for block size nb (1..3; d[k + nb m], y[k] per data point) and, with
+   `reduced`, on ReducedFunctionOnBoundary (one data point per face element, 1-point rule):
+   assemblePDEBoundarySystem / assemblePDEBoundarySingleReduced /
+   assemblePDEBoundarySystemReduced. */
+void ro_assemble_boundary_ex(int dim, const int64_t ne[3], const double dx[3], int nb, int reduced,
+                             const int32_t* ptr, const int32_t* idx, double* val, double* rhs,
+                             ro_coef d, ro_coef y);
+
 /* node -> Function (2^dim Gauss points) interpolation, Brick.cpp:3355-3391 */
 void ro_interpolate_nodes(int dim, const int64_t ne[3], const double* nodal, int ncomp,
                           double* out);
@@ -99,6 +107,10 @@ int ro_solve_cg(int64_t n, const int32_t* ptr, const int32_t* idx, const double*
 void ro_assemble_system(int dim, const int64_t ne[3], const double dx[3], int nb,
                         const int32_t* ptr, const int32_t* idx, double* val, double* rhs,
                         ro_coef A, ro_coef B, ro_coef C, ro_coef D, ro_coef X, ro_coef Y);
+/* assemblePDESystemReduced: the system terms with the 1-point rule (ReducedFunction) */
+void ro_assemble_system_reduced(int dim, const int64_t ne[3], const double dx[3], int nb,
+                                const int32_t* ptr, const int32_t* idx, double* val, double* rhs,
+                                ro_coef A, ro_coef B, ro_coef C, ro_coef D, ro_coef X, ro_coef Y);
 void ro_spmv_block(int64_t nodes, int nb, const int32_t* ptr, const int32_t* idx, const double* val,
                    double alpha, const double* x, double beta, double* y);
 void ro_insert_constraint_block(int64_t nodes, int nb, const int32_t* ptr, const int32_t* idx,

@@ -182,6 +182,46 @@ def main():
         g[f"lame{tag}_A"], g[f"lame{tag}_Y"], g[f"lame{tag}_q"] = A, Y, q
         g[f"lame{tag}_x"], g[f"lame{tag}_iter"] = res.x, np.array(res.num_iter)
 
+    # face terms of PDE systems and on ReducedFunctionOnBoundary, and the reduced-order
+    # system terms: assemblePDEBoundarySystem, assemblePDEBoundarySingleReduced,
+    # assemblePDEBoundarySystemReduced, assemblePDESystemReduced
+    rb = np.random.default_rng(20261206)
+    for dim, ne in ((2, (5, 7)), (3, (3, 4, 5))):
+        dx = tuple(0.3 + 0.2 * k for k in range(dim))
+        tag = f"{dim}d"
+        pat = O.pattern(dim, ne)
+        nel = int(np.prod(ne))
+        nface = 2 * ne[1] + 2 * ne[0] if dim == 2 else 2 * (ne[1] * ne[2] + ne[0] * ne[2] + ne[0] * ne[1])
+        for case, nb, reduced in (("bred", 1, True), ("bsys", dim, False), ("bsysred", dim, True)):
+            nq = 1 if reduced else 1 << (dim - 1)
+            for kname, kind in (("const", O.CONSTANT), ("exp", O.EXPANDED)):
+                cnt = 1 if kind == O.CONSTANT else nface * nq
+                d = rb.standard_normal(cnt * nb * nb)
+                y = rb.standard_normal(cnt * nb)
+                bval = np.zeros(pat.nnz * nb * nb)
+                brhs = np.zeros(pat.n * nb)
+                O.assemble_boundary(dim, ne, dx, pat, bval, brhs, d=(kind, d), y=(kind, y), use_ref=True, nb=nb,
+                                    reduced=reduced)
+                g[f"{case}{tag}_{kname}_d"], g[f"{case}{tag}_{kname}_y"] = d, y
+                g[f"{case}{tag}_{kname}_val"], g[f"{case}{tag}_{kname}_rhs"] = bval, brhs
+        nb = dim
+        sizes = {"A": nb * nb * dim * dim, "B": nb * nb * dim, "C": nb * nb * dim, "D": nb * nb, "X": nb * dim,
+                 "Y": nb}
+        for kname, kind in (("const", O.CONSTANT), ("exp", O.EXPANDED)):
+            cs = {k: rb.standard_normal(v if kind == O.CONSTANT else v * nel) for k, v in sizes.items()}
+            val, rhs = O.assemble_system(dim, ne, dx, pat, nb, use_ref=True, reduced=True,
+                                         **{("C_" if k == "C" else k): (kind, v) for k, v in cs.items()})
+            for k, v in cs.items():
+                g[f"sysred{tag}_{kname}_{k}"] = v
+            g[f"sysred{tag}_{kname}_val"] = val
+            g[f"sysred{tag}_{kname}_rhs"] = rhs
+
+    # arrays already in the committed file keep their values (the solve cases depend on the
+    # reference's OpenMP thread count at the 1e-13 level); new keys are added
+    if os.path.exists(out):
+        with np.load(out) as old:
+            kept = {k: old[k] for k in old.files}
+        g.update(kept)
     np.savez_compressed(out, **g)
     print(f"wrote {out}: {len(g)} arrays, {os.path.getsize(out) / 1024:.0f} KiB; "
           f"iterations r200={int(g['r200_iter'])} solve2d={int(g['solve2d_iter'])} "

@@ -317,3 +317,61 @@ def test_system_known_answer(dim, ne):
     res = O.solve_paso_block(pat, nb, val, rhs, tol=1e-10)
     assert res.status == 0
     assert np.abs(res.x - 1.0).max() < 1e-8
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+@pytest.mark.parametrize("case", ["bred", "bsys", "bsysred"])
+@pytest.mark.parametrize("kname,kind", [("const", O.CONSTANT), ("exp", O.EXPANDED)])
+def test_general_boundary_assembly_matches_reference(golden, dim, case, kname, kind):
+    """Face terms on ReducedFunctionOnBoundary (bred: assemblePDEBoundarySingleReduced) and
+    of PDE systems (bsys: assemblePDEBoundarySystem, bsysred: ...SystemReduced) against the
+    reference's own output."""
+    tag = f"{dim}d"
+    ne = tuple(golden[f"asm{tag}_ne"])
+    dx = tuple(golden[f"asm{tag}_dx"])
+    nb = 1 if case == "bred" else dim
+    pat = O.pattern(dim, ne)
+    val = np.zeros(pat.nnz * nb * nb)
+    rhs = np.zeros(pat.n * nb)
+    O.assemble_boundary(dim, ne, dx, pat, val, rhs, d=(kind, golden[f"{case}{tag}_{kname}_d"]),
+                        y=(kind, golden[f"{case}{tag}_{kname}_y"]), nb=nb, reduced=case != "bsys")
+    rv, rr = golden[f"{case}{tag}_{kname}_val"], golden[f"{case}{tag}_{kname}_rhs"]
+    assert np.abs(val - rv).max() <= ASM_TOL * np.abs(rv).max()
+    assert np.abs(rhs - rr).max() <= ASM_TOL * np.abs(rr).max()
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+@pytest.mark.parametrize("kname,kind", [("const", O.CONSTANT), ("exp", O.EXPANDED)])
+def test_system_reduced_assembly_matches_reference(golden, dim, kname, kind):
+    """assemblePDESystemReduced (block size dim, one data point per element)."""
+    tag = f"{dim}d"
+    ne = tuple(golden[f"asm{tag}_ne"])
+    dx = tuple(golden[f"asm{tag}_dx"])
+    pat = O.pattern(dim, ne)
+    cs = {("C_" if k == "C" else k): (kind, golden[f"sysred{tag}_{kname}_{k}"]) for k in "ABCDXY"}
+    val, rhs = O.assemble_system(dim, ne, dx, pat, dim, reduced=True, **cs)
+    ref = golden[f"sysred{tag}_{kname}_val"]
+    assert np.abs(val - ref).max() <= ASM_TOL * np.abs(ref).max()
+    ref_rhs = golden[f"sysred{tag}_{kname}_rhs"]
+    assert np.abs(rhs - ref_rhs).max() <= ASM_TOL * np.abs(ref_rhs).max()
+
+
+@pytest.mark.parametrize("dim,ne", [(2, (4, 6)), (3, (3, 2, 4))])
+@pytest.mark.parametrize("nb", [1, 2, 3])
+@pytest.mark.parametrize("reduced", [False, True])
+def test_boundary_integrals_known_answer(dim, ne, nb, reduced):
+    """Constant d = D (nb x nb) and y = v on every face: each block column sum of the
+    matrix is D times the boundary measure, the rhs component sums are v times it."""
+    dx = tuple(0.25 + 0.1 * k for k in range(dim))
+    L_ = [e * h for e, h in zip(ne, dx)]
+    area = 2 * (L_[0] + L_[1]) if dim == 2 else 2 * (L_[0] * L_[1] + L_[0] * L_[2] + L_[1] * L_[2])
+    rng = np.random.default_rng(nb + 10 * dim)
+    Dm = rng.standard_normal(nb * nb)
+    v = rng.standard_normal(nb)
+    pat = O.pattern(dim, ne)
+    val = np.zeros(pat.nnz * nb * nb)
+    rhs = np.zeros(pat.n * nb)
+    O.assemble_boundary(dim, ne, dx, pat, val, rhs, d=(O.CONSTANT, Dm), y=(O.CONSTANT, v), nb=nb, reduced=reduced)
+    blocks = val.reshape(pat.nnz, nb * nb).sum(axis=0)  # column-major blocks: ir + nb ic
+    assert np.allclose(blocks, Dm * area, rtol=1e-12, atol=1e-12)
+    assert np.allclose(rhs.reshape(pat.n, nb).sum(axis=0), v * area, rtol=1e-12, atol=1e-12)
