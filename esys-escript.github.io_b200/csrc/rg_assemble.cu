@@ -303,7 +303,13 @@ __global__ void __launch_bounds__(kRowsPerCta) k_assemble(const __grid_constant_
 // face terms d (matrix) and y (rhs) on FunctionOnBoundary.  Face f of axis ax, side s:
 // faces ordered left,right,bottom,top,front,back; face element (ka,kb) over the lower
 // and upper in-face axes has index offset_f + ka + NEa*kb; its Gauss points are
-// q = qa + 2*qb.  One thread per node; nodes off the boundary exit at once.
+// q = qa + 2*qb.  One thread per (node, equation k, component m); threads of nodes off the
+// boundary exit at once.  The same kernel covers
+//   * PDE systems, block size NBLK (assemblePDEBoundarySystem, DefaultAssembler3D.cpp:
+//     5753-6464): d[k + NBLK m] and y[k] per data point, blocks val[e NBLK^2 + k + NBLK m];
+//   * ReducedFunctionOnBoundary (assemblePDEBoundarySingleReduced, 3274-3628, and
+//     ...SystemReduced, 6878-7255): one data point per face element, the 1-point rule at the
+//     face centre with weight = face area.
 struct BndArgs {
     CoefArg d, y;
     double g[2];  // 1D Gauss points
@@ -316,12 +322,16 @@ struct BndArgs {
     double* rhs;
 };
 
-template <int DIM>
+template <int DIM, int NBLK, bool RED>
 __global__ void __launch_bounds__(128) k_assemble_boundary(const __grid_constant__ BndArgs a)
 {
     constexpr int NB = DIM == 3 ? 27 : 9;
-    constexpr int NQF = 1 << (DIM - 1);
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    constexpr int NQF = RED ? 1 : 1 << (DIM - 1);
+    constexpr int BS = NBLK * NBLK;
+    const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t i = tid / BS;
+    const int km = (int)(tid % BS);
+    const int k = km % NBLK, m = km / NBLK;
     if (i >= a.n) return;
     int64_t c3[3];
     c3[0] = i % a.NN[0];
@@ -331,6 +341,7 @@ __global__ void __launch_bounds__(128) k_assemble_boundary(const __grid_constant
 #pragma unroll
     for (int ax = 0; ax < DIM; ++ax) on |= (c3[ax] == 0) || (c3[ax] == a.NN[ax] - 1);
     if (!on) return;
+    const bool with_y = a.y.kind && m == 0;
     double acc[NB];
 #pragma unroll
     for (int b = 0; b < NB; ++b) acc[b] = 0.0;
@@ -350,45 +361,45 @@ __global__ void __launch_bounds__(128) k_assemble_boundary(const __grid_constant
                 const int64_t fe = a.face_off[face] + ka + na * kb;
                 const int r = (1 - sa) + (DIM == 3 ? 2 * (1 - sb) : 0);  // face-local node
                 for (int q = 0; q < NQF; ++q) {
-                    const double xa = a.g[q & 1], xb = a.g[(q >> 1) & 1];
+                    const double xa = RED ? 0.5 : a.g[q & 1], xb = RED ? 0.5 : a.g[(q >> 1) & 1];
                     double Nf[4];
-                    for (int k = 0; k < (DIM == 3 ? 4 : 2); ++k) {
-                        double w = (k & 1) ? xa : 1.0 - xa;
-                        if (DIM == 3) w *= ((k >> 1) & 1) ? xb : 1.0 - xb;
-                        Nf[k] = w;
+                    for (int kk = 0; kk < (DIM == 3 ? 4 : 2); ++kk) {
+                        double w = (kk & 1) ? xa : 1.0 - xa;
+                        if (DIM == 3) w *= ((kk >> 1) & 1) ? xb : 1.0 - xb;
+                        Nf[kk] = w;
                     }
-                    const double Wf = a.Wf[ax];
-                    if (a.y.kind) {
-                        const double* yp = a.y.kind == RG_COEF_EXPANDED ? a.y.p + fe * NQF + q
-                                         : a.y.kind == RG_COEF_PER_ELEMENT ? a.y.p + fe : a.y.p;
-                        facc = fma(Wf, __ldg(yp) * Nf[r], facc);
+                    const double Wf = RED ? a.Wf[ax] * (1 << (DIM - 1)) : a.Wf[ax];
+                    if (with_y) {
+                        const double* yp = a.y.kind == RG_COEF_EXPANDED ? a.y.p + (fe * NQF + q) * NBLK
+                                         : a.y.kind == RG_COEF_PER_ELEMENT ? a.y.p + fe * NBLK : a.y.p;
+                        facc = fma(Wf, __ldg(yp + k) * Nf[r], facc);
                     }
                     if (a.d.kind) {
-                        const double* dp = a.d.kind == RG_COEF_EXPANDED ? a.d.p + fe * NQF + q
-                                         : a.d.kind == RG_COEF_PER_ELEMENT ? a.d.p + fe : a.d.p;
-                        const double dr = __ldg(dp) * Nf[r];
-                        for (int k = 0; k < (DIM == 3 ? 4 : 2); ++k) {
+                        const double* dp = a.d.kind == RG_COEF_EXPANDED ? a.d.p + (fe * NQF + q) * BS
+                                         : a.d.kind == RG_COEF_PER_ELEMENT ? a.d.p + fe * BS : a.d.p;
+                        const double dr = __ldg(dp + k + NBLK * m) * Nf[r];
+                        for (int kk = 0; kk < (DIM == 3 ? 4 : 2); ++kk) {
                             int off[3] = {0, 0, 0};
-                            off[fa0] = (int)(ka + (k & 1) - u);
-                            if (DIM == 3) off[fa1] = (int)(kb + ((k >> 1) & 1) - v);
+                            off[fa0] = (int)(ka + (kk & 1) - u);
+                            if (DIM == 3) off[fa1] = (int)(kb + ((kk >> 1) & 1) - v);
                             const int b = (off[0] + 1) + 3 * (off[1] + 1) + (DIM == 3 ? 9 * (off[2] + 1) : 0);
-                            acc[b] = fma(Wf, dr * Nf[k], acc[b]);
+                            acc[b] = fma(Wf, dr * Nf[kk], acc[b]);
                         }
                     }
                 }
             }
     }
-    if (a.rhs && a.y.kind) a.rhs[i] += facc;
+    if (a.rhs && with_y) a.rhs[i * NBLK + k] += facc;
     if (a.val && a.d.kind) {
-        int64_t k = a.ptr[i];
+        int64_t e = a.ptr[i];
         for (int b = 0; b < NB; ++b) {
             const int bx = b % 3 - 1, by = (b / 3) % 3 - 1, bz = DIM == 3 ? b / 9 - 1 : 0;
             const bool in = c3[0] + bx >= 0 && c3[0] + bx < a.NN[0] && c3[1] + by >= 0 &&
                             c3[1] + by < a.NN[1] &&
                             (DIM == 2 || (c3[2] + bz >= 0 && c3[2] + bz < a.NN[2]));
             if (in) {
-                a.val[k] += acc[b];
-                ++k;
+                a.val[e * BS + k + NBLK * m] += acc[b];
+                ++e;
             }
         }
     }
@@ -487,7 +498,18 @@ int assemble_single_impl(const Domain* d, double* val, double* rhs, const rg_coe
     return RG_OK;
 }
 
-int assemble_boundary_impl(const Domain* d, double* val, double* rhs, const rg_coef* dc,
+template <int DIM, bool RED>
+void launch_boundary(const BndArgs& a, int nb, int grid)
+{
+    if (nb == 1)
+        RG_TIMED(T_BOUNDARY, (k_assemble_boundary<DIM, 1, RED><<<grid, 128, 0, stream()>>>(a)));
+    else if (nb == 2)
+        RG_TIMED(T_BOUNDARY, (k_assemble_boundary<DIM, 2, RED><<<grid, 128, 0, stream()>>>(a)));
+    else
+        RG_TIMED(T_BOUNDARY, (k_assemble_boundary<DIM, 3, RED><<<grid, 128, 0, stream()>>>(a)));
+}
+
+int assemble_boundary_impl(const Domain* d, int nb, bool reduced, double* val, double* rhs, const rg_coef* dc,
                            const rg_coef* yc)
 {
     BndArgs a;
@@ -524,11 +546,15 @@ int assemble_boundary_impl(const Domain* d, double* val, double* rhs, const rg_c
     a.ptr = d->ptr;
     a.val = val;
     a.rhs = rhs;
-    const int grid = (int)((d->n + 127) / 128);
-    if (d->dim == 3)
-        RG_TIMED(T_BOUNDARY, (k_assemble_boundary<3><<<grid, 128, 0, stream()>>>(a)));
+    const int grid = (int)((d->n * nb * nb + 127) / 128);
+    if (d->dim == 3 && !reduced)
+        launch_boundary<3, false>(a, nb, grid);
+    else if (d->dim == 3)
+        launch_boundary<3, true>(a, nb, grid);
+    else if (!reduced)
+        launch_boundary<2, false>(a, nb, grid);
     else
-        RG_TIMED(T_BOUNDARY, (k_assemble_boundary<2><<<grid, 128, 0, stream()>>>(a)));
+        launch_boundary<2, true>(a, nb, grid);
     RG_CHECK_LAUNCH();
     return RG_OK;
 }

@@ -347,8 +347,8 @@ int rg_assemble_single_reduced(rg_matrix* mat, double* rhs, const rg_coef* A, co
 {
     RG_REQUIRE(mat, "rg_assemble_single_reduced: a matrix handle is required (it names the domain)");
     if (mat->m.nb != 1) {
-        set_error("rg_assemble_single_reduced: reduced-order terms of PDE systems are not implemented");
-        return RG_NOT_SUPPORTED;
+        set_error("rg_assemble_single_reduced: the matrix is a PDE system; use rg_assemble_system_reduced");
+        return RG_INVALID_ARG;
     }
     const rg_coef* c[6] = {A, B, C, D, X, Y};
     for (int j = 0; j < 6; ++j) RG_REQUIRE(coef_ok(c[j]), "rg_assemble_single_reduced: invalid coefficient");
@@ -374,23 +374,52 @@ int rg_assemble_system(rg_matrix* mat, double* rhs, const rg_coef* A, const rg_c
         mat->m.solver_ready = false;
     }
     if (mat->m.nb == 1) return assemble_single_impl(mat->m.dom, mat->m.val, rhs, c, false);
-    return assemble_system_impl(mat->m.dom, mat->m.nb, mat->m.val, rhs, c);
+    return assemble_system_impl(mat->m.dom, mat->m.nb, mat->m.val, rhs, c, false);
+}
+
+int rg_assemble_system_reduced(rg_matrix* mat, double* rhs, const rg_coef* A, const rg_coef* B,
+                               const rg_coef* C, const rg_coef* D, const rg_coef* X, const rg_coef* Y)
+{
+    RG_REQUIRE(mat, "rg_assemble_system_reduced: a matrix handle is required (it names the domain and block size)");
+    const rg_coef* c[6] = {A, B, C, D, X, Y};
+    for (int j = 0; j < 6; ++j) RG_REQUIRE(coef_ok(c[j]), "rg_assemble_system_reduced: invalid coefficient");
+    const bool addS = (A && A->kind) || (B && B->kind) || (C && C->kind) || (D && D->kind);
+    if (addS) {
+        int rc = require_unbalanced(&mat->m, "rg_assemble_system_reduced");
+        if (rc) return rc;
+        mat->m.solver_ready = false;
+    }
+    if (mat->m.nb == 1) return assemble_single_impl(mat->m.dom, mat->m.val, rhs, c, true);
+    return assemble_system_impl(mat->m.dom, mat->m.nb, mat->m.val, rhs, c, true);
+}
+
+static int assemble_boundary_any(rg_matrix* mat, double* rhs, const rg_coef* d, const rg_coef* y, bool reduced,
+                                 const char* who)
+{
+    if (!mat) {
+        set_error(std::string(who) + ": a matrix handle is required");
+        return RG_INVALID_ARG;
+    }
+    if (!coef_ok(d) || !coef_ok(y)) {
+        set_error(std::string(who) + ": invalid coefficient");
+        return RG_INVALID_ARG;
+    }
+    if (d && d->kind) {
+        int rc = require_unbalanced(&mat->m, who);
+        if (rc) return rc;
+        mat->m.solver_ready = false;
+    }
+    return assemble_boundary_impl(mat->m.dom, mat->m.nb, reduced, mat->m.val, rhs, d, y);
 }
 
 int rg_assemble_boundary(rg_matrix* mat, double* rhs, const rg_coef* d, const rg_coef* y)
 {
-    RG_REQUIRE(mat, "rg_assemble_boundary: a matrix handle is required");
-    if (mat->m.nb != 1) {
-        set_error("rg_assemble_boundary: boundary terms of PDE systems are not implemented");
-        return RG_NOT_SUPPORTED;
-    }
-    RG_REQUIRE(coef_ok(d) && coef_ok(y), "rg_assemble_boundary: invalid coefficient");
-    if (d && d->kind) {
-        int rc = require_unbalanced(&mat->m, "rg_assemble_boundary");
-        if (rc) return rc;
-        mat->m.solver_ready = false;
-    }
-    return assemble_boundary_impl(mat->m.dom, mat->m.val, rhs, d, y);
+    return assemble_boundary_any(mat, rhs, d, y, false, "rg_assemble_boundary");
+}
+
+int rg_assemble_boundary_reduced(rg_matrix* mat, double* rhs, const rg_coef* d, const rg_coef* y)
+{
+    return assemble_boundary_any(mat, rhs, d, y, true, "rg_assemble_boundary_reduced");
 }
 
 int rg_insert_constraint(rg_matrix* mat, double* rhs, const double* q, const double* r, int rhs_only)

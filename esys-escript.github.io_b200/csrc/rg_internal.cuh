@@ -212,7 +212,7 @@ void timers_add(const long long delta[T_COUNT], long long times);
 // ---------------------------------------------------------------- entry points between units
 int launch_pattern(Domain* d);
 int assemble_single_impl(const Domain* d, double* val, double* rhs, const rg_coef* c[6], bool reduced);
-int assemble_boundary_impl(const Domain* d, double* val, double* rhs, const rg_coef* dc,
+int assemble_boundary_impl(const Domain* d, int nb, bool reduced, double* val, double* rhs, const rg_coef* dc,
                            const rg_coef* yc);
 int launch_interpolate(const Domain* d, const double* nodal, int ncomp, double* out, int reduced);
 int launch_insert_constraint(Matrix* m, double* rhs, const double* q, const double* r, int rhs_only);
@@ -232,7 +232,7 @@ int solver_config(const Matrix* m, int* spmv_cfg, int* update_grid, double* spmv
 int solver_set_config(Matrix* m, int spmv_cfg);
 void free_workspace(Matrix* m);
 // PDE systems (rg_system.cu): block size m->nb in {2, 3}
-int assemble_system_impl(const Domain* d, int nb, double* val, double* rhs, const rg_coef* c[6]);
+int assemble_system_impl(const Domain* d, int nb, double* val, double* rhs, const rg_coef* c[6], bool reduced);
 int launch_system_constraint(Matrix* m, double* rhs, const double* q, const double* r, int rhs_only);
 int launch_system_nullify(Matrix* m, const double* mr, const double* mc, double diag);
 int launch_system_spmv(const Matrix* m, double alpha, const double* x, double beta, double* y);

@@ -111,11 +111,11 @@ __device__ __forceinline__ const double* cptr(const CoefArg& c, int64_t e, int q
 //   f     = sum_q W (X_ki G_Ri + Y_k N_R)   (for m == 0)
 // layouts A[k + NB (i + DIM (m + NB j))], B[k + NB (i + DIM m)], C[k + NB (m + NB j)],
 // D[k + NB m], X[k + NB i], Y[k]
-template <int DIM, int NB, int R>
+template <int DIM, int NB, int NQ, int R>
 __device__ __forceinline__ void element_row(const SysArgs& a, int64_t e, int k, int m, double (&em)[1 << DIM],
                                             double& f)
 {
-    constexpr int NK = 1 << DIM, NQ = 1 << DIM;
+    constexpr int NK = 1 << DIM;
     constexpr int SA = NB * DIM * NB * DIM, SB = NB * DIM * NB, SC = NB * NB * DIM, SD = NB * NB;
     constexpr int SX = NB * DIM, SY = NB;
     const CoefArg& A = a.c[0];
@@ -179,7 +179,7 @@ __host__ __device__ constexpr int band_of(int sx, int sy, int sz, int c)
                     : (sx + (c & 1)) + 3 * (sy + ((c >> 1) & 1));
 }
 
-template <int DIM, int NB, int SX, int SY, int SZ>
+template <int DIM, int NB, int NQ, int SX, int SY, int SZ>
 __device__ __forceinline__ void add_element(const SysArgs& a, int64_t x, int64_t y, int64_t z, int k, int m,
                                             double (&acc)[DIM == 3 ? 27 : 9], double& facc)
 {
@@ -190,15 +190,18 @@ __device__ __forceinline__ void add_element(const SysArgs& a, int64_t x, int64_t
     const int64_t e = ex + a.NE0 * ey + (DIM == 3 ? a.NE0 * a.NE1 * ez : 0);
     constexpr int R = (1 - SX) + 2 * (1 - SY) + (DIM == 3 ? 4 * (1 - SZ) : 0);
     double em[NK], f;
-    element_row<DIM, NB, R>(a, e, k, m, em, f);
+    element_row<DIM, NB, NQ, R>(a, e, k, m, em, f);
 #pragma unroll
     for (int c = 0; c < NK; ++c) acc[band_of<DIM>(SX, SY, SZ, c)] += em[c];
     facc += f;
 }
 
 // one thread per (node, equation k, component m): the node's block row entries (k, m) over
-// its <= 27 (9) neighbours, gathered from the adjacent elements; no atomics
-template <int DIM, int NB>
+// its <= 27 (9) neighbours, gathered from the adjacent elements; no atomics.  NQ = 2^DIM
+// Gauss points, or 1 (the element centre with weight = volume) for coefficients on
+// ReducedFunction (assemblePDESystemReduced, DefaultAssembler3D.cpp:6466-6876,
+// DefaultAssembler2D.cpp assemblePDESystemReduced)
+template <int DIM, int NB, int NQ>
 __global__ void __launch_bounds__(kRows) k_assemble_sys(const __grid_constant__ SysArgs a)
 {
     constexpr int NBD = DIM == 3 ? 27 : 9;
@@ -212,15 +215,15 @@ __global__ void __launch_bounds__(kRows) k_assemble_sys(const __grid_constant__ 
     for (int b = 0; b < NBD; ++b) acc[b] = 0.0;
     double facc = 0.0;
     const int64_t x = i % a.NN0, y = (i / a.NN0) % a.NN1, z = DIM == 3 ? i / (a.NN0 * a.NN1) : 0;
-    add_element<DIM, NB, 0, 0, 0>(a, x, y, z, k, m, acc, facc);
-    add_element<DIM, NB, 1, 0, 0>(a, x, y, z, k, m, acc, facc);
-    add_element<DIM, NB, 0, 1, 0>(a, x, y, z, k, m, acc, facc);
-    add_element<DIM, NB, 1, 1, 0>(a, x, y, z, k, m, acc, facc);
+    add_element<DIM, NB, NQ, 0, 0, 0>(a, x, y, z, k, m, acc, facc);
+    add_element<DIM, NB, NQ, 1, 0, 0>(a, x, y, z, k, m, acc, facc);
+    add_element<DIM, NB, NQ, 0, 1, 0>(a, x, y, z, k, m, acc, facc);
+    add_element<DIM, NB, NQ, 1, 1, 0>(a, x, y, z, k, m, acc, facc);
     if (DIM == 3) {
-        add_element<DIM, NB, 0, 0, 1>(a, x, y, z, k, m, acc, facc);
-        add_element<DIM, NB, 1, 0, 1>(a, x, y, z, k, m, acc, facc);
-        add_element<DIM, NB, 0, 1, 1>(a, x, y, z, k, m, acc, facc);
-        add_element<DIM, NB, 1, 1, 1>(a, x, y, z, k, m, acc, facc);
+        add_element<DIM, NB, NQ, 0, 0, 1>(a, x, y, z, k, m, acc, facc);
+        add_element<DIM, NB, NQ, 1, 0, 1>(a, x, y, z, k, m, acc, facc);
+        add_element<DIM, NB, NQ, 0, 1, 1>(a, x, y, z, k, m, acc, facc);
+        add_element<DIM, NB, NQ, 1, 1, 1>(a, x, y, z, k, m, acc, facc);
     }
     if (a.rhs && m == 0) a.rhs[i * NB + k] += facc;
     if (!a.val) return;
@@ -886,7 +889,7 @@ int residual_norms_system(Matrix* m, const double* b, const double* x, double* l
     return RG_OK;
 }
 
-int assemble_system_impl(const Domain* d, int nb, double* val, double* rhs, const rg_coef* c[6])
+int assemble_system_impl(const Domain* d, int nb, double* val, double* rhs, const rg_coef* c[6], bool reduced)
 {
     sys::SysArgs a;
     bool addS = false, addF = false;
@@ -895,7 +898,7 @@ int assemble_system_impl(const Domain* d, int nb, double* val, double* rhs, cons
         a.c[j].kind = (c[j] && c[j]->ptr) ? c[j]->kind : RG_COEF_EMPTY;
         if (a.c[j].kind) (j < 4 ? addS : addF) = true;
     }
-    a.t = d->q1;
+    a.t = reduced ? d->q1r : d->q1;
     a.NE0 = d->ne[0];
     a.NE1 = d->ne[1];
     a.NE2 = d->ne[2];
@@ -909,10 +912,18 @@ int assemble_system_impl(const Domain* d, int nb, double* val, double* rhs, cons
     if (!a.val && !a.rhs) return RG_OK;
     const int64_t threads = d->n * nb * nb;
     const int grid = (int)((threads + sys::kRows - 1) / sys::kRows);
-    if (d->dim == 3 && nb == 2) RG_TIMED(T_ASSEMBLE, (sys::k_assemble_sys<3, 2><<<grid, sys::kRows, 0, stream()>>>(a)));
-    else if (d->dim == 3) RG_TIMED(T_ASSEMBLE, (sys::k_assemble_sys<3, 3><<<grid, sys::kRows, 0, stream()>>>(a)));
-    else if (nb == 2) RG_TIMED(T_ASSEMBLE, (sys::k_assemble_sys<2, 2><<<grid, sys::kRows, 0, stream()>>>(a)));
-    else RG_TIMED(T_ASSEMBLE, (sys::k_assemble_sys<2, 3><<<grid, sys::kRows, 0, stream()>>>(a)));
+#define RG_SYS_ASM(DIM, NB, NQ) \
+    RG_TIMED(T_ASSEMBLE, (sys::k_assemble_sys<DIM, NB, NQ><<<grid, sys::kRows, 0, stream()>>>(a)))
+    if (d->dim == 3 && nb == 2) {
+        if (reduced) RG_SYS_ASM(3, 2, 1); else RG_SYS_ASM(3, 2, 8);
+    } else if (d->dim == 3) {
+        if (reduced) RG_SYS_ASM(3, 3, 1); else RG_SYS_ASM(3, 3, 8);
+    } else if (nb == 2) {
+        if (reduced) RG_SYS_ASM(2, 2, 1); else RG_SYS_ASM(2, 2, 4);
+    } else {
+        if (reduced) RG_SYS_ASM(2, 3, 1); else RG_SYS_ASM(2, 3, 4);
+    }
+#undef RG_SYS_ASM
     RG_CHECK_LAUNCH();
     return RG_OK;
 }

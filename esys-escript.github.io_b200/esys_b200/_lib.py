@@ -86,8 +86,12 @@ _SIGNATURES = {
     "rg_assemble_single": (C.c_int, [C.c_void_p, C.c_void_p] + [C.POINTER(rg_coef)] * 6),
     "rg_assemble_boundary": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(rg_coef),
                                        C.POINTER(rg_coef)]),
+    "rg_assemble_boundary_reduced": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(rg_coef),
+                                               C.POINTER(rg_coef)]),
     "rg_assemble_single_reduced": (C.c_int, [C.c_void_p, C.c_void_p] + [C.POINTER(rg_coef)] * 6),
     "rg_assemble_system": (C.c_int, [C.c_void_p, C.c_void_p] + [C.POINTER(rg_coef)] * 6),
+    "rg_matrix_create_system": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]),
+    "rg_assemble_system_reduced": (C.c_int, [C.c_void_p, C.c_void_p] + [C.POINTER(rg_coef)] * 6),
     "rg_matrix_create_system": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]),
     "rg_matrix_block_size": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
     "rg_insert_constraint": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),

@@ -5,8 +5,10 @@ This mirrors the reference's Python surface for the path
 ``LinearPDE(dom); pde.setValue(A=..., D=..., Y=..., q=..., r=...); u = pde.getSolution()``
 (escriptcore/py_src/linearPDEs.py:1760-2207) with the same names, argument meaning and
 error classes.  Data lives on the GPU as torch float64 tensors; assembly, constraints
-and the solve run in libripley_gpu.so.  Only the single-equation PDE is provided;
-systems, lumping and reduced-order coefficients raise NotImplementedError.
+and the solve run in libripley_gpu.so.  Single equations and systems of 2 or 3 equations
+are provided, with coefficients on Function, ReducedFunction, FunctionOnBoundary and
+ReducedFunctionOnBoundary; lumping, contact and Dirac-point coefficients raise
+NotImplementedError.
 """
 from __future__ import annotations
 
@@ -44,8 +46,9 @@ class FunctionSpace:
         return self._domain.getDim()
 
     def getTypeCode(self):
-        return {"ContinuousFunction": 1, "Solution": 3, "ReducedSolution": 4, "Function": 6,
-                "ReducedFunction": 10, "FunctionOnBoundary": 7,
+        # ripley's function space codes (ripley/src/Ripley.h:49-59, RipleyDomain.h getXCode)
+        return {"Solution": 1, "ReducedSolution": 2, "ContinuousFunction": 3, "Function": 4,
+                "ReducedFunction": 10, "FunctionOnBoundary": 5, "ReducedFunctionOnBoundary": 11,
                 "ReducedContinuousFunction": 14}[self._kind]
 
     def __str__(self):
@@ -64,18 +67,21 @@ class FunctionSpace:
         return hash((id(self._domain), self._storage()))
 
     def _storage(self):
-        """Where values live: 'nodes' (DOF = nodes on one rank), 'qp', 'elem' or 'face'."""
+        """Where values live: 'nodes' (DOF = nodes on one rank), 'qp', 'elem', 'face' (the face
+        Gauss points) or 'rface' (face centres)."""
         if self._kind in _NODES:
             return "nodes"
-        return {"Function": "qp", "ReducedFunction": "elem", "FunctionOnBoundary": "face"}[self._kind]
+        return {"Function": "qp", "ReducedFunction": "elem", "FunctionOnBoundary": "face",
+                "ReducedFunctionOnBoundary": "rface"}[self._kind]
 
     def getNumSamples(self):
         d = self._domain
-        return {"nodes": d._n, "qp": d._nel, "elem": d._nel, "face": d._nfaces}[self._storage()]
+        return {"nodes": d._n, "qp": d._nel, "elem": d._nel, "face": d._nfaces,
+                "rface": d._nfaces}[self._storage()]
 
     def getNumDataPointsPerSample(self):
         d = self._domain
-        return {"nodes": 1, "qp": 1 << d._dim, "elem": 1, "face": 1 << (d._dim - 1)}[self._storage()]
+        return {"nodes": 1, "qp": 1 << d._dim, "elem": 1, "face": 1 << (d._dim - 1), "rface": 1}[self._storage()]
 
     def _num_points(self):
         return self.getNumSamples() * self.getNumDataPointsPerSample()
@@ -111,6 +117,10 @@ def ReducedFunction(domain):
 
 def FunctionOnBoundary(domain):
     return FunctionSpace(domain, "FunctionOnBoundary")
+
+
+def ReducedFunctionOnBoundary(domain):
+    return FunctionSpace(domain, "ReducedFunctionOnBoundary")
 
 
 # ---------------------------------------------------------------------------------------------
@@ -256,6 +266,11 @@ class Data:
             return Data._wrap(out, self._shape, fs)
         if src == "nodes" and dst == "face":
             return Data._wrap(dom._nodes_to_face(self._dev()), self._shape, fs)
+        if src == "nodes" and dst == "rface":
+            return Data._wrap(dom._nodes_to_face(self._dev(), reduced=True), self._shape, fs)
+        if src == "face" and dst == "rface":
+            q = 1 << (dom._dim - 1)
+            return Data._wrap(self._dev().reshape(-1, q, self._t.shape[1]).mean(1), self._shape, fs)
         if src == "qp" and dst == "elem":
             q = 1 << dom._dim
             return Data._wrap(self._dev().reshape(-1, q, self._t.shape[1]).mean(1), self._shape, fs)
@@ -361,7 +376,7 @@ class Data:
 
 
 def _common_fs(a, b):
-    order = {"nodes": 0, "qp": 1, "elem": 2, "face": 3}
+    order = {"nodes": 0, "qp": 1, "elem": 2, "face": 3, "rface": 4}
     sa, sb = a._storage(), b._storage()
     if sa == sb:
         return a
@@ -371,6 +386,8 @@ def _common_fs(a, b):
         return a if sa == "elem" else b
     if {sa, sb} == {"nodes", "face"}:
         return a if sa == "face" else b
+    if {sa, sb} == {"nodes", "rface"} or {sa, sb} == {"face", "rface"}:
+        return a if sa == "rface" else b
     raise ValueError(f"cannot combine data on {a} and {b}")
 
 
@@ -819,9 +836,10 @@ def _tensor_from_ptr(ptr, count, dtype):
 _INTERIOR = ("A", "B", "C", "D", "X", "Y")
 _REDUCED = ("A_reduced", "B_reduced", "C_reduced", "D_reduced", "X_reduced", "Y_reduced")
 _BOUNDARY = ("d", "y")
+_BOUNDARY_REDUCED = ("d_reduced", "y_reduced")
 _CONSTRAINT = ("q", "r")
-_UNSUPPORTED = ("d_reduced", "y_reduced", "d_contact", "y_contact", "d_contact_reduced",
-                "y_contact_reduced", "d_dirac", "y_dirac")
+_UNSUPPORTED = ("d_contact", "y_contact", "d_contact_reduced", "y_contact_reduced", "d_dirac", "y_dirac")
+_ALL = _INTERIOR + _REDUCED + _BOUNDARY + _BOUNDARY_REDUCED + _CONSTRAINT
 
 
 class LinearPDE:
@@ -893,6 +911,8 @@ class LinearPDE:
             return ReducedFunction(self._domain)
         if name in _BOUNDARY:
             return FunctionOnBoundary(self._domain)
+        if name in _BOUNDARY_REDUCED:
+            return ReducedFunctionOnBoundary(self._domain)
         if name in _CONSTRAINT:
             return Solution(self._domain)
         raise ValueError(f"unknown coefficient {name}")
@@ -918,7 +938,7 @@ class LinearPDE:
     def getCoefficient(self, name):
         if name in self._coef:
             return self._coef[name]
-        if name in _INTERIOR + _REDUCED + _BOUNDARY + _CONSTRAINT + _UNSUPPORTED:
+        if name in _ALL + _UNSUPPORTED:
             return Data()
         raise ValueError(f"unknown coefficient {name}")
 
@@ -929,11 +949,8 @@ class LinearPDE:
                 if value is None or (isinstance(value, Data) and value.isEmpty()):
                     continue
                 raise NotImplementedError(f"coefficient {name} is not part of the GPU path")
-            if name not in _INTERIOR + _REDUCED + _BOUNDARY + _CONSTRAINT:
+            if name not in _ALL:
                 raise ValueError(f"illegal coefficient {name} requested for general PDE.")
-            if self._nb > 1 and name in _REDUCED + _BOUNDARY and not (
-                    value is None or (isinstance(value, Data) and value.isEmpty())):
-                raise NotImplementedError(f"coefficient {name} of a PDE system is not part of the GPU path")
             if value is None or (isinstance(value, Data) and value.isEmpty()):
                 self._coef.pop(name, None)
             else:
@@ -950,9 +967,9 @@ class LinearPDE:
                         raise ValueError(f"coefficient {name}: expected shape {shape}")
                     dat = Data(a, shape, fs)
                 self._coef[name] = dat
-            if name in ("A", "B", "C", "D", "d", "A_reduced", "B_reduced", "C_reduced", "D_reduced"):
+            if name in ("A", "B", "C", "D", "d", "A_reduced", "B_reduced", "C_reduced", "D_reduced", "d_reduced"):
                 self._operator_valid = False
-            if name in ("X", "Y", "y", "r", "X_reduced", "Y_reduced"):
+            if name in ("X", "Y", "y", "r", "X_reduced", "Y_reduced", "y_reduced"):
                 self._rhs_valid = False
             if name == "q":
                 self._operator_valid = False
@@ -970,60 +987,39 @@ class LinearPDE:
         return L.rg_coef(t.data_ptr(), kind)
 
     def getSystem(self):
-        """Build operator and right hand side (linearPDEs.py:1881-2082, non-lumped branch)."""
+        """Build operator and right hand side (linearPDEs.py:1881-2082, non-lumped branch):
+        interior terms (Function and ReducedFunction), face terms (FunctionOnBoundary and
+        ReducedFunctionOnBoundary), then the constraint.  A right hand side rebuilt alone
+        assembles only X, Y, y (and their reduced forms) into the existing operator."""
         if self._operator_valid and self._rhs_valid:
             return self._operator, self._rhs
         keep = []
         lib = L.lib()
-        if not self._operator_valid and self._nb > 1:
-            # PDE system: interior terms (assemblePDESystem) and the constraint
+        empty = L.rg_coef(None, L.RG_COEF_EMPTY)
+        rhs_only = self._operator_valid
+        if not rhs_only:
             self._operator = SystemMatrix(self._domain, self._nb)
-            self._rhs = self.createRightHandSide()
-            L.set_stream_from_torch()
-            cs = [self._coef_c(n, keep) for n in _INTERIOR]
-            L.check(lib.rg_assemble_system(self._operator._handle, C.c_void_p(self._rhs._t.data_ptr()),
-                                           *[C.byref(c) for c in cs]))
-            self._insert_constraint(rhs_only=False)
-        elif self._nb > 1:
-            self._rhs = self.createRightHandSide()
-            L.set_stream_from_torch()
-            empty = L.rg_coef(None, L.RG_COEF_EMPTY)
-            cs = [empty, empty, empty, empty, self._coef_c("X", keep), self._coef_c("Y", keep)]
-            L.check(lib.rg_assemble_system(self._operator._handle, C.c_void_p(self._rhs._t.data_ptr()),
-                                           *[C.byref(c) for c in cs]))
-            self._insert_constraint(rhs_only=True)
-        elif not self._operator_valid:
-            self._operator = SystemMatrix(self._domain)
-            self._rhs = self.createRightHandSide()
-            L.set_stream_from_torch()
-            cs = [self._coef_c(n, keep) for n in _INTERIOR]
-            L.check(lib.rg_assemble_single(self._operator._handle, C.c_void_p(self._rhs._t.data_ptr()),
-                                           *[C.byref(c) for c in cs]))
-            if any(n in self._coef for n in _REDUCED):
-                cr = [self._coef_c(n, keep) for n in _REDUCED]
-                L.check(lib.rg_assemble_single_reduced(self._operator._handle,
-                                                       C.c_void_p(self._rhs._t.data_ptr()),
-                                                       *[C.byref(c) for c in cr]))
-            bd = [self._coef_c(n, keep) for n in _BOUNDARY]
-            L.check(lib.rg_assemble_boundary(self._operator._handle, C.c_void_p(self._rhs._t.data_ptr()),
-                                             C.byref(bd[0]), C.byref(bd[1])))
-            self._insert_constraint(rhs_only=False)
-        else:
-            self._rhs = self.createRightHandSide()
-            L.set_stream_from_torch()
-            empty = L.rg_coef(None, L.RG_COEF_EMPTY)
-            cs = [empty, empty, empty, empty, self._coef_c("X", keep), self._coef_c("Y", keep)]
-            L.check(lib.rg_assemble_single(self._operator._handle, C.c_void_p(self._rhs._t.data_ptr()),
-                                           *[C.byref(c) for c in cs]))
-            if "X_reduced" in self._coef or "Y_reduced" in self._coef:
-                cr = [empty, empty, empty, empty, self._coef_c("X_reduced", keep), self._coef_c("Y_reduced", keep)]
-                L.check(lib.rg_assemble_single_reduced(self._operator._handle,
-                                                       C.c_void_p(self._rhs._t.data_ptr()),
-                                                       *[C.byref(c) for c in cr]))
-            yc = self._coef_c("y", keep)
-            L.check(lib.rg_assemble_boundary(self._operator._handle, C.c_void_p(self._rhs._t.data_ptr()),
-                                             C.byref(empty), C.byref(yc)))
-            self._insert_constraint(rhs_only=True)
+        self._rhs = self.createRightHandSide()
+        h = self._operator._handle
+        rp = C.c_void_p(self._rhs._t.data_ptr())
+        L.set_stream_from_torch()
+
+        def names(group):
+            return [(n if (not rhs_only or n[0] in "XYy") else None) for n in group]
+
+        def coefs(group):
+            return [self._coef_c(n, keep) if n else empty for n in names(group)]
+
+        L.check(lib.rg_assemble_system(h, rp, *[C.byref(c) for c in coefs(_INTERIOR)]))
+        if any(n and n in self._coef for n in names(_REDUCED)):
+            L.check(lib.rg_assemble_system_reduced(h, rp, *[C.byref(c) for c in coefs(_REDUCED)]))
+        if any(n and n in self._coef for n in names(_BOUNDARY)):
+            bd = coefs(_BOUNDARY)
+            L.check(lib.rg_assemble_boundary(h, rp, C.byref(bd[0]), C.byref(bd[1])))
+        if any(n and n in self._coef for n in names(_BOUNDARY_REDUCED)):
+            bd = coefs(_BOUNDARY_REDUCED)
+            L.check(lib.rg_assemble_boundary_reduced(h, rp, C.byref(bd[0]), C.byref(bd[1])))
+        self._insert_constraint(rhs_only=rhs_only)
         torch.cuda.current_stream().synchronize()
         self._operator_valid = True
         self._rhs_valid = True

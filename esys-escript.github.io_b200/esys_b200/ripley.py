@@ -153,17 +153,21 @@ class RipleyDomain:
             return torch.stack([x.reshape(-1), y.reshape(-1), z.reshape(-1)], 1)
         if storage == "face":
             return torch.cat([self._face_points(f) for f in range(2 * d)])
+        if storage == "rface":
+            return torch.cat([self._face_points(f, reduced=True) for f in range(2 * d)])
         raise ValueError(storage)
 
     def _face_axes(self, face):
         ax = face // 2
         return ax, [a for a in range(self._dim) if a != ax]
 
-    def _face_points(self, face):
-        """Gauss points of face ``face``: (face element (lower in-face axis fastest), q)."""
+    def _face_points(self, face, reduced=False):
+        """Gauss points of face ``face``: (face element (lower in-face axis fastest), q); with
+        ``reduced`` the face element centres."""
         ax, fa = self._face_axes(face)
         side = face % 2
-        g = torch.tensor(_G, dtype=torch.float64, device=DEVICE)
+        g = torch.tensor((0.5,) if reduced else _G, dtype=torch.float64, device=DEVICE)
+        nq = g.numel()
         c_fixed = self._x0[ax] + (self._x1[ax] - self._x0[ax]) * side
         cols = {}
         if self._dim == 2:
@@ -177,19 +181,20 @@ class RipleyDomain:
             pa = self._x0[a] + self._dx[a] * (torch.arange(self._ne[a], dtype=torch.float64, device=DEVICE)[:, None] + g[None, :])
             pb = self._x0[b] + self._dx[b] * (torch.arange(self._ne[b], dtype=torch.float64, device=DEVICE)[:, None] + g[None, :])
             # index order: (kb, ka, qb, qa)
-            A = pa[None, :, None, :].expand(self._ne[b], -1, 2, -1)
-            B = pb[:, None, :, None].expand(-1, self._ne[a], -1, 2)
+            A = pa[None, :, None, :].expand(self._ne[b], -1, nq, -1)
+            B = pb[:, None, :, None].expand(-1, self._ne[a], -1, nq)
             cols[a] = A.reshape(-1)
             cols[b] = B.reshape(-1)
             cols[ax] = torch.full_like(cols[a], c_fixed)
         return torch.stack([cols[k] for k in range(self._dim)], 1)
 
-    def _nodes_to_face(self, nodal):
-        """Interpolate nodal values (n, ncomp) to the face Gauss points."""
+    def _nodes_to_face(self, nodal, reduced=False):
+        """Interpolate nodal values (n, ncomp) to the face Gauss points (``reduced``: to the
+        face element centres)."""
         ncomp = nodal.shape[1]
         d = self._dim
         grid = nodal.reshape(tuple(reversed(self._nn[:d])) + (ncomp,))  # (.., NN1, NN0, c)
-        g = torch.tensor(_G, dtype=torch.float64, device=DEVICE)
+        g = torch.tensor((0.5,) if reduced else _G, dtype=torch.float64, device=DEVICE)
         out = []
         for face in range(2 * d):
             ax, fa = self._face_axes(face)

@@ -118,10 +118,23 @@ int rg_assemble_single_reduced(rg_matrix* mat, double* rhs, const rg_coef* A, co
    C (bs, bs, dim), D (bs, bs), X (bs, dim), Y (bs); rhs has n bs entries. */
 int rg_assemble_system(rg_matrix* mat, double* rhs, const rg_coef* A, const rg_coef* B,
                        const rg_coef* C, const rg_coef* D, const rg_coef* X, const rg_coef* Y);
-/* assemblePDEBoundarySingle: adds the face terms d (matrix) and y (rhs).  d/y are on
-   FunctionOnBoundary: faces left,right,bottom,top(,front,back), face elements lower
-   in-face axis fastest, 2^(dim-1) Gauss points per face element. */
+/* assemblePDESystemReduced (ripley/src/DefaultAssembler3D.cpp:6466-6876, DefaultAssembler2D
+   assemblePDESystemReduced): the terms of rg_assemble_system for coefficients on
+   ReducedFunction, 1-point rule at the element centre (one data point per element).  For a
+   matrix of block size 1 this is rg_assemble_single_reduced. */
+int rg_assemble_system_reduced(rg_matrix* mat, double* rhs, const rg_coef* A, const rg_coef* B,
+                               const rg_coef* C, const rg_coef* D, const rg_coef* X, const rg_coef* Y);
+/* assemblePDEBoundarySingle / assemblePDEBoundarySystem (DefaultAssembler3D.cpp:2232-2888,
+   5753-6464): adds the face terms d (matrix) and y (rhs).  d/y are on FunctionOnBoundary:
+   faces left,right,bottom,top(,front,back), face elements lower in-face axis fastest,
+   2^(dim-1) Gauss points per face element.  For a matrix of block size bs the data points
+   are d (bs, bs) = d[k + bs m] and y (bs); rhs has n bs entries. */
 int rg_assemble_boundary(rg_matrix* mat, double* rhs, const rg_coef* d, const rg_coef* y);
+/* assemblePDEBoundarySingleReduced / assemblePDEBoundarySystemReduced (DefaultAssembler3D.cpp:
+   3274-3628, 6878-7255): the face terms for d_reduced / y_reduced on
+   ReducedFunctionOnBoundary, one data point per face element, 1-point rule at the face
+   centre. */
+int rg_assemble_boundary_reduced(rg_matrix* mat, double* rhs, const rg_coef* d, const rg_coef* y);
 
 /* LinearPDE.insertConstraint(rhs_only=0): rhs -= A*u with u = r on q>0 else 0; rows and
    columns with q>0 nullified with 1 on the diagonal; rhs[q>0] = r.  r may be NULL (= 0).

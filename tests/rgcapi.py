@@ -108,11 +108,19 @@ def assemble_reduced(mat, rhs_t, keep, **coefs):
     L.check(lib().rg_assemble_single_reduced(mat.h if mat else None, ptr(rhs_t), *[C.byref(c) for c in cs]))
 
 
-def assemble_boundary(mat, rhs_t, keep, d=None, y=None):
+def assemble_system_reduced(mat, rhs_t, keep, **coefs):
+    """coefs: name -> (array, kind) for A,B,C,D,X,Y of a PDE system on ReducedFunction."""
+    cs = [coef(*coefs[k], keep) if k in coefs else L.rg_coef(None, 0) for k in "ABCDXY"]
+    L.set_stream_from_torch()
+    L.check(lib().rg_assemble_system_reduced(mat.h, ptr(rhs_t), *[C.byref(c) for c in cs]))
+
+
+def assemble_boundary(mat, rhs_t, keep, d=None, y=None, reduced=False):
     dc = coef(*d, keep) if d else L.rg_coef(None, 0)
     yc = coef(*y, keep) if y else L.rg_coef(None, 0)
     L.set_stream_from_torch()
-    L.check(lib().rg_assemble_boundary(mat.h, ptr(rhs_t), C.byref(dc), C.byref(yc)))
+    fn = lib().rg_assemble_boundary_reduced if reduced else lib().rg_assemble_boundary
+    L.check(fn(mat.h, ptr(rhs_t), C.byref(dc), C.byref(yc)))
 
 
 def insert_constraint(mat, rhs_t, q_t, r_t=None, rhs_only=0):

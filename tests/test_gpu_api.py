@@ -114,7 +114,7 @@ def test_unsupported_features_raise(cuda):
         LinearPDE(dom, numEquations=2, numSolutions=3)
     pde = LinearPDE(dom)
     with pytest.raises(NotImplementedError):
-        pde.setValue(y_reduced=1.0)
+        pde.setValue(y_contact=1.0)
     with pytest.raises(ValueError):
         pde.setValue(Z=1.0)
     pde.setValue(A=kronecker(2), Y=1.0)
@@ -183,5 +183,60 @@ def test_system_coupled_known_answer(cuda):
     pde.setValue(A=A, D=D, Y=D.sum(axis=1))
     u = pde.getSolution()
     assert float((u._dev() - 1.0).abs().max()) < 1e-8
-    with pytest.raises(NotImplementedError):
-        pde.setValue(d=np.eye(3))
+
+
+@pytest.mark.parametrize("reduced", [False, True])
+def test_robin_boundary_known_answer(domain, reduced):
+    """A = I, D = 0, d = y = 2 on the whole boundary (FunctionOnBoundary, or
+    ReducedFunctionOnBoundary for d_reduced / y_reduced): n.grad u + d u = y has u = 1."""
+    pde = LinearPDE(domain)
+    sfx = "_reduced" if reduced else ""
+    pde.setValue(A=kronecker(domain), **{"d" + sfx: 2.0, "y" + sfx: 2.0})
+    assert check(pde.getSolution(), 1.0)
+
+
+@pytest.mark.parametrize("reduced", [False, True])
+def test_system_boundary_and_reduced_known_answer(cuda, reduced):
+    """Lame system with d = I and y = c on the boundary: the constant displacement c
+    (zero strain) solves it; then D_reduced = I, Y_reduced = c alone (mass matrix on
+    ReducedFunction) gives c too.  Face terms of systems: assemblePDEBoundarySystem
+    (d, y) and assemblePDEBoundarySystemReduced (d_reduced, y_reduced)."""
+    dom = ripley.Brick(5, 4, 3)
+    c = np.array([1.0, -2.0, 0.5])
+    lam, mu = 1.0, 0.5
+    A = np.zeros((3, 3, 3, 3))
+    for k in range(3):
+        for i in range(3):
+            for m in range(3):
+                for j in range(3):
+                    A[k, i, m, j] = lam * (k == i) * (m == j) + mu * ((k == m) * (i == j) + (k == j) * (i == m))
+    sfx = "_reduced" if reduced else ""
+    pde = LinearPDE(dom, numEquations=3)
+    pde.setValue(A=A, **{"d" + sfx: np.eye(3), "y" + sfx: c})
+    u = pde.getSolution()
+    assert float((u._dev() - torch_tensor(c)).abs().max()) < 1e-8
+    pde2 = LinearPDE(dom, numEquations=3)
+    pde2.setValue(D_reduced=np.eye(3), Y_reduced=c)
+    u2 = pde2.getSolution()
+    assert float((u2._dev() - torch_tensor(c)).abs().max()) < 1e-8
+
+
+def torch_tensor(a):
+    import torch
+    return torch.as_tensor(a, dtype=torch.float64, device="cuda")
+
+
+def test_reduced_boundary_function_space(cuda):
+    from esys_b200.escript import FunctionOnBoundary, ReducedFunctionOnBoundary
+    dom = ripley.Brick(3, 2, 2)
+    fs = ReducedFunctionOnBoundary(dom)
+    assert fs.getTypeCode() == 11 and FunctionOnBoundary(dom).getTypeCode() == 5
+    assert fs.getNumDataPointsPerSample() == 1
+    xr = fs.getX().toNumpy()
+    assert xr.shape == (2 * (2 * 2 + 3 * 2 + 3 * 2), 3)
+    # the face centres of face 0 (x = 0), face element (ka, kb) = (0, 0): (0, 0.25, 0.25)
+    assert np.allclose(xr[0], [0.0, 0.25, 0.25])
+    # a linear field interpolates exactly to the face centres, from the nodes or the Gauss points
+    lin = Solution(dom).getX()[0] + 2.0 * Solution(dom).getX()[1]
+    assert np.allclose(lin.interpolate(fs).toNumpy(), xr[:, 0] + 2 * xr[:, 1])
+    assert np.allclose(lin.interpolate(FunctionOnBoundary(dom)).interpolate(fs).toNumpy(), xr[:, 0] + 2 * xr[:, 1])

@@ -120,3 +120,78 @@ def test_system_known_answer_and_unsupported_paths(cuda):
     assert float((x - 1.0).abs().max()) < 1e-8
     st, _ = R.solve(m, rhs, x, R.opts(precision=L.RG_PREC_FP32_REFINE))
     assert st == L.RG_NOT_SUPPORTED
+
+
+def _asm_domain(golden, dim):
+    tag = f"{dim}d"
+    ne = tuple(int(v) for v in golden[f"asm{tag}_ne"])
+    dx = golden[f"asm{tag}_dx"]
+    return R.Domain(dim, ne, x1=[dx[k] * ne[k] for k in range(dim)])
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+@pytest.mark.parametrize("case", ["bred", "bsys", "bsysred"])
+@pytest.mark.parametrize("kname", ["const", "exp", "elem"])
+def test_general_boundary_assembly_matches_reference(cuda, golden, dim, case, kname):
+    """rg_assemble_boundary on systems (bsys: assemblePDEBoundarySystem) and
+    rg_assemble_boundary_reduced (bred: assemblePDEBoundarySingleReduced, bsysred:
+    assemblePDEBoundarySystemReduced) against the reference's own outputs.  On
+    ReducedFunctionOnBoundary per-element data is the expanded data."""
+    tag = f"{dim}d"
+    nb = 1 if case == "bred" else dim
+    reduced = case != "bsys"
+    gk = "const" if kname == "const" else "exp"
+    if kname == "elem" and not reduced:
+        pytest.skip("per-element face data differs from the expanded data on FunctionOnBoundary")
+    d = _asm_domain(golden, dim)
+    m = R.Matrix(d, nb)
+    rhs = torch.zeros(d.n * nb, dtype=torch.float64, device="cuda")
+    keep = []
+    R.assemble_boundary(m, rhs, keep, d=(golden[f"{case}{tag}_{gk}_d"], R.KINDS[kname]),
+                        y=(golden[f"{case}{tag}_{gk}_y"], R.KINDS[kname]), reduced=reduced)
+    rv, rr = golden[f"{case}{tag}_{gk}_val"], golden[f"{case}{tag}_{gk}_rhs"]
+    assert np.abs(m.values() - rv).max() <= ASM_TOL * np.abs(rv).max()
+    assert np.abs(rhs.cpu().numpy() - rr).max() <= ASM_TOL * np.abs(rr).max()
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+@pytest.mark.parametrize("kname", ["const", "exp", "elem"])
+def test_system_reduced_assembly_matches_reference(cuda, golden, dim, kname):
+    """rg_assemble_system_reduced against assemblePDESystemReduced."""
+    tag = f"{dim}d"
+    gk = "const" if kname == "const" else "exp"
+    d = _asm_domain(golden, dim)
+    m = R.Matrix(d, dim)
+    rhs = torch.zeros(d.n * dim, dtype=torch.float64, device="cuda")
+    keep = []
+    R.assemble_system_reduced(m, rhs, keep, **{k: (golden[f"sysred{tag}_{gk}_{k}"], R.KINDS[kname])
+                                               for k in "ABCDXY"})
+    ref = golden[f"sysred{tag}_{gk}_val"]
+    assert np.abs(m.values() - ref).max() <= ASM_TOL * np.abs(ref).max()
+    ref_rhs = golden[f"sysred{tag}_{gk}_rhs"]
+    assert np.abs(rhs.cpu().numpy() - ref_rhs).max() <= ASM_TOL * np.abs(ref_rhs).max()
+
+
+@pytest.mark.parametrize("nb", [2, 3])
+def test_large_system_boundary_matches_oracle(cuda, nb):
+    """Brick 24x20x16, expanded d and y of a system on every face, full and reduced rule,
+    against the oracle."""
+    rng = np.random.default_rng(40 + nb)
+    ne = (24, 20, 16)
+    dx = (1 / 24, 1 / 20, 1 / 16)
+    nface = 2 * (ne[1] * ne[2] + ne[0] * ne[2] + ne[0] * ne[1])
+    pat = O.pattern(3, ne)
+    for reduced in (False, True):
+        nq = 1 if reduced else 4
+        dd = rng.standard_normal(nface * nq * nb * nb)
+        yy = rng.standard_normal(nface * nq * nb)
+        d = R.Domain(3, ne)
+        m = R.Matrix(d, nb)
+        rhs = torch.zeros(d.n * nb, dtype=torch.float64, device="cuda")
+        keep = []
+        R.assemble_boundary(m, rhs, keep, d=(dd, R.KINDS["exp"]), y=(yy, R.KINDS["exp"]), reduced=reduced)
+        val = np.zeros(pat.nnz * nb * nb)
+        rr = np.zeros(pat.n * nb)
+        O.assemble_boundary(3, ne, dx, pat, val, rr, d=(O.EXPANDED, dd), y=(O.EXPANDED, yy), nb=nb, reduced=reduced)
+        assert np.abs(m.values() - val).max() <= ASM_TOL * np.abs(val).max()
+        assert np.abs(rhs.cpu().numpy() - rr).max() <= ASM_TOL * np.abs(rr).max()
