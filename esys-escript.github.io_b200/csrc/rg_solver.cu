@@ -76,7 +76,9 @@ struct Workspace {
     Scal* hpoll = nullptr;                   // 2 pinned slots for pipelined polling
     cudaGraphExec_t graph[3] = {nullptr, nullptr, nullptr};
     int graph_chunk[3] = {0, 0, 0};
+    int graph_sweeps[3] = {0, 0, 0};  // Jacobi sweeps the captured iterations apply
     long long graph_launches[3][T_COUNT] = {};
+    int sweeps = 1;  // Jacobi sweeps of the current paso solve (Smoother.cpp:100-128)
     int spmv_cfg = -1;   // FP32 band SpMV pipeline: 0 = 3 stages x 1 CTA/SM, 1 = 2 stages x 2 CTAs/SM
     int grid_upd32 = 0;  // CTAs of k_f32_update (tuned with the SpMV; 0 = grid_vec)
     double spmv_us[2] = {0, 0};  // tuner's time per launch of each SpMV configuration
@@ -345,6 +347,47 @@ __global__ void __launch_bounds__(kThreads) k_paso_spmv(int64_t n, const int32_t
             s->iter += 1;
             s->status = ST_BREAK;
             s->done = 1;
+        }
+    }
+}
+
+// One more sweep of the Jacobi smoother used as preconditioner when sweeps > 1
+// (Preconditioner_LocalSmoother_solve, paso/src/Smoother.cpp:161-184: b_new = b - A x,
+// x += D^-1 b_new): zout = zin + dinv (b - A zin).  mode 0: that alone; mode 1 (the last
+// sweep inside the PCG loop): tau_next = zout.b and beta = tau_next/tau; mode 2 (the last
+// sweep of the PCG start): tau = zout.b and p = zout.
+__global__ void __launch_bounds__(kThreads) k_jacobi_sweep(int64_t n, const int32_t* __restrict__ ptr,
+                                                           const int32_t* __restrict__ idx,
+                                                           const double* __restrict__ val,
+                                                           const double* __restrict__ dinv,
+                                                           const double* __restrict__ b,
+                                                           const double* __restrict__ zin,
+                                                           double* __restrict__ zout, double* __restrict__ p,
+                                                           ReduceBuf rb, Scal* s, int mode)
+{
+    if (mode == 1 && s->done) return;
+    double v[1] = {0.0};
+    RG_ROW_LOOP(n)
+    {
+        double acc = row < n ? csr_row_dot(ptr, idx, val, zin, row, lane) : 0.0;
+        acc = group_sum(acc);
+        if (row < n && lane == 0) {
+            const double bi = b[row];
+            const double db = dinv[row] * (bi - acc);
+            const double zi = zin[row] + db;
+            zout[row] = zi;
+            if (mode == 2) p[row] = zi;
+            v[0] += zi * bi;
+        }
+    }
+    if (mode == 0) return;
+    double t[1];
+    if (grid_reduce<1>(v, rb, t) && threadIdx.x == 0) {
+        if (mode == 1) {
+            s->tau_next = t[0];
+            s->beta = t[0] / s->tau;
+        } else {
+            s->tau = t[0];
         }
     }
 }
@@ -938,7 +981,7 @@ int run_until_done(Matrix* m, int kind, IterFn step, int chunk, long long cap, l
         *status = w->hs->status;
         return RG_OK;
     }
-    if (!w->graph[kind] || w->graph_chunk[kind] != chunk) {
+    if (!w->graph[kind] || w->graph_chunk[kind] != chunk || w->graph_sweeps[kind] != w->sweeps) {
         if (w->graph[kind]) cudaGraphExecDestroy(w->graph[kind]);
         w->graph[kind] = nullptr;
         long long before[T_COUNT], after[T_COUNT];
@@ -960,6 +1003,7 @@ int run_until_done(Matrix* m, int kind, IterFn step, int chunk, long long cap, l
             return RG_CUDA_ERROR;
         }
         w->graph_chunk[kind] = chunk;
+        w->graph_sweeps[kind] = w->sweeps;
         timers_snapshot(after);
         long long undo[T_COUNT];
         for (int k = 0; k < T_COUNT; ++k) {
@@ -997,6 +1041,24 @@ int run_until_done(Matrix* m, int kind, IterFn step, int chunk, long long cap, l
     return RG_OK;
 }
 
+// sweeps - 1 more Jacobi sweeps on the preconditioned vector z (of b), alternating between
+// z and `spare`; returns the buffer that holds the result.  mode of the last sweep as in
+// k_jacobi_sweep.
+double* jacobi_sweeps(Matrix* m, const double* b, double* z, double* spare, double* p, int last_mode)
+{
+    Workspace* w = m->ws;
+    const Domain* d = m->dom;
+    double* src = z;
+    double* dst = spare;
+    for (int k = 1; k < w->sweeps; ++k) {
+        const int mode = k == w->sweeps - 1 ? last_mode : 0;
+        RG_TIMED(T_PASO_UPDATE1, (k_jacobi_sweep<<<w->grid_rows, kThreads, 0, stream()>>>(
+                                     d->n, d->ptr, d->idx, m->val, m->dinv, b, src, dst, p, rbuf(w), w->s, mode)));
+        std::swap(src, dst);
+    }
+    return src;
+}
+
 int paso_step(Matrix* m)
 {
     Workspace* w = m->ws;
@@ -1005,8 +1067,10 @@ int paso_step(Matrix* m)
                               d->n, d->ptr, d->idx, m->val, w->p, w->q, rbuf(w), w->s)));
     RG_TIMED(T_PASO_UPDATE1, (k_paso_update1<<<w->grid_vec, kThreads, 0, stream()>>>(
                                  d->n, w->r, w->q, w->rs, w->x2, w->p, m->dinv, w->z, rbuf(w), w->s)));
+    // v = prec(r) with more than one Jacobi sweep: q (free after update1) is the spare buffer
+    const double* v = jacobi_sweeps(m, w->r, w->z, w->q, nullptr, 1);
     RG_TIMED(T_PASO_UPDATE2, (k_paso_update2<<<w->grid_vec, kThreads, 0, stream()>>>(
-                                 d->n, w->rs, w->r, w->x, w->x2, w->z, w->p, rbuf(w), w->s)));
+                                 d->n, w->rs, w->r, w->x, w->x2, v, w->p, rbuf(w), w->s)));
     RG_CHECK_LAUNCH();
     return RG_OK;
 }
@@ -1311,6 +1375,8 @@ int solve_fp64(Matrix* m, const rg_solver_opts* o, bool paso, OuterState& st, rg
             RG_TIMED(T_VECTOR, (k_paso_init<<<w->grid_rows, kThreads, 0, stream()>>>(
                                    n, w->r, w->x, m->dinv, w->rs, w->x2, w->p, w->z, rbuf(w), w->s, tol, cnt)));
             RG_CHECK_LAUNCH();
+            jacobi_sweeps(m, w->r, w->z, w->q, w->p, 2);  // the first v = prec(r): p and tau
+            RG_CHECK_LAUNCH();
             if ((rc = run_until_done(m, 0, paso_step, chunk, cnt, &it, &dst))) return rc;
         } else {
             RG_TIMED(T_VECTOR, (k_std_init<<<w->grid_rows, kThreads, 0, stream()>>>(
@@ -1495,12 +1561,13 @@ int solve_impl(Matrix* m, const double* rhs, double* x, const rg_solver_opts* o,
     RG_REQUIRE(o->tolerance >= 100. * EPS, "Solver: Tolerance is too small.");
     RG_REQUIRE(o->tolerance <= 1., "Solver: Tolerance must be less than one.");
     RG_REQUIRE(o->guess_sweeps >= 0 && o->guess_sweeps <= 1000, "solver: guess_sweeps must be in [0, 1000]");
-    if (o->sweeps > 1) {
-        set_error("solver: Jacobi with more than one sweep is not implemented on the GPU");
-        return RG_NOT_SUPPORTED;
-    }
     const bool fp32 = o->precision == RG_PREC_FP32_REFINE;
     const bool paso = o->mode == RG_MODE_PASO && !fp32;
+    if (o->sweeps > 1 && !paso) {
+        set_error("solver: Jacobi with more than one sweep runs in paso mode with FP64 (RG_MODE_PASO, "
+                  "RG_PREC_FP64)");
+        return RG_NOT_SUPPORTED;
+    }
     RG_REQUIRE(!(paso && o->initial_guess), "solver: paso mode ignores initial guesses; use RG_MODE_STANDARD");
     int rc = ensure_workspace(m, fp32);
     if (rc) return rc;
@@ -1538,6 +1605,11 @@ int solve_impl(Matrix* m, const double* rhs, double* x, const rg_solver_opts* o,
         // initial guess: Jacobi of B b in paso (Solver.cpp:181); x0 / B or 0 otherwise
         if (paso) {
             RG_TIMED(T_VECTOR, (k_mul<<<eg, kThreads, 0, stream()>>>(n, m->dinv, w->bb, w->x)));
+            RG_CHECK_LAUNCH();
+            w->sweeps = o->sweeps > 1 ? o->sweeps : 1;
+            const double* x0 = jacobi_sweeps(m, w->bb, w->x, w->q, nullptr, 0);
+            if (x0 != w->x)
+                RG_CHECK_CUDA(cudaMemcpyAsync(w->x, x0, sizeof(double) * n, cudaMemcpyDeviceToDevice, stream()));
         } else if (o->initial_guess) {
             RG_TIMED(T_VECTOR, (k_div<<<eg, kThreads, 0, stream()>>>(n, o->initial_guess, m->bv, w->x)));
             RG_CHECK_LAUNCH();

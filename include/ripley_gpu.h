@@ -187,7 +187,7 @@ typedef struct {
     int preconditioner;         /* RG_PRECOND_JACOBI                                        */
     double tolerance;           /* relative tolerance, default 1e-8                         */
     int64_t iter_max;           /* default 100000                                           */
-    int sweeps;                 /* Jacobi sweeps, default 1 (only 1 supported on the GPU)   */
+    int sweeps;                 /* Jacobi sweeps, default 1 (> 1: paso mode, FP64)          */
     int verbose;                /* print per-step residuals like paso                       */
     int accept_convergence_failure;
     int mode;                   /* RG_MODE_*                                                */

@@ -216,6 +216,17 @@ def main():
             g[f"sysred{tag}_{kname}_val"] = val
             g[f"sysred{tag}_{kname}_rhs"] = rhs
 
+    # paso Solver/PCG with Jacobi(sweeps) for sweeps = 2, 3 (Smoother.cpp:100-128) on the
+    # solve systems above
+    for tag in ("2d", "3d"):
+        ne = tuple(int(v) for v in g[f"solve{tag}_ne"])
+        pat = O.pattern(len(ne), ne)
+        for sw in (2, 3):
+            res = O.solve_paso(pat, g[f"solve{tag}_val"].copy(), g[f"solve{tag}_rhs"], tol=1e-10, sweeps=sw,
+                               use_ref=True)
+            g[f"sweep{tag}_{sw}_x"] = res.x
+            g[f"sweep{tag}_{sw}_iter"] = np.array(res.num_iter)
+
     # arrays already in the committed file keep their values (the solve cases depend on the
     # reference's OpenMP thread count at the 1e-13 level); new keys are added
     if os.path.exists(out):

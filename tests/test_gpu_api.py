@@ -240,3 +240,22 @@ def test_reduced_boundary_function_space(cuda):
     lin = Solution(dom).getX()[0] + 2.0 * Solution(dom).getX()[1]
     assert np.allclose(lin.interpolate(fs).toNumpy(), xr[:, 0] + 2 * xr[:, 1])
     assert np.allclose(lin.interpolate(FunctionOnBoundary(dom)).interpolate(fs).toNumpy(), xr[:, 0] + 2 * xr[:, 1])
+
+
+def test_jacobi_sweeps_through_solver_options(domain):
+    """SolverOptions.setNumSweeps(2): paso's Jacobi smoother with two sweeps as
+    preconditioner; the known answer u = 1 of test_PCG_JACOBI, and on a problem with
+    Dirichlet data the same solution as with one sweep."""
+    pde = LinearPDE(domain)
+    pde.setValue(A=kronecker(domain), D=1.0, Y=1.0)
+    pde.getSolverOptions().setNumSweeps(2)
+    assert check(pde.getSolution(), 1.0)
+    x = Solution(domain).getX()
+    us = []
+    for sw in (1, 2):
+        p = LinearPDE(domain)
+        p.setValue(A=kronecker(domain), Y=1.0, q=whereZero(x[0]))
+        p.getSolverOptions().setNumSweeps(sw)
+        p.getSolverOptions().setTolerance(1e-10)
+        us.append(p.getSolution())
+    assert Lsup(us[1] - us[0]) <= 1e-8 * Lsup(us[0])

@@ -285,7 +285,9 @@ def test_solver_errors_are_reported(cuda, golden):
     assert st == L.RG_NAN
     st, dg = R.solve(m, torch.zeros_like(rhs), x, R.opts())
     assert st == 0 and dg.converged and not bool(x.any())
-    st, _ = R.solve(m, rhs, x, R.opts(sweeps=2))
+    st, _ = R.solve(m, rhs, x, R.opts(sweeps=2, mode=L.RG_MODE_STANDARD))
+    assert st == L.RG_NOT_SUPPORTED
+    st, _ = R.solve(m, rhs, x, R.opts(sweeps=2, precision=L.RG_PREC_FP32_REFINE))
     assert st == L.RG_NOT_SUPPORTED
 
 
@@ -316,3 +318,23 @@ def test_residual_norms_before_and_after_balancing(cuda, golden):
     # the solution's residual is small relative to the right hand side
     l2s, _ = _residual_norms(m, rhs, x)
     assert l2s <= 1e-8 * np.linalg.norm(golden["solve3d_rhs"])
+
+
+@pytest.mark.parametrize("tag", ["2d", "3d"])
+@pytest.mark.parametrize("sweeps", [2, 3])
+def test_jacobi_sweeps_match_reference(cuda, golden, tag, sweeps):
+    """paso PCG with the Jacobi smoother of `sweeps` sweeps as preconditioner (the
+    reference's Smoother.cpp:161-184, used by PCG.cpp:152 and the initial guess of
+    Solver.cpp:181): iterations within one of the reference's, solution within 1e-8."""
+    d, m, rhs, _ = _system(golden, tag)
+    x = torch.zeros(d.n, dtype=torch.float64, device="cuda")
+    st, dg = R.solve(m, rhs, x, R.opts(tolerance=1e-10, sweeps=sweeps))
+    assert st == 0 and dg.converged
+    assert abs(int(dg.num_iter) - int(golden[f"sweep{tag}_{sweeps}_iter"])) <= 1
+    ref = golden[f"sweep{tag}_{sweeps}_x"]
+    assert np.linalg.norm(x.cpu().numpy() - ref) / np.linalg.norm(ref) < 1e-8
+    # a second solve with one sweep on the same (now balanced) matrix: the captured
+    # iterations are rebuilt for the other sweep count
+    x1 = torch.zeros_like(x)
+    st, dg1 = R.solve(m, rhs, x1, R.opts(tolerance=1e-10))
+    assert st == 0 and abs(int(dg1.num_iter) - int(golden[f"solve{tag}_iter"])) <= 1

@@ -375,3 +375,18 @@ def test_boundary_integrals_known_answer(dim, ne, nb, reduced):
     blocks = val.reshape(pat.nnz, nb * nb).sum(axis=0)  # column-major blocks: ir + nb ic
     assert np.allclose(blocks, Dm * area, rtol=1e-12, atol=1e-12)
     assert np.allclose(rhs.reshape(pat.n, nb).sum(axis=0), v * area, rtol=1e-12, atol=1e-12)
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+@pytest.mark.parametrize("sweeps", [2, 3])
+def test_jacobi_sweeps_solve_matches_reference(golden, dim, sweeps):
+    """paso Solver/PCG with Jacobi(sweeps): x = D^-1 b, then sweeps-1 times
+    x += D^-1 (b - A x) (Smoother.cpp:100-128), against the reference's own solve."""
+    tag = f"{dim}d"
+    ne = tuple(golden[f"solve{tag}_ne"])
+    pat = O.pattern(dim, ne)
+    res = O.solve_paso(pat, golden[f"solve{tag}_val"].copy(), golden[f"solve{tag}_rhs"], tol=1e-10, sweeps=sweeps)
+    assert res.status == 0 and res.converged
+    assert res.num_iter == int(golden[f"sweep{tag}_{sweeps}_iter"])
+    ref = golden[f"sweep{tag}_{sweeps}_x"]
+    assert np.linalg.norm(res.x - ref) / np.linalg.norm(ref) < 1e-10
