@@ -591,6 +591,67 @@ __global__ void __launch_bounds__(kThreads) k_update1_sys(int64_t nodes, double*
     }
 }
 
+// One more sweep of the block Jacobi smoother used as preconditioner when sweeps > 1
+// (Preconditioner_LocalSmoother_solve, paso/src/Smoother.cpp:161-184): t = b - A z here,
+// then z += Dinv t in k_sys_sweep_update.  mode 1 (inside the PCG loop) skips finished
+// solves.
+template <int NB>
+__global__ void __launch_bounds__(kThreads) k_sys_sweep_resid(int64_t nodes, const int32_t* __restrict__ ptr,
+                                                              const int32_t* __restrict__ idx,
+                                                              const double* __restrict__ val,
+                                                              const double* __restrict__ b,
+                                                              const double* __restrict__ z,
+                                                              double* __restrict__ t, const BScal* s, int mode)
+{
+    if (mode == 1 && s->done) return;
+    const int64_t N = nodes * NB;
+    RG_SROW_LOOP(N)
+    {
+        double acc = row < N ? brow_dot<NB>(ptr, idx, val, z, row / NB, (int)(row % NB), lane) : 0.0;
+        acc = group_sum(acc);
+        if (row < N && lane == 0) t[row] = b[row] - acc;
+    }
+}
+
+// z += Dinv t per node.  mode 0: that alone; mode 1 (the last sweep inside the PCG loop):
+// tau_next = z.b and beta = tau_next/tau; mode 2 (the last sweep of the PCG start): tau = z.b
+// and p = z.
+template <int NB>
+__global__ void __launch_bounds__(kThreads) k_sys_sweep_update(int64_t nodes, const double* __restrict__ dinv,
+                                                               const double* __restrict__ t,
+                                                               const double* __restrict__ b,
+                                                               double* __restrict__ z, double* __restrict__ p,
+                                                               ReduceBuf rb, BScal* s, int mode)
+{
+    if (mode == 1 && s->done) return;
+    double v[1] = {0.0};
+    for (int64_t i = gtid(); i < nodes; i += gstride()) {
+        double tt[NB];
+#pragma unroll
+        for (int c = 0; c < NB; ++c) tt[c] = t[i * NB + c];
+#pragma unroll
+        for (int ir = 0; ir < NB; ++ir) {
+            double dz = 0.0;
+#pragma unroll
+            for (int ic = 0; ic < NB; ++ic) dz = fma(dinv[i * NB * NB + ir + NB * ic], tt[ic], dz);
+            const double zz = z[i * NB + ir] + dz;
+            z[i * NB + ir] = zz;
+            if (mode == 2) p[i * NB + ir] = zz;
+            v[0] += zz * b[i * NB + ir];
+        }
+    }
+    if (mode == 0) return;
+    double r[1];
+    if (grid_reduce<1>(v, rb, r) && threadIdx.x == 0) {
+        if (mode == 1) {
+            s->tau_next = r[0];
+            s->beta = r[0] / s->tau;
+        } else {
+            s->tau = r[0];
+        }
+    }
+}
+
 // rs, x smoothing; stopping tests (PCG.cpp:307-347); p = z + beta p (PCG.cpp:193-218)
 __global__ void __launch_bounds__(kThreads) k_update2_sys(int64_t n, double* __restrict__ rs,
                                                           const double* __restrict__ r, double* __restrict__ x,
@@ -706,8 +767,8 @@ int solve_sys(Matrix* m, const double* rhs, double* x, const rg_solver_opts* o, 
                "solver: only PCG with the Jacobi preconditioner is implemented");
     RG_REQUIRE(o->tolerance >= 100. * EPS, "Solver: Tolerance is too small.");
     RG_REQUIRE(o->tolerance <= 1., "Solver: Tolerance must be less than one.");
-    if (o->sweeps > 1 || o->precision != RG_PREC_FP64 || o->initial_guess) {
-        set_error("solver: PDE systems are solved by the paso algorithm in FP64 with one Jacobi sweep");
+    if (o->precision != RG_PREC_FP64 || o->initial_guess) {
+        set_error("solver: PDE systems are solved by the paso algorithm in FP64");
         return RG_NOT_SUPPORTED;
     }
     SysWorkspace* w = ensure_ws(m);
@@ -721,6 +782,16 @@ int solve_sys(Matrix* m, const double* rhs, double* x, const rg_solver_opts* o, 
     const int gv = grid_for(N, kThreads, 8);
     const int gn = grid_for(nodes, kThreads, 8);
     const int gr = grid_for(N, kThreads / kLpr, 8);
+    // sweeps - 1 more block Jacobi sweeps on z (the preconditioned b), t in the spare buffer q
+    auto sweeps = [&](const double* b, double* z, double* p, int last_mode) {
+        for (int k = 1; k < o->sweeps; ++k) {
+            const int mode = k == o->sweeps - 1 ? last_mode : 0;
+            RG_TIMED(T_PASO_UPDATE1, (k_sys_sweep_resid<NB><<<gr, kThreads, 0, stream()>>>(
+                                         nodes, d->ptr, d->idx, m->val, b, z, w->q, s, mode)));
+            RG_TIMED(T_PASO_UPDATE1, (k_sys_sweep_update<NB><<<gn, kThreads, 0, stream()>>>(
+                                         nodes, m->dinv, w->q, b, z, p, rbuf(w), s, mode)));
+        }
+    };
     dg.set_up_time = now_s() - t0;
     RG_TIMED(T_NORMS, (k_scale_norms<<<gv, kThreads, 0, stream()>>>(N, m->bv, rhs, w->bb, rbuf(w), s)));
     RG_CHECK_LAUNCH();
@@ -738,6 +809,7 @@ int solve_sys(Matrix* m, const double* rhs, double* x, const rg_solver_opts* o, 
     } else {
         // initial guess: block Jacobi of the balanced rhs (Solver.cpp:181)
         RG_TIMED(T_VECTOR, (k_block_jacobi<NB><<<gn, kThreads, 0, stream()>>>(nodes, m->dinv, w->bb, w->x)));
+        sweeps(w->bb, w->x, nullptr, 0);
         RG_CHECK_LAUNCH();
         long long totIter = 1;
         double last2 = n2b, lastm = nmb;
@@ -774,6 +846,7 @@ int solve_sys(Matrix* m, const double* rhs, double* x, const rg_solver_opts* o, 
             RG_TIMED(T_VECTOR, (k_init_sys<NB><<<gn, kThreads, 0, stream()>>>(nodes, w->r, w->x, m->dinv, w->rs,
                                                                              w->x2, w->p, w->z, rbuf(w), s, tol,
                                                                              cnt)));
+            sweeps(w->r, w->z, w->p, 2);  // the first v = prec(r): p and tau
             RG_CHECK_LAUNCH();
             // iterations in chunks between polls of the done flag
             const int chunk = 16;
@@ -784,6 +857,7 @@ int solve_sys(Matrix* m, const double* rhs, double* x, const rg_solver_opts* o, 
                                               nodes, d->ptr, d->idx, m->val, w->p, w->q, rbuf(w), s)));
                     RG_TIMED(T_PASO_UPDATE1, (k_update1_sys<NB><<<gn, kThreads, 0, stream()>>>(
                                                  nodes, w->r, w->q, w->rs, w->x2, w->p, m->dinv, w->z, rbuf(w), s)));
+                    sweeps(w->r, w->z, nullptr, 1);
                     RG_TIMED(T_PASO_UPDATE2, (k_update2_sys<<<gv, kThreads, 0, stream()>>>(
                                                  N, w->rs, w->r, w->x, w->x2, w->z, w->p, rbuf(w), s)));
                 }

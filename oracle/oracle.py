@@ -294,8 +294,9 @@ def insert_constraint_block(pat: Pattern, nb, val, rhs, q, r=None):
                                      _dp(q), _dp(rr) if rr is not None else None)
 
 
-def solve_paso_block(pat: Pattern, nb, val, b, tol=1e-8, iter_max=100000, use_ref=False) -> SolveResult:
-    """paso::Solver PCG + block Jacobi on a block CSR matrix; ``val`` is balanced IN PLACE."""
+def solve_paso_block(pat: Pattern, nb, val, b, tol=1e-8, iter_max=100000, use_ref=False, sweeps=1) -> SolveResult:
+    """paso::Solver PCG + block Jacobi (``sweeps`` sweeps) on a block CSR matrix; ``val`` is
+    balanced IN PLACE."""
     b = np.ascontiguousarray(b, dtype=np.float64).copy()
     x = np.zeros(pat.n * nb)
     if use_ref:
@@ -304,13 +305,14 @@ def solve_paso_block(pat: Pattern, nb, val, b, tol=1e-8, iter_max=100000, use_re
         rn = C.c_double(0)
         conv = C.c_int(0)
         st = R.ref_solve_block(C.c_int64(pat.n), int(nb), _ip(pat.ptr), _ip(pat.idx), _dp(val), _dp(b), _dp(x),
-                               C.c_double(tol), C.c_int64(iter_max), C.byref(it), C.byref(rn), C.byref(conv))
+                               C.c_double(tol), C.c_int64(iter_max), int(sweeps), C.byref(it), C.byref(rn),
+                               C.byref(conv))
         if st < 0:
             raise RuntimeError(R.ref_last_error().decode())
         return SolveResult(x, st, it.value, rn.value, bool(conv.value))
     bv = np.zeros(pat.n * nb)
     d = _Diag()
-    o = _Opts(tol, iter_max, 1, 0)
+    o = _Opts(tol, iter_max, int(sweeps), 0)
     st = lib().ro_solve_paso_block(C.c_int64(pat.n), int(nb), _ip(pat.ptr), _ip(pat.idx), _dp(val), _dp(b),
                                    _dp(x), _dp(bv), C.byref(o), C.byref(d))
     return SolveResult(x, st, d.num_iter, d.residual_norm, bool(d.converged), bv)

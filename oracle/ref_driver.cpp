@@ -521,7 +521,8 @@ int ref_solve(int64_t n, int32_t* ptr, int32_t* idx, double* val, double* b, dou
 
 // paso::Solver with PCG + (block) Jacobi on a block CSR matrix with block size nb
 int ref_solve_block(int64_t nodes, int nb, int32_t* ptr, int32_t* idx, double* val, double* b, double* x,
-                    double tol, int64_t iter_max, int64_t* num_iter, double* residual_norm, int* converged)
+                    double tol, int64_t iter_max, int sweeps, int64_t* num_iter, double* residual_norm,
+                    int* converged)
 {
     try {
         auto A = std::make_shared<paso::SystemMatrix<double>>();
@@ -538,6 +539,7 @@ int ref_solve_block(int64_t nodes, int nb, int32_t* ptr, int32_t* idx, double* v
         paso::Options o;
         o.tolerance = tol;
         o.iter_max = (paso::dim_t)iter_max;
+        o.sweeps = sweeps;
         paso::Performance pp;
         paso::SolverResult res = paso::Solver(A, x, b, &o, &pp);
         *num_iter = o.num_iter;

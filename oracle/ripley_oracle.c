@@ -1007,9 +1007,29 @@ static int invert_block(int nb, const double* A, double* inv)
     return 0;
 }
 
+/* the block Jacobi smoother with `sweeps` sweeps (Smoother.cpp:161-184): x = D^-1 b, then
+   sweeps-1 times x += D^-1 (b - A x) with D the main diagonal blocks */
+static void prec_block(int64_t nodes, int nb, const int32_t* ptr, const int32_t* idx, const double* val,
+                       const double* dinv, int sweeps, const double* b, double* x)
+{
+    jacobi_block(nodes, nb, dinv, b, x);
+    if (sweeps <= 1) return;
+    const int64_t n = nodes * nb;
+    double* t = (double*)malloc(sizeof(double) * (size_t)n);
+    double* c = (double*)malloc(sizeof(double) * (size_t)n);
+    for (int s = 1; s < sweeps; ++s) {
+        memcpy(t, b, sizeof(double) * (size_t)n);
+        ro_spmv_block(nodes, nb, ptr, idx, val, -1.0, x, 1.0, t);
+        jacobi_block(nodes, nb, dinv, t, c);
+        for (int64_t i = 0; i < n; ++i) x[i] += c[i];
+    }
+    free(t);
+    free(c);
+}
+
 /* Solver_PCG (PCG.cpp:62-367) on a block matrix */
 static int pcg_block(int64_t nodes, int nb, const int32_t* ptr, const int32_t* idx, const double* val,
-                     const double* dinv, double* r, double* x, int64_t* iter, double* tol)
+                     const double* dinv, int sweeps, double* r, double* x, int64_t* iter, double* tol)
 {
     const int64_t n = nodes * nb;
     double* rs = (double*)malloc(sizeof(double) * (size_t)n);
@@ -1024,7 +1044,7 @@ static int pcg_block(int64_t nodes, int nb, const int32_t* ptr, const int32_t* i
     int converge = 0, maxflag = 0, brk = 0;
     while (!(converge || maxflag || brk)) {
         ++num_iter;
-        jacobi_block(nodes, nb, dinv, r, v);
+        prec_block(nodes, nb, ptr, idx, val, dinv, sweeps, r, v);
         const double sum1 = dot(n, v, r);
         tau_old = tau;
         tau = sum1;
@@ -1069,7 +1089,7 @@ static int pcg_block(int64_t nodes, int nb, const int32_t* ptr, const int32_t* i
     return RO_OK;
 }
 
-/* paso::Solver (Solver.cpp:46-330), PCG + block Jacobi (sweeps = 1), block matrix balanced
+/* paso::Solver (Solver.cpp:46-330), PCG + block Jacobi (opts->sweeps), block matrix balanced
    in place per scalar row (SparseMatrix::maxAbsRow_CSR_OFFSET0 and applyDiagonal). */
 int ro_solve_paso_block(int64_t nodes, int nb, const int32_t* ptr, const int32_t* idx, double* val,
                         const double* b, double* x, double* bv, const ro_opts* opts, ro_diag* diag)
@@ -1112,7 +1132,7 @@ int ro_solve_paso_block(int64_t nodes, int nb, const int32_t* ptr, const int32_t
             if (kd < 0 || invert_block(nb, val + kd * bs, dinv + i * bs)) err = RO_INPUT_ERROR;
         }
         if (err == RO_OK) {
-            jacobi_block(nodes, nb, dinv, r, x);
+            prec_block(nodes, nb, ptr, idx, val, dinv, opts->sweeps, r, x);
             int64_t totIter = 1;
             int fin = 0;
             double last2 = n2b, lastm = nmb;
@@ -1135,7 +1155,7 @@ int ro_solve_paso_block(int64_t nodes, int nb, const int32_t* ptr, const int32_t
                     double tol = tolerance * fmin(n2b, 0.1 * n2r / nmr * nmb);
                     last2 = n2r;
                     lastm = nmr;
-                    int st = pcg_block(nodes, nb, ptr, idx, val, dinv, r, x, &cnt, &tol);
+                    int st = pcg_block(nodes, nb, ptr, idx, val, dinv, opts->sweeps, r, x, &cnt, &tol);
                     totIter += cnt;
                     if (st == RO_OK) {
                         fin = 0;

@@ -227,6 +227,18 @@ def main():
             g[f"sweep{tag}_{sw}_x"] = res.x
             g[f"sweep{tag}_{sw}_iter"] = np.array(res.num_iter)
 
+    # the Lame systems with block Jacobi of 2 sweeps
+    for dim in (2, 3):
+        tag = f"{dim}d"
+        ne = tuple(int(v) for v in g[f"lame{tag}_ne"])
+        dx = tuple(1.0 / e for e in ne)
+        pat = O.pattern(dim, ne)
+        val, rhs = O.assemble_system(dim, ne, dx, pat, dim, A=(O.CONSTANT, g[f"lame{tag}_A"]),
+                                     Y=(O.EXPANDED, g[f"lame{tag}_Y"]), use_ref=True)
+        O.insert_constraint_block(pat, dim, val, rhs, g[f"lame{tag}_q"])
+        res = O.solve_paso_block(pat, dim, val, rhs, tol=1e-10, use_ref=True, sweeps=2)
+        g[f"lamesw{tag}_x"], g[f"lamesw{tag}_iter"] = res.x, np.array(res.num_iter)
+
     # arrays already in the committed file keep their values (the solve cases depend on the
     # reference's OpenMP thread count at the 1e-13 level); new keys are added
     if os.path.exists(out):
