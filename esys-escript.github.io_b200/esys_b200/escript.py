@@ -58,13 +58,13 @@ class FunctionSpace:
 
     def __eq__(self, other):
         return (isinstance(other, FunctionSpace) and other._domain is self._domain and
-                other._storage() == self._storage())
+                other.getTypeCode() == self.getTypeCode())
 
     def __ne__(self, other):
         return not self.__eq__(other)
 
     def __hash__(self):
-        return hash((id(self._domain), self._storage()))
+        return hash((id(self._domain), self.getTypeCode()))
 
     def _storage(self):
         """Where values live: 'nodes' (DOF = nodes on one rank), 'qp', 'elem', 'face' (the face
@@ -248,14 +248,22 @@ class Data:
 
     # ---- interpolation
     def interpolate(self, fs):
-        if fs == self._fs:
-            return self.copy()
-        if self.isConstant():
-            return Data._wrap(self._t.clone(), self._shape, fs)
         src, dst = self._fs._storage(), fs._storage()
+        if not _can_interpolate(src, dst):
+            raise ValueError(f"interpolate: cannot interpolate from {self._fs} to {fs}")
+        if src == dst or self.isConstant():
+            # the same points (the node spaces of one rank are one set of nodes) or a constant
+            return Data._wrap(self._t.clone(), self._shape, fs)
         dom = self._fs.getDomain()
         if fs.getDomain() is not dom:
             raise ValueError("interpolate: function spaces belong to different domains")
+        if (src, dst) in (("elem", "qp"), ("rface", "face")):
+            # ReducedElements -> Elements, ReducedFaceElements -> FaceElements: the value of a
+            # sample at each of its points (RipleyDomain::probeInterpolationOnDomain allows both)
+            q = fs.getNumDataPointsPerSample()
+            ncomp = self._t.shape[1]
+            out = self._dev()[:, None, :].expand(-1, q, ncomp).reshape(-1, ncomp).contiguous()
+            return Data._wrap(out, self._shape, fs)
         if src == "nodes" and dst in ("qp", "elem"):
             ncomp = self._t.shape[1]
             out = torch.empty((fs._num_points(), ncomp), dtype=torch.float64, device=DEVICE)
@@ -373,6 +381,18 @@ class Data:
         return f"Data(shape={self._shape}, fs={self._fs}, points={0 if self._t is None else self._t.shape[0]})"
 
     __repr__ = __str__
+
+
+def _can_interpolate(src, dst):
+    """RipleyDomain::probeInterpolationOnDomain (ripley/src/RipleyDomain.cpp:288-324) by
+    storage: nodes go anywhere, element points stay on elements, face points on faces."""
+    if src == "nodes":
+        return True
+    if src in ("qp", "elem"):
+        return dst in ("qp", "elem")
+    if src in ("face", "rface"):
+        return dst in ("face", "rface")
+    return src == dst
 
 
 def _common_fs(a, b):
@@ -833,6 +853,61 @@ def _tensor_from_ptr(ptr, count, dtype):
 # LinearPDE / Poisson (escriptcore/py_src/linearPDEs.py)
 # ---------------------------------------------------------------------------------------------
 
+class IllegalCoefficient(ValueError):
+    """An unknown coefficient name (linearPDEs.py:56)."""
+
+
+class IllegalCoefficientValue(ValueError):
+    """A coefficient value of the wrong shape (linearPDEs.py:63)."""
+
+
+class IllegalCoefficientFunctionSpace(ValueError):
+    """A coefficient on a function space that cannot be interpolated to the one the PDE
+    needs (linearPDEs.py:69)."""
+
+
+class UndefinedPDEError(ValueError):
+    """The number of equations or solutions cannot be determined yet (linearPDEs.py:75)."""
+
+
+# index pattern of each coefficient: E = equation, S = solution component, D = space
+# dimension; E (S) is dropped when the PDE has one equation (solution component)
+_PATTERN = {"A": "EDSD", "B": "EDS", "C": "ESD", "D": "ES", "X": "ED", "Y": "E", "d": "ES", "y": "E",
+            "q": "S", "r": "S"}
+
+
+def _pattern_of(name):
+    return _PATTERN[name[:-len("_reduced")] if name.endswith("_reduced") else name]
+
+
+def _shape_for(pattern, dim, ne, ns):
+    out = []
+    for t in pattern:
+        if t == "E":
+            if ne > 1:
+                out.append(ne)
+        elif t == "S":
+            if ns > 1:
+                out.append(ns)
+        else:
+            out.append(dim)
+    return tuple(out)
+
+
+def _estimate_counts(pattern, dim, shape):
+    """(numEquations, numSolutions) a coefficient of this shape implies (None where the
+    coefficient says nothing about it), or None if no counts fit: the largest counts whose
+    shape matches, as PDECoef.estimateNumEquationsAndNumSolutions does."""
+    shape = tuple(shape)
+    top = (max(shape) if shape else 0) + 1
+    es = list(range(1, top + 1)) if "E" in pattern else [None]
+    us = list(range(1, top + 1)) if "S" in pattern else [None]
+    for e, u in sorted(((e, u) for e in es for u in us), key=lambda c: -((c[0] or 0) + (c[1] or 0))):
+        if _shape_for(pattern, dim, e or 1, u or 1) == shape:
+            return e, u
+    return None
+
+
 _INTERIOR = ("A", "B", "C", "D", "X", "Y")
 _REDUCED = ("A_reduced", "B_reduced", "C_reduced", "D_reduced", "X_reduced", "Y_reduced")
 _BOUNDARY = ("d", "y")
@@ -847,17 +922,12 @@ class LinearPDE:
     + d u = n_i X_i + y on the boundary and u = r where q > 0 (single equation)."""
 
     def __init__(self, domain, numEquations=None, numSolutions=None, isComplex=False, debug=False):
-        ne = numEquations if numEquations is not None else numSolutions
-        ns = numSolutions if numSolutions is not None else ne
-        ne = 1 if ne is None else int(ne)
-        ns = 1 if ns is None else int(ns)
-        if ne != ns:
-            raise ValueError("number of equations and number of solutions don't match")
-        if ne > 3:
-            raise NotImplementedError("PDE systems of more than 3 equations are not part of the GPU path")
         if isComplex:
             raise NotImplementedError("complex PDEs are not part of the GPU path")
-        self._nb = ne
+        self._ne = None if numEquations is None else int(numEquations)
+        self._ns = None if numSolutions is None else int(numSolutions)
+        if max(self._ne or 0, self._ns or 0) > 3:
+            raise NotImplementedError("PDE systems of more than 3 equations are not part of the GPU path")
         self._domain = domain
         self._coef = {}
         self._options = SolverBuddy()
@@ -868,6 +938,8 @@ class LinearPDE:
         self._solution = None
         self._debug = debug
         self._symmetric = False
+        self._reduce_sol = False
+        self._reduce_eq = False
 
     # ---- escript API
     def getDomain(self):
@@ -877,10 +949,30 @@ class LinearPDE:
         return self._domain.getDim()
 
     def getNumEquations(self):
-        return self._nb
+        """The number of equations; the number of solutions when only that is known."""
+        if self._ne is None:
+            if self._ns is None:
+                raise UndefinedPDEError("Number of equations is undefined. Please specify argument numEquations.")
+            self._ne = self._ns
+        return self._ne
 
     def getNumSolutions(self):
-        return self._nb
+        """The number of solution components; the number of equations when only that is known."""
+        if self._ns is None:
+            if self._ne is None:
+                raise UndefinedPDEError("Number of solution is undefined. Please specify argument numSolutions.")
+            self._ns = self._ne
+        return self._ns
+
+    @property
+    def _nb(self):
+        """Block size of the operator: the GPU path solves square systems of 1..3 equations."""
+        ne, ns = self.getNumEquations(), self.getNumSolutions()
+        if ne != ns:
+            raise ValueError("number of equations and number of solutions don't match")
+        if ne > 3:
+            raise NotImplementedError("PDE systems of more than 3 equations are not part of the GPU path")
+        return ne
 
     def getSolverOptions(self):
         return self._options
@@ -898,11 +990,61 @@ class LinearPDE:
     def isSymmetric(self):
         return self._symmetric
 
+    # reduced order (linearPDEs.py:854-960).  On ripley the reduced solution space has the same
+    # nodes (Q1 has no lower order, RipleyDomain::newSystemMatrix accepts both), so only the
+    # function spaces of the solution, q and r change.
+    def _set_reduced(self, sol=None, eq=None):
+        if (sol is not None and sol != self._reduce_sol) or (eq is not None and eq != self._reduce_eq):
+            if self._coef:
+                raise RuntimeError("order cannot be altered after coefficients have been defined.")
+            if sol is not None:
+                self._reduce_sol = sol
+            if eq is not None:
+                self._reduce_eq = eq
+            self._operator_valid = self._rhs_valid = False
+            self._solution = None
+
+    def setReducedOrderOn(self):
+        self._set_reduced(True, True)
+
+    def setReducedOrderOff(self):
+        self._set_reduced(False, False)
+
+    def setReducedOrderTo(self, flag=False):
+        self._set_reduced(bool(flag), bool(flag))
+
+    def setReducedOrderForSolutionOn(self):
+        self._set_reduced(sol=True)
+
+    def setReducedOrderForSolutionOff(self):
+        self._set_reduced(sol=False)
+
+    def setReducedOrderForSolutionTo(self, flag=False):
+        self._set_reduced(sol=bool(flag))
+
+    def setReducedOrderForEquationOn(self):
+        self._set_reduced(eq=True)
+
+    def setReducedOrderForEquationOff(self):
+        self._set_reduced(eq=False)
+
+    def setReducedOrderForEquationTo(self, flag=False):
+        self._set_reduced(eq=bool(flag))
+
+    def reduceSolutionOrder(self):
+        return self._reduce_sol
+
+    def reduceEquationOrder(self):
+        return self._reduce_eq
+
     def getFunctionSpaceForEquation(self):
-        return Solution(self._domain)
+        return ReducedSolution(self._domain) if self._reduce_eq else Solution(self._domain)
 
     def getFunctionSpaceForSolution(self):
-        return Solution(self._domain)
+        return ReducedSolution(self._domain) if self._reduce_sol else Solution(self._domain)
+
+    def hasCoefficient(self, name):
+        return name in _ALL or name in _UNSUPPORTED
 
     def getFunctionSpaceForCoefficient(self, name):
         if name in _INTERIOR:
@@ -914,66 +1056,128 @@ class LinearPDE:
         if name in _BOUNDARY_REDUCED:
             return ReducedFunctionOnBoundary(self._domain)
         if name in _CONSTRAINT:
-            return Solution(self._domain)
-        raise ValueError(f"unknown coefficient {name}")
+            return self.getFunctionSpaceForSolution()
+        raise IllegalCoefficient(f"illegal coefficient {name} requested for general PDE.")
+
+    def getShapeOfCoefficient(self, name):
+        if name not in _ALL:
+            raise IllegalCoefficient(f"illegal coefficient {name} requested for general PDE.")
+        return _shape_for(_pattern_of(name), self.getDim(), self.getNumEquations(), self.getNumSolutions())
 
     def _shape_of(self, name):
-        d, n = self.getDim(), self._nb
-        base = name[:-len("_reduced")] if name.endswith("_reduced") else name
-        if n == 1:
-            return {"A": (d, d), "B": (d,), "C": (d,), "D": (), "X": (d,), "Y": (), "d": (),
-                    "y": (), "q": (), "r": ()}[base]
-        # LinearPDE coefficient shapes of a system (linearPDEs.py: A (n, d, n, d), ...)
-        return {"A": (n, d, n, d), "B": (n, d, n), "C": (n, n, d), "D": (n, n), "X": (n, d), "Y": (n,),
-                "d": (n, n), "y": (n,), "q": (n,), "r": (n,)}[base]
+        return self.getShapeOfCoefficient(name)
 
     def createSolution(self):
-        if self._nb == 1:
-            return Scalar(0.0, Solution(self._domain), expanded=True)
-        return Data(0.0, (self._nb,), Solution(self._domain), expanded=True)
+        ns = self.getNumSolutions()
+        fs = self.getFunctionSpaceForSolution()
+        if ns == 1:
+            return Scalar(0.0, fs, expanded=True)
+        return Data(0.0, (ns,), fs, expanded=True)
 
     def createRightHandSide(self):
-        return self.createSolution()
+        ne = self.getNumEquations()
+        fs = self.getFunctionSpaceForEquation()
+        if ne == 1:
+            return Scalar(0.0, fs, expanded=True)
+        return Data(0.0, (ne,), fs, expanded=True)
 
     def getCoefficient(self, name):
         if name in self._coef:
             return self._coef[name]
-        if name in _ALL + _UNSUPPORTED:
+        if self.hasCoefficient(name):
             return Data()
-        raise ValueError(f"unknown coefficient {name}")
+        raise IllegalCoefficient(f"illegal coefficient {name} requested for general PDE.")
+
+    def _coef_data(self, name, value):
+        """The coefficient as Data on its function space with its shape; raises
+        IllegalCoefficientFunctionSpace / IllegalCoefficientValue."""
+        fs = self.getFunctionSpaceForCoefficient(name)
+        shape = self.getShapeOfCoefficient(name)
+        if isinstance(value, Data):
+            try:
+                dat = value.interpolate(fs)
+            except ValueError as e:
+                raise IllegalCoefficientFunctionSpace(f"{value.getFunctionSpace()} cannot be interpolated to {fs}: "
+                                                      f"{e}") from None
+        else:
+            a = np.asarray(value, dtype=np.float64)
+            if a.shape != shape:
+                raise IllegalCoefficientValue(f"Coefficient {name}: expected shape {shape}, got {a.shape}")
+            dat = Data(a, shape, fs)
+        if dat._shape != shape:
+            raise IllegalCoefficientValue(f"Coefficient {name}: expected shape {shape}, got {dat._shape}")
+        return dat
 
     def setValue(self, **coefficients):
-        """LinearProblem.setValue (linearPDEs.py:1392-1449 / 2114-2207)."""
+        """LinearProblem.setValue (linearPDEs.py:1392-1449 / 2114-2207): unknown names raise
+        IllegalCoefficient; the numbers of equations and solutions, when not given, come from
+        the first coefficients' shapes; a value on a function space that cannot be
+        interpolated to the coefficient's goes to the reduced coefficient of the same name
+        where there is one."""
+        for name in coefficients:
+            if not self.hasCoefficient(name):
+                raise IllegalCoefficient(f"Attempt to set unknown coefficient {name}")
+        for name, value in coefficients.items():
+            if name in _UNSUPPORTED and not (value is None or (isinstance(value, Data) and value.isEmpty())):
+                raise NotImplementedError(f"coefficient {name} is not part of the GPU path")
+
+        def empty(v):
+            return v is None or (isinstance(v, Data) and v.isEmpty())
+
+        if self._ne is None or self._ns is None:
+            for name, value in sorted(coefficients.items()):
+                if empty(value) or name in _UNSUPPORTED:
+                    continue
+                shape = value.getShape() if isinstance(value, Data) else np.asarray(value).shape
+                est = _estimate_counts(_pattern_of(name), self.getDim(), shape)
+                if est is None:
+                    raise IllegalCoefficientValue(f"Illegal shape {shape} of coefficient {name}")
+                if self._ne is None and est[0] is not None:
+                    self._ne = est[0]
+                if self._ns is None and est[1] is not None:
+                    self._ns = est[1]
+        self.getNumEquations()
+        self.getNumSolutions()
         for name, value in coefficients.items():
             if name in _UNSUPPORTED:
-                if value is None or (isinstance(value, Data) and value.isEmpty()):
-                    continue
-                raise NotImplementedError(f"coefficient {name} is not part of the GPU path")
-            if name not in _ALL:
-                raise ValueError(f"illegal coefficient {name} requested for general PDE.")
-            if value is None or (isinstance(value, Data) and value.isEmpty()):
+                continue
+            target = name
+            if empty(value):
                 self._coef.pop(name, None)
             else:
-                fs = self.getFunctionSpaceForCoefficient(name)
-                shape = self._shape_of(name)
-                if isinstance(value, Data):
-                    dat = value if value._fs == fs else value.interpolate(fs)
-                    dat = dat.copy()
-                    if dat._shape != shape:
-                        raise ValueError(f"coefficient {name}: expected shape {shape}, got {dat._shape}")
-                else:
-                    a = np.asarray(value, dtype=np.float64)
-                    if a.shape == () and shape != ():
-                        raise ValueError(f"coefficient {name}: expected shape {shape}")
-                    dat = Data(a, shape, fs)
-                self._coef[name] = dat
-            if name in ("A", "B", "C", "D", "d", "A_reduced", "B_reduced", "C_reduced", "D_reduced", "d_reduced"):
-                self._operator_valid = False
-            if name in ("X", "Y", "y", "r", "X_reduced", "Y_reduced", "y_reduced"):
-                self._rhs_valid = False
-            if name == "q":
-                self._operator_valid = False
-                self._rhs_valid = False
+                try:
+                    dat = self._coef_data(name, value)
+                except IllegalCoefficientFunctionSpace:
+                    red = name + "_reduced"
+                    if red in _ALL and red not in coefficients:
+                        dat = self._coef_data(red, value)
+                        target = red
+                    else:
+                        raise
+                self._coef[target] = dat
+            self._altered(target)
+        self._solution = None
+
+    def _altered(self, name):
+        if name in ("A", "B", "C", "D", "d", "A_reduced", "B_reduced", "C_reduced", "D_reduced", "d_reduced"):
+            self._operator_valid = False
+        if name in ("X", "Y", "y", "r", "X_reduced", "Y_reduced", "y_reduced"):
+            self._rhs_valid = False
+        if name == "q":
+            self._operator_valid = False
+            self._rhs_valid = False
+
+    def resetRightHandSideCoefficients(self):
+        """Removes the coefficients that define the right hand side (X, Y, y, their reduced
+        forms and r)."""
+        for name in ("X", "Y", "y", "X_reduced", "Y_reduced", "y_reduced", "r"):
+            if self._coef.pop(name, None) is not None:
+                self._altered(name)
+        self._solution = None
+
+    def resetAllCoefficients(self):
+        self._coef.clear()
+        self._operator_valid = self._rhs_valid = False
         self._solution = None
 
     def _coef_c(self, name, keep):
@@ -1050,7 +1254,9 @@ class LinearPDE:
         """LinearPDE.getSolution (linearPDEs.py:1861-1879)."""
         if self._solution is None:
             mat, f = self.getSystem()
-            self._solution = mat.solve(f, self._options)
+            u = mat.solve(f, self._options)
+            fs = self.getFunctionSpaceForSolution()
+            self._solution = u if u.getFunctionSpace() == fs else u.interpolate(fs)
         return self._solution
 
     def getResidualNorms(self, u=None):

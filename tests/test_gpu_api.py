@@ -110,8 +110,11 @@ def test_unsupported_features_raise(cuda):
     dom = ripley.Rectangle(4, 4)
     with pytest.raises(NotImplementedError):
         LinearPDE(dom, numEquations=4)
+    # a non-square PDE can be defined (as in escript) but not solved on the GPU path
+    ns = LinearPDE(dom, numEquations=2, numSolutions=3)
+    ns.setValue(D=np.ones((2, 3)))
     with pytest.raises(ValueError):
-        LinearPDE(dom, numEquations=2, numSolutions=3)
+        ns.getSolution()
     pde = LinearPDE(dom)
     with pytest.raises(NotImplementedError):
         pde.setValue(y_contact=1.0)
@@ -259,3 +262,112 @@ def test_jacobi_sweeps_through_solver_options(domain):
         p.getSolverOptions().setTolerance(1e-10)
         us.append(p.getSolution())
     assert Lsup(us[1] - us[0]) <= 1e-8 * Lsup(us[0])
+
+
+
+# ---- LinearPDE coefficient handling, after escriptcore/test/python/test_linearPDEs.py
+# (Test_LinearPDE: test_setCoefficient_*_Scalar / _System, test_reducedOn,
+# test_setCoefficient_WithIllegalFunctionSpace, test_resetCoefficient_WithWrongShape)
+from esys_b200.escript import (IllegalCoefficient, IllegalCoefficientValue,  # noqa: E402
+                               IllegalCoefficientFunctionSpace, UndefinedPDEError, ReducedFunction,
+                               FunctionOnBoundary, ReducedFunctionOnBoundary, ReducedSolution, Vector)
+
+_SCALAR = {"A": lambda d: np.ones((d, d)), "B": lambda d: np.ones(d), "C": lambda d: np.ones(d),
+           "D": lambda d: 1.0, "X": lambda d: np.ones(d), "Y": lambda d: 1.0, "y": lambda d: 1.0,
+           "d": lambda d: 1.0}
+_FS = {"A": Function, "B": Function, "C": Function, "D": Function, "X": Function, "Y": Function,
+       "y": FunctionOnBoundary, "d": FunctionOnBoundary}
+_RHS = ("X", "Y", "y")
+
+
+@pytest.fixture
+def dom2(cuda):
+    return ripley.Rectangle(6, 5)
+
+
+@pytest.mark.parametrize("name", sorted(_SCALAR))
+@pytest.mark.parametrize("reduced", [False, True])
+def test_set_coefficient_scalar(dom2, name, reduced):
+    d = dom2.getDim()
+    key = name + ("_reduced" if reduced else "")
+    pde = LinearPDE(dom2)
+    pde.setValue(**{key: _SCALAR[name](d)})
+    c = pde.getCoefficient(key)
+    fs = _FS[name](dom2)
+    if reduced:
+        fs = {Function(dom2): ReducedFunction(dom2),
+              FunctionOnBoundary(dom2): ReducedFunctionOnBoundary(dom2)}[fs]
+    assert (c.getShape(), c.getFunctionSpace(), pde.getNumSolutions(), pde.getNumEquations()) == \
+        (np.shape(_SCALAR[name](d)), fs, 1, 1)
+    pde.resetRightHandSideCoefficients()
+    assert pde.getCoefficient(key).isEmpty() == (name in _RHS)
+
+
+@pytest.mark.parametrize("name", ["A", "B", "C", "D", "X", "Y", "d", "y"])
+def test_set_coefficient_system_infers_counts(dom2, name):
+    """LinearPDE(domain) without counts: the first coefficient's shape sets them."""
+    d, N = dom2.getDim(), 3
+    shapes = {"A": (N, d, N, d), "B": (N, d, N), "C": (N, N, d), "D": (N, N), "X": (N, d), "Y": (N,),
+              "d": (N, N), "y": (N,)}
+    pde = LinearPDE(dom2)
+    pde.setValue(**{name: np.ones(shapes[name])})
+    c = pde.getCoefficient(name)
+    assert c.getShape() == shapes[name] and c.getFunctionSpace() == _FS[name](dom2)
+    assert pde.getNumEquations() == N
+    if name not in ("X", "Y", "y"):
+        assert pde.getNumSolutions() == N
+
+
+def test_counts_from_q_and_r(dom2):
+    pde = LinearPDE(dom2, numEquations=3)
+    pde.setValue(r=1.0)
+    assert pde.getCoefficient("r").getFunctionSpace() == Solution(dom2)
+    pde.resetRightHandSideCoefficients()
+    assert pde.getCoefficient("r").isEmpty()
+    pde2 = LinearPDE(dom2)
+    with pytest.raises(UndefinedPDEError):
+        pde2.getNumEquations()
+
+
+def test_reduced_order_on(dom2):
+    """test_reducedOn: u = 1 with the solution on ReducedSolution; q goes there too; the
+    order cannot change once a coefficient is set."""
+    pde = LinearPDE(dom2)
+    x = dom2.getX()
+    pde.setReducedOrderOn()
+    pde.setValue(A=kronecker(dom2), D=x[0], Y=x[0])
+    u = pde.getSolution()
+    assert u.getFunctionSpace() == ReducedSolution(dom2)
+    assert check(u, 1.0)
+    with pytest.raises(RuntimeError):
+        pde.setReducedOrderOff()
+    p2 = LinearPDE(dom2, numEquations=3)
+    p2.setReducedOrderOn()
+    p2.setValue(q=np.ones(3))
+    assert p2.getCoefficient("q").getFunctionSpace() == ReducedSolution(dom2)
+
+
+def test_coefficient_errors(dom2):
+    pde = LinearPDE(dom2)
+    with pytest.raises(IllegalCoefficientFunctionSpace):
+        pde.setValue(C=Vector(0.0, FunctionOnBoundary(dom2)))
+    with pytest.raises(IllegalCoefficient):
+        pde.setValue(ROMA=0.0)
+    with pytest.raises(IllegalCoefficientValue):
+        LinearPDE(dom2, numEquations=2).setValue(C=0.0)
+    assert issubclass(IllegalCoefficient, ValueError)
+
+
+def test_reduced_data_goes_to_full_coefficient(dom2):
+    """Data on ReducedFunction given as A interpolates to Function on ripley (a sample's
+    value at each of its points); given as A_reduced it stays there; both assemble the
+    same operator as the reduced path with the equivalent values."""
+    d = dom2.getDim()
+    A = Data(np.eye(d), (d, d), ReducedFunction(dom2), expanded=True)
+    pde = LinearPDE(dom2)
+    pde.setValue(A=A)
+    assert pde.getCoefficient("A").getFunctionSpace() == Function(dom2)
+    y = Data(2.0, (), ReducedFunctionOnBoundary(dom2), expanded=True)
+    pde.setValue(y=y)
+    assert pde.getCoefficient("y").getFunctionSpace() == FunctionOnBoundary(dom2)
+    assert np.allclose(pde.getCoefficient("y").toNumpy(), 2.0)
