@@ -10,6 +10,7 @@
 // CSR arrays, so each CTA stages its rows in shared memory and writes them back with
 // coalesced stores.
 #include <cmath>
+#include <cstring>
 
 #include "rg_internal.cuh"
 
@@ -146,9 +147,23 @@ struct CoefArg {
     int kind;
 };
 
+// Element-matrix tables integrated over the Gauss points, for operator coefficients that
+// are constant over an element (CONSTANT or PER_ELEMENT):
+//   SA[i][j][R][c] = sum_q W G_qRi G_qcj,  SB[i][R][c] = sum_q W G_qRi N_qc,
+//   SC[j][R][c] = sum_q W N_qR G_qcj,      M[R][c] = sum_q W N_qR N_qc,
+// so a row of the element matrix costs one multiply-add per table entry instead of a sum
+// over the Gauss points.
+struct UniTables {
+    double SA[3][3][8][8];
+    double SB[3][8][8];
+    double SC[3][8][8];
+    double M[8][8];
+};
+
 struct AsmArgs {
     CoefArg c[6];  // A B C D X Y
     Q1Tables t;
+    UniTables u;
     int64_t NE0, NE1, NE2, NN0, NN1, NN2, n;
     const int32_t* ptr;
     double* val;
@@ -167,10 +182,71 @@ __device__ __forceinline__ const double* coef_ptr(const CoefArg& c, int64_t e, i
 // Row R of the element matrix and vector of element e:
 //   em[c] = sum_q W (A_ij G_Ri G_cj + B_i G_Ri N_c + C_j N_R G_cj + D N_R N_c)
 //   f     = sum_q W (X_i G_Ri + Y N_R)
-template <int DIM, int NQ, int R>
+// UNI: A, B, C, D are constant over the element, em comes from the integrated tables.
+template <int DIM, int NQ, int R, bool UNI>
 __device__ __forceinline__ void element_row(const AsmArgs& a, int64_t e, double (&em)[1 << DIM],
                                             double& f)
 {
+    if constexpr (UNI) {
+        constexpr int NK = 1 << DIM;
+        const CoefArg& A = a.c[0];
+        const CoefArg& B = a.c[1];
+        const CoefArg& C = a.c[2];
+        const CoefArg& D = a.c[3];
+        const CoefArg& X = a.c[4];
+        const CoefArg& Y = a.c[5];
+#pragma unroll
+        for (int c = 0; c < NK; ++c) em[c] = 0.0;
+        if (A.kind) {
+            const double* ap = coef_ptr<DIM * DIM, 1>(A, e, 0);
+#pragma unroll
+            for (int j = 0; j < DIM; ++j)
+#pragma unroll
+                for (int i = 0; i < DIM; ++i) {
+                    const double aij = __ldg(ap + i + DIM * j);
+#pragma unroll
+                    for (int c = 0; c < NK; ++c) em[c] = fma(aij, a.u.SA[i][j][R][c], em[c]);
+                }
+        }
+        if (B.kind) {
+            const double* bp = coef_ptr<DIM, 1>(B, e, 0);
+#pragma unroll
+            for (int i = 0; i < DIM; ++i) {
+                const double bi = __ldg(bp + i);
+#pragma unroll
+                for (int c = 0; c < NK; ++c) em[c] = fma(bi, a.u.SB[i][R][c], em[c]);
+            }
+        }
+        if (C.kind) {
+            const double* cp = coef_ptr<DIM, 1>(C, e, 0);
+#pragma unroll
+            for (int j = 0; j < DIM; ++j) {
+                const double cj = __ldg(cp + j);
+#pragma unroll
+                for (int c = 0; c < NK; ++c) em[c] = fma(cj, a.u.SC[j][R][c], em[c]);
+            }
+        }
+        if (D.kind) {
+            const double dd = __ldg(coef_ptr<1, 1>(D, e, 0));
+#pragma unroll
+            for (int c = 0; c < NK; ++c) em[c] = fma(dd, a.u.M[R][c], em[c]);
+        }
+        f = 0.0;
+        if (X.kind || Y.kind) {
+#pragma unroll
+            for (int q = 0; q < NQ; ++q) {
+                double fq = 0.0;
+                if (Y.kind) fq = __ldg(coef_ptr<1, NQ>(Y, e, q)) * a.t.N[q][R];
+                if (X.kind) {
+                    const double* xp = coef_ptr<DIM, NQ>(X, e, q);
+#pragma unroll
+                    for (int i = 0; i < DIM; ++i) fq = fma(__ldg(xp + i), a.t.G[q][R][i], fq);
+                }
+                f = fma(a.t.W, fq, f);
+            }
+        }
+        return;
+    }
     constexpr int NK = 1 << DIM, D2 = DIM * DIM;
     const CoefArg& A = a.c[0];
     const CoefArg& B = a.c[1];
@@ -233,7 +309,7 @@ __host__ __device__ constexpr int band_of(int sx, int sy, int sz, int c)
                     : (sx + (c & 1)) + 3 * (sy + ((c >> 1) & 1));
 }
 
-template <int DIM, int NQ, int SX, int SY, int SZ>
+template <int DIM, int NQ, bool UNI, int SX, int SY, int SZ>
 __device__ __forceinline__ void add_element(const AsmArgs& a, int64_t x, int64_t y, int64_t z,
                                             double (&acc)[DIM == 3 ? 27 : 9], double& facc)
 {
@@ -244,7 +320,7 @@ __device__ __forceinline__ void add_element(const AsmArgs& a, int64_t x, int64_t
     const int64_t e = ex + a.NE0 * ey + (DIM == 3 ? a.NE0 * a.NE1 * ez : 0);
     constexpr int R = (1 - SX) + 2 * (1 - SY) + (DIM == 3 ? 4 * (1 - SZ) : 0);
     double em[NK], f;
-    element_row<DIM, NQ, R>(a, e, em, f);
+    element_row<DIM, NQ, R, UNI>(a, e, em, f);
 #pragma unroll
     for (int c = 0; c < NK; ++c) acc[band_of<DIM>(SX, SY, SZ, c)] += em[c];
     facc += f;
@@ -252,7 +328,7 @@ __device__ __forceinline__ void add_element(const AsmArgs& a, int64_t x, int64_t
 
 // NQ = 2^DIM Gauss points (assemblePDESingle) or 1, the element centre
 // (assemblePDESingleReduced); the tables in `a.t` hold the matching rule
-template <int DIM, int NQ>
+template <int DIM, int NQ, bool UNI>
 __global__ void __launch_bounds__(kRowsPerCta) k_assemble(const __grid_constant__ AsmArgs a)
 {
     constexpr int NB = DIM == 3 ? 27 : 9;
@@ -269,15 +345,15 @@ __global__ void __launch_bounds__(kRowsPerCta) k_assemble(const __grid_constant_
         x = i % a.NN0;
         y = (i / a.NN0) % a.NN1;
         z = DIM == 3 ? i / (a.NN0 * a.NN1) : 0;
-        add_element<DIM, NQ, 0, 0, 0>(a, x, y, z, acc, facc);
-        add_element<DIM, NQ, 1, 0, 0>(a, x, y, z, acc, facc);
-        add_element<DIM, NQ, 0, 1, 0>(a, x, y, z, acc, facc);
-        add_element<DIM, NQ, 1, 1, 0>(a, x, y, z, acc, facc);
+        add_element<DIM, NQ, UNI, 0, 0, 0>(a, x, y, z, acc, facc);
+        add_element<DIM, NQ, UNI, 1, 0, 0>(a, x, y, z, acc, facc);
+        add_element<DIM, NQ, UNI, 0, 1, 0>(a, x, y, z, acc, facc);
+        add_element<DIM, NQ, UNI, 1, 1, 0>(a, x, y, z, acc, facc);
         if (DIM == 3) {
-            add_element<DIM, NQ, 0, 0, 1>(a, x, y, z, acc, facc);
-            add_element<DIM, NQ, 1, 0, 1>(a, x, y, z, acc, facc);
-            add_element<DIM, NQ, 0, 1, 1>(a, x, y, z, acc, facc);
-            add_element<DIM, NQ, 1, 1, 1>(a, x, y, z, acc, facc);
+            add_element<DIM, NQ, UNI, 0, 0, 1>(a, x, y, z, acc, facc);
+            add_element<DIM, NQ, UNI, 1, 0, 1>(a, x, y, z, acc, facc);
+            add_element<DIM, NQ, UNI, 0, 1, 1>(a, x, y, z, acc, facc);
+            add_element<DIM, NQ, UNI, 1, 1, 1>(a, x, y, z, acc, facc);
         }
         if (a.rhs) a.rhs[i] += facc;
     }
@@ -474,6 +550,24 @@ int assemble_single_impl(const Domain* d, double* val, double* rhs, const rg_coe
         if (a.c[j].kind) (j < 4 ? addS : addF) = true;
     }
     a.t = reduced ? d->q1r : d->q1;
+    // operator coefficients constant over each element: integrated element tables
+    bool uni = !reduced;
+    for (int j = 0; j < 4; ++j) uni = uni && a.c[j].kind != RG_COEF_EXPANDED;
+    if (uni) {
+        const int nk = 1 << d->dim, nq = nk, dim = d->dim;
+        const Q1Tables& t = a.t;
+        std::memset(&a.u, 0, sizeof(a.u));
+        for (int r = 0; r < nk; ++r)
+            for (int c = 0; c < nk; ++c)
+                for (int q = 0; q < nq; ++q) {
+                    a.u.M[r][c] += t.W * t.N[q][r] * t.N[q][c];
+                    for (int i = 0; i < dim; ++i) {
+                        a.u.SB[i][r][c] += t.W * t.G[q][r][i] * t.N[q][c];
+                        a.u.SC[i][r][c] += t.W * t.N[q][r] * t.G[q][c][i];
+                        for (int j = 0; j < dim; ++j) a.u.SA[i][j][r][c] += t.W * t.G[q][r][i] * t.G[q][c][j];
+                    }
+                }
+    }
     a.NE0 = d->ne[0];
     a.NE1 = d->ne[1];
     a.NE2 = d->ne[2];
@@ -486,14 +580,18 @@ int assemble_single_impl(const Domain* d, double* val, double* rhs, const rg_coe
     a.rhs = addF ? rhs : nullptr;
     if (!a.val && !a.rhs) return RG_OK;
     const int grid = (int)((d->n + kRowsPerCta - 1) / kRowsPerCta);
-    if (d->dim == 3 && !reduced)
-        RG_TIMED(T_ASSEMBLE, (k_assemble<3, 8><<<grid, kRowsPerCta, 0, stream()>>>(a)));
+    if (d->dim == 3 && !reduced && uni)
+        RG_TIMED(T_ASSEMBLE, (k_assemble<3, 8, true><<<grid, kRowsPerCta, 0, stream()>>>(a)));
+    else if (d->dim == 3 && !reduced)
+        RG_TIMED(T_ASSEMBLE, (k_assemble<3, 8, false><<<grid, kRowsPerCta, 0, stream()>>>(a)));
     else if (d->dim == 3)
-        RG_TIMED(T_ASSEMBLE, (k_assemble<3, 1><<<grid, kRowsPerCta, 0, stream()>>>(a)));
+        RG_TIMED(T_ASSEMBLE, (k_assemble<3, 1, false><<<grid, kRowsPerCta, 0, stream()>>>(a)));
+    else if (!reduced && uni)
+        RG_TIMED(T_ASSEMBLE, (k_assemble<2, 4, true><<<grid, kRowsPerCta, 0, stream()>>>(a)));
     else if (!reduced)
-        RG_TIMED(T_ASSEMBLE, (k_assemble<2, 4><<<grid, kRowsPerCta, 0, stream()>>>(a)));
+        RG_TIMED(T_ASSEMBLE, (k_assemble<2, 4, false><<<grid, kRowsPerCta, 0, stream()>>>(a)));
     else
-        RG_TIMED(T_ASSEMBLE, (k_assemble<2, 1><<<grid, kRowsPerCta, 0, stream()>>>(a)));
+        RG_TIMED(T_ASSEMBLE, (k_assemble<2, 1, false><<<grid, kRowsPerCta, 0, stream()>>>(a)));
     RG_CHECK_LAUNCH();
     return RG_OK;
 }
