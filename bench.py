@@ -275,24 +275,32 @@ def run_ours(args):
     learned.initial_guess = guess.data_ptr()
     learned.guess_sweeps = args.sweeps
     timed = learned if args.path == "learned" else fast
+    side = torch.cuda.Stream(device=dev)
 
     def step(o, A_dev=None, Y_dev=None, q_dev=None):
         ca = cA if A_dev is None else L.rg_coef(A_dev.data_ptr(), L.RG_COEF_PER_ELEMENT)
         cy = cY if Y_dev is None else L.rg_coef(Y_dev.data_ptr(), L.RG_COEF_EXPANDED)
         qq = q_d if q_dev is None else q_dev
         if o is learned:
+            # the network (tensor-core convolutions) runs on a second stream while the
+            # assembly (memory-bound) runs on the main one; the solve waits for both.
             # network input: kappa (A's first diagonal entry) and Y per element
             Ad = A_d if A_dev is None else A_dev
             Yd = Y_d if Y_dev is None else Y_dev
-            kap32.view(-1).copy_(Ad.view(-1, 9)[:, 0])
-            y32.view(-1).copy_(Yd.view(-1, 8).mean(dim=1))
-            warm.guess(kap32, y32, (ne, ne, ne), q=qq, out=guess)
+            side.wait_stream(stream)
+            with torch.cuda.stream(side):
+                kap32.view(-1).copy_(Ad.view(-1, 9)[:, 0])
+                y32.view(-1).copy_(Yd.view(-1, 8).mean(dim=1))
+                warm.guess(kap32, y32, (ne, ne, ne), q=qq, out=guess)
+            L.set_stream_from_torch()  # library work back on the main stream
         L.check(lib.rg_matrix_reset(mat))
         rhs.zero_()
         L.check(lib.rg_assemble_single(mat, C.c_void_p(rhs.data_ptr()), C.byref(ca), C.byref(empty),
                                        C.byref(empty), C.byref(empty), C.byref(empty), C.byref(cy)))
         L.check(lib.rg_insert_constraint(mat, C.c_void_p(rhs.data_ptr()), C.c_void_p(qq.data_ptr()), None, 0))
         d = L.rg_diag()
+        if o is learned:
+            stream.wait_stream(side)
         L.check(lib.rg_solve(mat, C.c_void_p(rhs.data_ptr()), C.c_void_p(x.data_ptr()), C.byref(o), C.byref(d)))
         return d
 

@@ -642,6 +642,33 @@ struct TmaBandArgs {
     int64_t halo;  // largest |offset|
 };
 
+// k_cheb_step on the FP32 band copy (tile-major, absent neighbours hold 0): the same step
+// with the balanced matrix rounded to FP32, x, d and y in FP64.  One thread per row; the
+// band values of a tile are read coalesced band by band.
+template <int NB>
+__global__ void __launch_bounds__(kThreads) k_cheb_step_band(const __grid_constant__ TmaBandArgs ta,
+                                                             const float* __restrict__ band,
+                                                             const double* __restrict__ dinv,
+                                                             const double* __restrict__ x,
+                                                             const double* __restrict__ bb, double c_d, double c_r,
+                                                             double* __restrict__ d, double* __restrict__ y)
+{
+    const int64_t n = ta.n;
+    for (int64_t i = gtid(); i < n; i += gstride()) {
+        const float* bt = band + (i >> 8) * (int64_t)NB * 256 + (i & 255);
+        double acc = 0.0;
+#pragma unroll
+        for (int b = 0; b < NB; ++b) {
+            const int64_t j = i + ta.off[b];
+            const int64_t jc = j < 0 ? 0 : (j >= n ? n - 1 : j);
+            acc = fma((double)__ldg(bt + b * 256), __ldg(x + jc), acc);
+        }
+        const double dn = c_d * (c_d != 0.0 ? d[i] : 0.0) + c_r * dinv[i] * (bb[i] - acc);
+        d[i] = dn;
+        y[i] = x[i] + dn;
+    }
+}
+
 // r32 = r64 * inv_scale, z = dinv r, rho = r.z, ||r||.  fresh: d = 0, p_old = 0, beta = 0,
 // pk = 0 (a new recurrence).  Otherwise (residual replacement) the direction continues:
 // beta is rescaled to the replaced rho.
@@ -1635,8 +1662,21 @@ int solve_impl(Matrix* m, const double* rhs, double* x, const rg_solver_opts* o,
                         c_r = 2.0 * rho_n / delta;
                         rho = rho_n;
                     }
-                    RG_TIMED(T_VECTOR, (k_cheb_step<<<w->grid_rows, kThreads, 0, stream()>>>(
-                                           n, dm->ptr, dm->idx, m->val, m->dinv, src, w->bb, c_d, c_r, w->z, dst)));
+                    if (m->band32) {
+                        // the FP32 band copy streams a third of the bytes of the FP64 CSR
+                        TmaBandArgs ta{};
+                        for (int b = 0; b < dm->nbands; ++b) ta.off[b] = (int)dm->band_off[b];
+                        ta.n = n;
+                        if (dm->nbands == 27)
+                            RG_TIMED(T_VECTOR, (k_cheb_step_band<27><<<eg, kThreads, 0, stream()>>>(
+                                                   ta, m->band32, m->dinv, src, w->bb, c_d, c_r, w->z, dst)));
+                        else
+                            RG_TIMED(T_VECTOR, (k_cheb_step_band<9><<<eg, kThreads, 0, stream()>>>(
+                                                   ta, m->band32, m->dinv, src, w->bb, c_d, c_r, w->z, dst)));
+                    } else {
+                        RG_TIMED(T_VECTOR, (k_cheb_step<<<w->grid_rows, kThreads, 0, stream()>>>(
+                                               n, dm->ptr, dm->idx, m->val, m->dinv, src, w->bb, c_d, c_r, w->z, dst)));
+                    }
                     RG_CHECK_LAUNCH();
                 }
                 if (o->guess_sweeps & 1)
