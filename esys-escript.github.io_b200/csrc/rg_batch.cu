@@ -101,6 +101,8 @@ struct Batch {
     cudaEvent_t ev_in = nullptr, ev_out = nullptr;
     // tuning
     int grid_spmv = 0, grid_upd = 0, chunk = 16;
+    int spmv_kind = 0;    // 0: one row per thread (k_b_spmv); 1: two rows per thread (k_b_spmv2)
+    int force_kind = -1;  // SpMV kernel fixed by the caller (-1: the tuner's choice)
     bool tuned = false;
     cudaGraphExec_t graph = nullptr;
     int graph_chunk = 0;
@@ -164,11 +166,11 @@ struct Vec<8> {
     }
 };
 
-// block-wide sums of NV values (kTile threads); thread 0 writes them to out[0..NV)
-template <int NV>
+// block-wide sums of NV values (NT threads); thread 0 writes them to out[0..NV)
+template <int NV, int NT = kTile>
 __device__ void block_sum_to(double (&v)[NV], double* out)
 {
-    __shared__ double sh[kTile / 32][NV];
+    __shared__ double sh[NT / 32][NV];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     warp_sum<NV>(v);
     if (lane == 0)
@@ -179,7 +181,7 @@ __device__ void block_sum_to(double (&v)[NV], double* out)
 #pragma unroll
         for (int j = 0; j < NV; ++j) {
             double a = 0.0;
-            for (int w = 0; w < kTile / 32; ++w) a += sh[w][j];
+            for (int w = 0; w < NT / 32; ++w) a += sh[w][j];
             out[j] = a;
         }
     __syncthreads();
@@ -187,7 +189,7 @@ __device__ void block_sum_to(double (&v)[NV], double* out)
 
 // Ticket of system i: true in the CTA that wrote the last of the system's `count` partials
 // (slots first..first+count-1), which then reduces them in a fixed order into tot[0..NV).
-template <int NV>
+template <int NV, int NT = kTile>
 __device__ bool last_reduce(int i, int64_t first, int64_t count, unsigned* cnt, const double* part, int stride,
                             double (&tot)[NV])
 {
@@ -201,11 +203,11 @@ __device__ bool last_reduce(int i, int64_t first, int64_t count, unsigned* cnt, 
     double a[NV];
 #pragma unroll
     for (int j = 0; j < NV; ++j) a[j] = 0.0;
-    for (int64_t t = threadIdx.x; t < count; t += kTile)
+    for (int64_t t = threadIdx.x; t < count; t += NT)
 #pragma unroll
         for (int j = 0; j < NV; ++j) a[j] += __ldcg(part + (first + t) * stride + j);
     __shared__ double res[NV];
-    block_sum_to<NV>(a, res);
+    block_sum_to<NV, NT>(a, res);
 #pragma unroll
     for (int j = 0; j < NV; ++j) tot[j] = res[j];
     if (threadIdx.x == 0) cnt[i] = 0u;
@@ -294,6 +296,109 @@ __global__ void __launch_bounds__(kTile, 3) k_b_spmv(const Inst* __restrict__ in
         block_sum_to<R>(v, part + u * 2 * R);
         double tot[R];
         if (last_reduce<R>(i, u - un.w, I.nunits, cnt, part, 2 * R, tot) && threadIdx.x < R) {
+            Rhs& s = st[i * R + threadIdx.x];
+            if (s.active) {
+                const double pq = tot[threadIdx.x];
+                s.pq = pq;
+                if (!(pq > 0.0)) {
+                    s.breakdown = 1;
+                    s.alpha = 0.0;
+                } else {
+                    s.alpha = s.rz / pq;
+                }
+            }
+        }
+    }
+}
+
+// The same product with two consecutive rows per thread (kTile/2 threads per tile): a
+// thread loads p at its two rows, the outer neighbours come from the adjacent lanes, so a
+// stencil line costs one shuffle per right hand side and direction for two rows instead
+// of one (the shuffles share the load/store pipe with the loads).
+constexpr int kPairThreads = kTile / 2;
+
+template <int R, int NB>
+__global__ void __launch_bounds__(kPairThreads, 4)
+    k_b_spmv2(const Inst* __restrict__ insts, const Unit* __restrict__ units, int64_t nunits,
+              const int* __restrict__ inst_active, const float* __restrict__ p, float* __restrict__ q,
+              double* __restrict__ part, unsigned* __restrict__ cnt, Rhs* __restrict__ st)
+{
+    constexpr int NL = NB / 3;
+    const int lane = threadIdx.x & 31;
+    const int t2 = 2 * threadIdx.x;  // the thread's first row within the tile
+    for (int64_t u = blockIdx.x; u < nunits; u += gridDim.x) {
+        const Unit un = units[u];
+        const int i = un.x;
+        if (!inst_active[i]) continue;
+        const Inst& I = insts[i];
+        const int64_t n = I.n;
+        int off[NL];
+#pragma unroll
+        for (int g = 0; g < NL; ++g) off[g] = (int)I.off[3 * g + 1];
+        const float* pv = p + I.voff * R;
+        float vf[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) vf[r] = 0.f;
+        for (int k = 0; k < un.z; ++k) {
+            const int64_t lt = un.y + k - I.tile0;
+            const int64_t row = lt * kTile + t2;
+            float acc0[R], acc1[R], self0[R], self1[R];
+#pragma unroll
+            for (int r = 0; r < R; ++r) acc0[r] = acc1[r] = self0[r] = self1[r] = 0.f;
+            const float* bt = I.band + lt * NB * kTile + t2;
+#pragma unroll
+            for (int g = 0; g < NL; ++g) {
+                const float2 am = __ldcs(reinterpret_cast<const float2*>(bt + (3 * g) * kTile));
+                const float2 a0 = __ldcs(reinterpret_cast<const float2*>(bt + (3 * g + 1) * kTile));
+                const float2 ap = __ldcs(reinterpret_cast<const float2*>(bt + (3 * g + 2) * kTile));
+                const int64_t c = row + off[g];  // the first row's centre column
+                const int64_t j0 = c < 0 ? 0 : (c >= n ? n - 1 : c);
+                const int64_t j1 = c + 1 < 0 ? 0 : (c + 1 >= n ? n - 1 : c + 1);
+                float w0[R], w1[R], lv[R], rv[R];
+                Vec<R>::ld(pv + j0 * R, w0);
+                Vec<R>::ld(pv + j1 * R, w1);
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    lv[r] = __shfl_up_sync(0xffffffffu, w1[r], 1);    // column c - 1
+                    rv[r] = __shfl_down_sync(0xffffffffu, w0[r], 1);  // column c + 2
+                }
+                if (lane == 0) {
+                    const int64_t jl = c - 1 < 0 ? 0 : (c - 1 >= n ? n - 1 : c - 1);
+                    Vec<R>::ld(pv + jl * R, lv);
+                }
+                if (lane == 31) {
+                    const int64_t jr = c + 2 < 0 ? 0 : (c + 2 >= n ? n - 1 : c + 2);
+                    Vec<R>::ld(pv + jr * R, rv);
+                }
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    acc0[r] = fmaf(am.x, lv[r], fmaf(a0.x, w0[r], fmaf(ap.x, w1[r], acc0[r])));
+                    acc1[r] = fmaf(am.y, w0[r], fmaf(a0.y, w1[r], fmaf(ap.y, rv[r], acc1[r])));
+                }
+                if (g == NL / 2)
+#pragma unroll
+                    for (int r = 0; r < R; ++r) {
+                        self0[r] = w0[r];
+                        self1[r] = w1[r];
+                    }
+            }
+            if (row < n) {
+                Vec<R>::st(q + (I.voff + row) * R, acc0);
+#pragma unroll
+                for (int r = 0; r < R; ++r) vf[r] = fmaf(self0[r], acc0[r], vf[r]);
+            }
+            if (row + 1 < n) {
+                Vec<R>::st(q + (I.voff + row + 1) * R, acc1);
+#pragma unroll
+                for (int r = 0; r < R; ++r) vf[r] = fmaf(self1[r], acc1[r], vf[r]);
+            }
+        }
+        double v[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) v[r] = vf[r];
+        block_sum_to<R, kPairThreads>(v, part + u * 2 * R);
+        double tot[R];
+        if (last_reduce<R, kPairThreads>(i, u - un.w, I.nunits, cnt, part, 2 * R, tot) && threadIdx.x < R) {
             Rhs& s = st[i * R + threadIdx.x];
             if (s.active) {
                 const double pq = tot[threadIdx.x];
@@ -698,14 +803,18 @@ template <int R>
 int iter_step(Batch* b)
 {
     const int nb = b->dim == 3 ? 27 : 9;
-    if (nb == 27)
-        RG_TIMED(T_BATCH_SPMV, (k_b_spmv<R, 27><<<b->grid_spmv, kTile, 0, stream()>>>(
-                                   b->d_inst, b->d_units, b->nunits, b->d_inst_active, b->p, b->q, b->d_part,
-                                   b->d_cnt, b->d_rhs)));
-    else
-        RG_TIMED(T_BATCH_SPMV, (k_b_spmv<R, 9><<<b->grid_spmv, kTile, 0, stream()>>>(
-                                   b->d_inst, b->d_units, b->nunits, b->d_inst_active, b->p, b->q, b->d_part,
-                                   b->d_cnt, b->d_rhs)));
+#define RG_B_SPMV(KERNEL, NBANDS, THREADS)                                                               \
+    RG_TIMED(T_BATCH_SPMV, (KERNEL<<<b->grid_spmv, THREADS, 0, stream()>>>(                                 \
+                               b->d_inst, b->d_units, b->nunits, b->d_inst_active, b->p, b->q, b->d_part, \
+                               b->d_cnt, b->d_rhs)))
+    if (b->spmv_kind == 1) {
+        if (nb == 27) RG_B_SPMV((k_b_spmv2<R, 27>), 27, kPairThreads);
+        else RG_B_SPMV((k_b_spmv2<R, 9>), 9, kPairThreads);
+    } else {
+        if (nb == 27) RG_B_SPMV((k_b_spmv<R, 27>), 27, kTile);
+        else RG_B_SPMV((k_b_spmv<R, 9>), 9, kTile);
+    }
+#undef RG_B_SPMV
     RG_CHECK_LAUNCH();
     RG_TIMED(T_BATCH_UPDATE, (k_b_update<R><<<b->grid_upd, kTile, 0, stream()>>>(
                                  b->d_inst, b->d_units, b->nunits, b->d_inst_active, b->p, b->q, b->r32, b->d32,
@@ -952,23 +1061,29 @@ int tune(Batch* b)
     const int saved_maxit = b->maxit;
     b->maxit = 1 << 30;
     double best = 1e30;
-    int best_g = 4, best_s = 8, best_u = 8;
-    for (int g : groups) {
-        if ((rc = set_group(b, g))) return rc;
-        for (int c : cands) {
-            if (c > 2 && (int64_t)c * kNumSMs > b->nunits) break;
-            b->grid_spmv = b->grid_upd = kNumSMs * c;
-            if ((rc = seed_all_active(b))) return rc;
-            double ms;
-            if ((rc = time_iters(b, 2, &ms))) return rc;  // warm
-            if ((rc = time_iters(b, 6, &ms))) return rc;
-            if (ms < best) {
-                best = ms;
-                best_g = g;
-                best_s = best_u = c;
+    int best_g = 4, best_s = 8, best_u = 8, best_k = 0;
+    for (int kind : {0, 1}) {
+        if (b->force_kind >= 0 && kind != b->force_kind) continue;
+        b->spmv_kind = kind;
+        for (int g : groups) {
+            if ((rc = set_group(b, g))) return rc;
+            for (int c : cands) {
+                if (c > 2 && (int64_t)c * kNumSMs > b->nunits) break;
+                b->grid_spmv = b->grid_upd = kNumSMs * c;
+                if ((rc = seed_all_active(b))) return rc;
+                double ms;
+                if ((rc = time_iters(b, 2, &ms))) return rc;  // warm
+                if ((rc = time_iters(b, 6, &ms))) return rc;
+                if (ms < best) {
+                    best = ms;
+                    best_g = g;
+                    best_s = best_u = c;
+                    best_k = kind;
+                }
             }
         }
     }
+    b->spmv_kind = best_k;
     if ((rc = set_group(b, best_g))) return rc;
     for (int c : cands) {
         if (c == best_s || (c > 2 && (int64_t)c * kNumSMs > b->nunits)) continue;
@@ -1176,7 +1291,7 @@ int rg_batch_destroy(rg_batch* h)
 }
 
 int rg_batch_info(const rg_batch* h, int64_t* rows, int64_t* tiles, int* group, int* grid_spmv, int* grid_update,
-                  int* chunk, double* iter_us)
+                  int* chunk, double* iter_us, int* spmv_kernel)
 {
     RG_REQUIRE(h, "rg_batch_info: NULL batch");
     const Batch* b = &h->b;
@@ -1187,6 +1302,16 @@ int rg_batch_info(const rg_batch* h, int64_t* rows, int64_t* tiles, int* group, 
     if (grid_update) *grid_update = b->grid_upd;
     if (chunk) *chunk = b->chunk;
     if (iter_us) *iter_us = b->tuned_iter_us;
+    if (spmv_kernel) *spmv_kernel = b->spmv_kind;
+    return RG_OK;
+}
+
+int rg_batch_set_spmv(rg_batch* h, int spmv_kernel)
+{
+    RG_REQUIRE(h, "rg_batch_set_spmv: NULL batch");
+    RG_REQUIRE(spmv_kernel >= -1 && spmv_kernel <= 1, "rg_batch_set_spmv: spmv_kernel must be -1, 0 or 1");
+    h->b.force_kind = spmv_kernel;
+    h->b.tuned = false;  // the next solve (or rg_batch_tune) tunes within the choice
     return RG_OK;
 }
 

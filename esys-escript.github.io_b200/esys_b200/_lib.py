@@ -138,7 +138,8 @@ _SIGNATURES = {
     "rg_batch_tune": (C.c_int, [C.c_void_p]),
     "rg_batch_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int),
                                 C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
-                                C.POINTER(C.c_double)]),
+                                C.POINTER(C.c_double), C.POINTER(C.c_int)]),
+    "rg_batch_set_spmv": (C.c_int, [C.c_void_p, C.c_int]),
     "rg_batch_solve": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(rg_solver_opts),
                                  C.c_void_p]),
     "rg_timers_enable": (C.c_int, [C.c_int]),

@@ -22,6 +22,11 @@ from . import _lib as L
 from . import warmstart as W
 
 
+# the batched SpMV kernels (rg_batch_info / rg_batch_set_spmv numbering): one row per
+# thread, two rows per thread
+_SPMV_KERNELS = ("row", "pair")
+
+
 class BatchSolver:
     def __init__(self, mats, nrhs):
         self.nsys = len(mats)
@@ -53,12 +58,18 @@ class BatchSolver:
 
     def info(self):
         rows, tiles = C.c_int64(), C.c_int64()
-        grp, gs, gu, ch = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        grp, gs, gu, ch, kind = C.c_int(), C.c_int(), C.c_int(), C.c_int(), C.c_int()
         us = C.c_double()
         L.check(L.lib().rg_batch_info(self._h, C.byref(rows), C.byref(tiles), C.byref(grp), C.byref(gs),
-                                      C.byref(gu), C.byref(ch), C.byref(us)))
+                                      C.byref(gu), C.byref(ch), C.byref(us), C.byref(kind)))
         return {"rows": rows.value, "tiles": tiles.value, "group": grp.value, "grid_spmv": gs.value,
-                "grid_update": gu.value, "chunk": ch.value, "iter_us": us.value}
+                "grid_update": gu.value, "chunk": ch.value, "iter_us": us.value,
+                "spmv_kernel": _SPMV_KERNELS[kind.value]}
+
+    def set_spmv(self, kernel):
+        """Restricts the tuner to one SpMV kernel: None (any) or a name of _SPMV_KERNELS."""
+        k = -1 if kernel is None else _SPMV_KERNELS.index(kernel)
+        L.check(L.lib().rg_batch_set_spmv(self._h, k))
 
     def solve(self, rhs, x, tol=1e-8, iter_max=100000, inner_tolerance=1e-2, accept_failure=False):
         """Solves all systems; returns the list of rg_diag (system-major)."""

@@ -252,9 +252,13 @@ int rg_batch_destroy(rg_batch* batch);
 int rg_batch_tune(rg_batch* batch);
 /* rows: padded batch rows; tiles: 256-row tiles; group: tiles per work unit of the
    iteration kernels; grids in CTAs; iter_us: measured time of one iteration of all systems
-   at the tuned configuration */
+   at the tuned configuration; spmv_kernel: 0 = one row per thread, 1 = two rows per thread.
+   Any output pointer may be NULL. */
 int rg_batch_info(const rg_batch* batch, int64_t* rows, int64_t* tiles, int* group, int* grid_spmv,
-                  int* grid_update, int* chunk, double* iter_us);
+                  int* grid_update, int* chunk, double* iter_us, int* spmv_kernel);
+/* Restricts the tuner to one SpMV kernel (0 or 1 as in rg_batch_info; -1: either, the
+   default); the next solve or rg_batch_tune re-tunes. */
+int rg_batch_set_spmv(rg_batch* batch, int spmv_kernel);
 /* rhs[i], x[i]: device arrays of n_i * nrhs doubles for system i, right hand side k at
    offset k * n_i.  opts: tolerance, iter_max, inner_tolerance, accept_convergence_failure
    (NULL: defaults).  diag: nsystems * nrhs entries (system-major) or NULL. */

@@ -63,3 +63,41 @@ def test_batch_rejects_changed_matrices(cuda):
     bs.close()
     for s in systems:
         s.close()
+
+
+@pytest.mark.parametrize("kernel", ["row", "pair"])
+def test_batch_spmv_kernels_agree(cuda, kernel):
+    """Both SpMV kernels, pinned through rg_batch_set_spmv, solve the same batch (Bricks of
+    edges up to 40, so that some systems span several work units) to solutions within 1e-6
+    of each other, each meeting the residual test.  The two kernels sum p.q in different
+    orders and FP32 PCG iteration counts move with that (single-tile systems match), so only
+    the totals are compared, within 10 %."""
+    systems, rhs = make_batch(4, 4, edges=(8, 24, 40), corr_cells=3.0, seed=21)
+    out = {}
+    for k in ("row", kernel):
+        xs = [torch.zeros_like(b) for b in rhs]
+        with BatchSolver([s.mat for s in systems], 4) as bs:
+            bs.set_spmv(k)
+            info = bs.tune()
+            assert info["spmv_kernel"] == k
+            diags = bs.solve(rhs, xs, tol=1e-8)
+        for d in diags:
+            assert d.converged and d.residual_norm <= 1e-8 * d.rhs_norm * (1 + 1e-9)
+        out[k] = (xs, [int(d.num_iter) for d in diags])
+    (x0, it0), (x1, it1) = out["row"], out[kernel]
+    for a, b in zip(x0, x1):
+        assert float((a - b).norm() / a.norm()) < 1e-6
+    assert abs(sum(it1) - sum(it0)) <= 0.1 * sum(it0)
+    for s in systems:
+        s.close()
+
+
+def test_batch_set_spmv_rejects_unknown(cuda):
+    import ctypes
+    from esys_b200 import _lib as L
+    systems, _ = make_batch(1, 1, edges=(8,), corr_cells=2.0, seed=5)
+    with BatchSolver([s.mat for s in systems], 1) as bs:
+        with pytest.raises(ValueError):
+            L.check(L.lib().rg_batch_set_spmv(bs._h, 2))
+    for s in systems:
+        s.close()
