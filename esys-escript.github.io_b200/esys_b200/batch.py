@@ -13,7 +13,6 @@ hand side, stopped by paso's dual-norm test.
 from __future__ import annotations
 
 import ctypes as C
-import math
 
 import numpy as np
 import torch

@@ -7,7 +7,6 @@ of these small systems."""
 import pytest
 import torch
 
-from esys_b200 import warmstart as W
 from esys_b200.batch import BatchSolver, make_batch
 
 pytestmark = pytest.mark.gpu
@@ -93,7 +92,6 @@ def test_batch_spmv_kernels_agree(cuda, kernel):
 
 
 def test_batch_set_spmv_rejects_unknown(cuda):
-    import ctypes
     from esys_b200 import _lib as L
     systems, _ = make_batch(1, 1, edges=(8,), corr_cells=2.0, seed=5)
     with BatchSolver([s.mat for s in systems], 1) as bs:

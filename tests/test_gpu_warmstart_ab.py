@@ -5,7 +5,6 @@ The committed weights (esys_b200/data/warmstart_unet.npz) were trained by
 `python -m esys_b200.warmstart_train --samples 20000 --epochs 6` on problems from generator
 seed 12345; the problems here come from other seeds.  Both arms solve with FP32 inner
 iterations and FP64 refinement to rtol 1e-8, so both meet the same residual test."""
-import numpy as np
 import pytest
 import torch
 
