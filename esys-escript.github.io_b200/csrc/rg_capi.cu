@@ -51,6 +51,16 @@ bool coef_ok(const rg_coef* c)
 
 void free_domain(Domain* d)
 {
+    free_domain_workspace(d);
+    {
+        Domain::Spare& sp = d->spare;
+        if (sp.val) cudaFree(sp.val);
+        if (sp.bv) cudaFree(sp.bv);
+        if (sp.dinv) cudaFree(sp.dinv);
+        if (sp.band32) cudaFree(sp.band32);
+        if (sp.dinv32) cudaFree(sp.dinv32);
+        sp = Domain::Spare();
+    }
     if (d->ptr) cudaFree(d->ptr);
     if (d->idx) cudaFree(d->idx);
     d->ptr = nullptr;
@@ -59,9 +69,23 @@ void free_domain(Domain* d)
 
 void free_matrix(Matrix* m)
 {
-    free_workspace(m);
+    release_workspace(m);
     free_residual_scratch(m);
     free_system_workspace(m);
+    if (m->nb == 1 && m->val) {
+        // keep the arrays for the next matrix on this domain (one set)
+        std::lock_guard<std::mutex> lock(pool_mutex());
+        Domain::Spare& sp = m->dom->spare;
+        if (!sp.val) {
+            sp.val = m->val;
+            sp.bv = m->bv;
+            sp.dinv = m->dinv;
+            sp.band32 = m->band32;
+            sp.dinv32 = m->dinv32;
+            m->val = m->bv = m->dinv = nullptr;
+            m->band32 = m->dinv32 = nullptr;
+        }
+    }
     if (m->val) cudaFree(m->val);
     if (m->bv) cudaFree(m->bv);
     if (m->dinv) cudaFree(m->dinv);
@@ -172,11 +196,26 @@ int rg_domain_create(int dim, const int64_t ne[3], const double x0[3], const dou
     RG_GUARD_END
 }
 
+// drops one reference to the domain; the last one frees it (matrices keep their domain
+// alive, so destroying a domain before its matrices is safe)
+static void release_domain(Domain* d)
+{
+    bool last;
+    {
+        std::lock_guard<std::mutex> lock(pool_mutex());
+        last = --d->refs == 0;
+    }
+    if (last) {
+        cudaStreamSynchronize(stream());
+        free_domain(d);
+        delete reinterpret_cast<rg_domain*>(d);  // Domain is rg_domain's only member
+    }
+}
+
 int rg_domain_destroy(rg_domain* dom)
 {
     if (!dom) return RG_OK;
-    free_domain(&dom->d);
-    delete dom;
+    release_domain(&dom->d);
     return RG_OK;
 }
 
@@ -230,14 +269,32 @@ int rg_matrix_create(rg_domain* dom, rg_matrix** out)
     rg_matrix* h = new rg_matrix();
     Matrix& m = h->m;
     m.dom = &dom->d;
-    cudaError_t e = cudaMalloc((void**)&m.val, sizeof(double) * dom->d.nnz);
-    if (e == cudaSuccess) e = cudaMalloc((void**)&m.bv, sizeof(double) * dom->d.n);
+    {
+        // the arrays of a destroyed matrix on this domain, when there are some
+        std::lock_guard<std::mutex> lock(pool_mutex());
+        Domain::Spare& sp = dom->d.spare;
+        if (sp.val) {
+            m.val = sp.val;
+            m.bv = sp.bv;
+            m.dinv = sp.dinv;
+            m.band32 = sp.band32;
+            m.dinv32 = sp.dinv32;
+            sp = Domain::Spare();
+        }
+    }
+    cudaError_t e = cudaSuccess;
+    if (!m.val) e = cudaMalloc((void**)&m.val, sizeof(double) * dom->d.nnz);
+    if (e == cudaSuccess && !m.bv) e = cudaMalloc((void**)&m.bv, sizeof(double) * dom->d.n);
     if (e == cudaSuccess) e = cudaMemsetAsync(m.val, 0, sizeof(double) * dom->d.nnz, stream());
     if (e != cudaSuccess) {
         free_matrix(&m);
         delete h;
         set_error(std::string("rg_matrix_create: ") + cudaGetErrorString(e));
         return RG_CUDA_ERROR;
+    }
+    {
+        std::lock_guard<std::mutex> lock(pool_mutex());
+        ++dom->d.refs;  // the matrix keeps its domain alive
     }
     *out = h;
     return RG_OK;
@@ -269,6 +326,10 @@ int rg_matrix_create_system(rg_domain* dom, int block_size, rg_matrix** out)
         set_error(std::string("rg_matrix_create_system: ") + cudaGetErrorString(e));
         return RG_CUDA_ERROR;
     }
+    {
+        std::lock_guard<std::mutex> lock(pool_mutex());
+        ++dom->d.refs;  // the matrix keeps its domain alive
+    }
     *out = h;
     return RG_OK;
     RG_GUARD_END
@@ -285,8 +346,10 @@ int rg_matrix_destroy(rg_matrix* mat)
 {
     if (!mat) return RG_OK;
     cudaStreamSynchronize(stream());
+    Domain* d = mat->m.dom;
     free_matrix(&mat->m);
     delete mat;
+    release_domain(d);
     return RG_OK;
 }
 

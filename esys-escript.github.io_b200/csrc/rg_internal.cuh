@@ -1,5 +1,6 @@
 // Internal declarations shared by the ripley_gpu translation units.
 #pragma once
+#include <mutex>
 
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -52,6 +53,7 @@ void build_q1_tables(int dim, const double dx[3], Q1Tables* t);
 void build_q1_reduced_tables(int dim, const double dx[3], Q1Tables* t);
 
 // ---------------------------------------------------------------- handles
+struct Workspace;
 struct Domain {
     int dim;
     int64_t ne[3], nn[3];  // unused axes hold 1
@@ -64,6 +66,13 @@ struct Domain {
     int64_t band_off[27];    // column offset of band b: dx + NN0*dy + NN0*NN1*dz
     Q1Tables q1;
     Q1Tables q1r;            // 1-point rule of the reduced-order assembly
+    int refs = 1;                   // the caller's handle + one per live matrix (rg_capi.cu)
+    Workspace* spare_ws = nullptr;  // solver vectors of a destroyed matrix, kept for the next one
+    // the value arrays of a destroyed block-size-1 matrix, kept for the next one
+    struct Spare {
+        double *val = nullptr, *bv = nullptr, *dinv = nullptr;
+        float *band32 = nullptr, *dinv32 = nullptr;
+    } spare;
 };
 
 struct Workspace;        // solver vectors, allocated lazily (rg_solver.cu)
@@ -231,6 +240,12 @@ int solver_config(const Matrix* m, int* spmv_cfg, int* update_grid, double* spmv
 // fixes the FP32 SpMV configuration (-1: tune at the next FP32 solve)
 int solver_set_config(Matrix* m, int spmv_cfg);
 void free_workspace(Matrix* m);
+// hands the matrix's solver vectors to its domain for the next matrix there (one is kept; a
+// further one is freed), instead of freeing them: a fresh matrix on the same grid then
+// solves without device and pinned host allocations
+void release_workspace(Matrix* m);
+void free_domain_workspace(Domain* d);
+std::mutex& pool_mutex();  // guards the domains' spare workspaces and arrays
 // PDE systems (rg_system.cu): block size m->nb in {2, 3}
 int assemble_system_impl(const Domain* d, int nb, double* val, double* rhs, const rg_coef* c[6], bool reduced);
 int launch_system_constraint(Matrix* m, double* rhs, const double* q, const double* r, int rhs_only);

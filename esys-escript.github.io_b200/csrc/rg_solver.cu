@@ -23,6 +23,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <mutex>
 #include <vector>
 
 #include "rg_bulk.cuh"
@@ -96,6 +97,17 @@ int dalloc(T** p, size_t count)
 int ensure_workspace(Matrix* m, bool fp32)
 {
     const int64_t n = m->dom->n;
+    if (!m->ws) {
+        // the solver vectors of a destroyed matrix on this grid: the captured iteration graphs
+        // named that matrix's arrays and were dropped; the SpMV pipeline is tuned again
+        std::lock_guard<std::mutex> lock(pool_mutex());
+        if (m->dom->spare_ws) {
+            m->ws = m->dom->spare_ws;
+            m->dom->spare_ws = nullptr;
+            m->ws->spmv_cfg = -1;
+            m->ws->grid_upd32 = 0;
+        }
+    }
     if (!m->ws) {
         Workspace* w = new Workspace();
         m->ws = w;
@@ -1508,6 +1520,45 @@ int solver_prepare(Matrix* m, bool band)
     int rc = ensure_workspace(m, band);
     if (rc) return rc;
     return prepare(m, band);
+}
+
+std::mutex& pool_mutex()
+{
+    static std::mutex mu;
+    return mu;
+}
+
+void release_workspace(Matrix* m)
+{
+    Workspace* w = m->ws;
+    if (!w) return;
+    {
+        std::lock_guard<std::mutex> lock(pool_mutex());
+        if (!m->dom->spare_ws) {
+            for (int k = 0; k < 3; ++k) {
+                if (w->graph[k]) cudaGraphExecDestroy(w->graph[k]);
+                w->graph[k] = nullptr;
+                w->graph_chunk[k] = 0;
+                w->graph_sweeps[k] = 0;
+            }
+            m->dom->spare_ws = w;
+            m->ws = nullptr;
+            return;
+        }
+    }
+    free_workspace(m);
+}
+
+void free_domain_workspace(Domain* d)
+{
+    Matrix tmp;
+    tmp.dom = d;
+    {
+        std::lock_guard<std::mutex> lock(pool_mutex());
+        tmp.ws = d->spare_ws;
+        d->spare_ws = nullptr;
+    }
+    free_workspace(&tmp);
 }
 
 void free_workspace(Matrix* m)

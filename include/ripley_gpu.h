@@ -59,6 +59,8 @@ int rg_set_stream(void* stream);
    l = (x0, x1) tuples).  The CSR pattern is built on the device at creation. */
 int rg_domain_create(int dim, const int64_t ne[3], const double x0[3], const double x1[3],
                      rg_domain** out);
+/* Frees the domain; its matrices (and batches) must be destroyed first.  Solver vectors of
+   a destroyed matrix are kept by the domain for the next matrix on it and freed here. */
 int rg_domain_destroy(rg_domain* dom);
 /* n: DOF count (= nodes); nnz: pattern entries; nn/ne: nodes/elements per axis; dx: spacing */
 int rg_domain_info(const rg_domain* dom, int64_t* n, int64_t* nnz, int64_t nn[3],

@@ -338,3 +338,33 @@ def test_jacobi_sweeps_match_reference(cuda, golden, tag, sweeps):
     x1 = torch.zeros_like(x)
     st, dg1 = R.solve(m, rhs, x1, R.opts(tolerance=1e-10))
     assert st == 0 and abs(int(dg1.num_iter) - int(golden[f"solve{tag}_iter"])) <= 1
+
+
+def test_matrix_keeps_its_domain_and_reuses_storage(cuda, golden):
+    """A matrix keeps its domain alive: destroying the domain first (as a garbage collector
+    may do) leaves the matrix usable; a matrix created after another on the same domain
+    reuses its device arrays and solver vectors and gives the same solution."""
+    d, m, rhs, _ = _system(golden, "3d")
+    x1 = torch.zeros(d.n, dtype=torch.float64, device="cuda")
+    assert R.solve(m, rhs, x1, R.opts(tolerance=1e-10))[0] == 0
+    # a second matrix after the first is gone: the domain's spare arrays and workspace
+    R.lib().rg_matrix_destroy(m.h)
+    m.h = None
+    d2, m2, rhs2, _ = _system(golden, "3d")
+    x2 = torch.zeros(d2.n, dtype=torch.float64, device="cuda")
+    assert R.solve(m2, rhs2, x2, R.opts(tolerance=1e-10))[0] == 0
+    assert torch.equal(x1, x2)
+    # domain destroyed before its matrix: the matrix still assembles and solves
+    dom = R.Domain(3, (4, 3, 5))
+    mat = R.Matrix(dom)
+    R.lib().rg_domain_destroy(dom.h)
+    dom.h = None
+    b = torch.zeros(dom.n, dtype=torch.float64, device="cuda")
+    keep = []
+    R.assemble(mat, b, keep, A=(np.eye(3).reshape(-1), R.KINDS["const"]), D=(np.ones(1), R.KINDS["const"]),
+               Y=(np.ones(1), R.KINDS["const"]))  # u = 1
+    x = torch.zeros(dom.n, dtype=torch.float64, device="cuda")
+    st, dg = R.solve(mat, b, x, R.opts(tolerance=1e-10))
+    assert st == 0 and float((x - 1.0).abs().max()) < 1e-8
+    R.lib().rg_matrix_destroy(mat.h)  # frees the domain as well
+    mat.h = None
