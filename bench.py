@@ -311,11 +311,15 @@ def run_ours(args):
     def max_over_ranks(v):
         return max_over_ranks_of(v, dist, dev)
 
-    if args.only == "plain":
+    if args.only in ("plain", "plain_band"):
+        o = plain
+        if args.only == "plain_band":
+            o = opts(L.RG_MODE_PASO, L.RG_PREC_FP64)
+            o.layout = L.RG_LAYOUT_BAND
         for _ in range(args.warmup + args.steps):
-            step(plain)
+            step(o)
         torch.cuda.synchronize()
-        print(json.dumps({"only": "plain", "iterations": int(step(plain).num_iter)}), flush=True)
+        print(json.dumps({"only": args.only, "iterations": int(step(o).num_iter)}), flush=True)
         return
     if args.only == "fast":
         for _ in range(args.warmup + args.steps):
@@ -341,6 +345,18 @@ def run_ours(args):
     ev1.record(stream)
     torch.cuda.synchronize()
     plain_ms = max_over_ranks(ev0.elapsed_time(ev1) / n_plain)
+
+    # --- the same FP64 paso PCG with its SpMV on the FP64 band copy (RG_LAYOUT_BAND)
+    plain_band = opts(L.RG_MODE_PASO, L.RG_PREC_FP64)
+    plain_band.layout = L.RG_LAYOUT_BAND
+    d_pb = step(plain_band)
+    barrier()
+    ev0.record(stream)
+    for _ in range(n_plain):
+        d_pb = step(plain_band)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    plain_band_ms = max_over_ranks(ev0.elapsed_time(ev1) / n_plain)
 
     # --- the FP32-refinement path without the learned guess, for comparison
     for _ in range(2):
@@ -536,7 +552,9 @@ def run_ours(args):
         "rel_residual": float(d_fast.residual_norm / d_fast.rhs_norm),
         "error_vs_fp64": err,
         "plain_fp64": {"ms": round(plain_ms, 3), "iterations": plain_iters,
-                       "algorithm": "paso PCG with residual smoothing, balanced CSR FP64"},
+                       "algorithm": "paso PCG with residual smoothing, balanced CSR FP64",
+                       "band_layout_ms": round(plain_band_ms, 3),
+                       "band_layout_iterations": int(d_pb.num_iter)},
         "speedup_vs_plain_fp64": round(plain_ms / ms, 3),
         "fp32_refine_no_guess": {"ms": round(f32_ms, 3), "iterations": int(d_f32.num_iter),
                                  "speedup_vs_plain_fp64": round(plain_ms / f32_ms, 3),
@@ -620,8 +638,9 @@ def main():
     ap.add_argument("--sweeps", type=int, default=8, help="Chebyshev smoothing steps on the learned guess")
     ap.add_argument("--no-batched", dest="batched", action="store_false",
                     help="skip the batched 64-system workload")
-    ap.add_argument("--only", choices=["all", "fast", "plain"], default="all",
-                    help="profiling runs: only the fast path, or only the plain FP64 paso solve")
+    ap.add_argument("--only", choices=["all", "fast", "plain", "plain_band"], default="all",
+                    help="profiling runs: only the fast path, or only the plain FP64 paso solve "
+                         "(CSR, or the FP64 band copy)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -1340,7 +1340,7 @@ int rg_batch_solve(rg_batch* h, const double* const* rhs, double* const* x, cons
     RG_REQUIRE(o->tolerance >= 100. * EPS && o->tolerance <= 1., "rg_batch_solve: tolerance out of range");
     RG_REQUIRE(o->initial_guess == nullptr, "rg_batch_solve: initial guesses are not supported for batches");
     for (int i = 0; i < b->ninst; ++i)
-        RG_REQUIRE(b->mats[i]->balanced && b->mats[i]->solver_ready && b->mats[i]->band32,
+        RG_REQUIRE(b->mats[i]->balanced && b->mats[i]->solver_ready && b->mats[i]->band32 && b->mats[i]->band32_ok,
                    "rg_batch_solve: a system's values changed after rg_batch_create (recreate the batch)");
     const double t0 = now_s();
     OnPrivate on(b);

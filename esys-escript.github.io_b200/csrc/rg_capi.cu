@@ -59,6 +59,7 @@ void free_domain(Domain* d)
         if (sp.dinv) cudaFree(sp.dinv);
         if (sp.band32) cudaFree(sp.band32);
         if (sp.dinv32) cudaFree(sp.dinv32);
+        if (sp.band64) cudaFree(sp.band64);
         sp = Domain::Spare();
     }
     if (d->ptr) cudaFree(d->ptr);
@@ -82,10 +83,13 @@ void free_matrix(Matrix* m)
             sp.dinv = m->dinv;
             sp.band32 = m->band32;
             sp.dinv32 = m->dinv32;
-            m->val = m->bv = m->dinv = nullptr;
+            sp.band64 = m->band64;
+            m->val = m->bv = m->dinv = m->band64 = nullptr;
             m->band32 = m->dinv32 = nullptr;
         }
     }
+    if (m->band64) cudaFree(m->band64);
+    m->band64 = nullptr;
     if (m->val) cudaFree(m->val);
     if (m->bv) cudaFree(m->bv);
     if (m->dinv) cudaFree(m->dinv);
@@ -279,6 +283,7 @@ int rg_matrix_create(rg_domain* dom, rg_matrix** out)
             m.dinv = sp.dinv;
             m.band32 = sp.band32;
             m.dinv32 = sp.dinv32;
+            m.band64 = sp.band64;
             sp = Domain::Spare();
         }
     }

@@ -70,7 +70,7 @@ struct Domain {
     Workspace* spare_ws = nullptr;  // solver vectors of a destroyed matrix, kept for the next one
     // the value arrays of a destroyed block-size-1 matrix, kept for the next one
     struct Spare {
-        double *val = nullptr, *bv = nullptr, *dinv = nullptr;
+        double *val = nullptr, *bv = nullptr, *dinv = nullptr, *band64 = nullptr;
         float *band32 = nullptr, *dinv32 = nullptr;
     } spare;
 };
@@ -88,8 +88,10 @@ struct Matrix {
     bool balanced = false;
     // solver data derived from the balanced values (paso's preconditioner data)
     bool solver_ready = false;
+    bool band32_ok = false, band64_ok = false;  // band copies hold the current balanced values
     double* dinv = nullptr;    // 1 / balanced diagonal
     float* band32 = nullptr;   // [nbands][npad] FP32 copy of the balanced matrix
+    double* band64 = nullptr;  // the same layout in FP64 (paso in FP64 with RG_LAYOUT_BAND)
     int force_spmv = -1;       // FP32 SpMV configuration fixed by the caller (-1: tuned)
     float* dinv32 = nullptr;
     Workspace* ws = nullptr;
@@ -230,7 +232,7 @@ int launch_spmv64(const Domain* d, const double* val, double alpha, const double
                   double* y);
 // balance in place (scale=1) and/or derive dinv (+dinv32, + the FP32 band copy when
 // want_band) from the current values; *d_bad is set when a diagonal is zero or missing
-int launch_balance(Matrix* m, int scale, int* d_bad, bool want_band);
+int launch_balance(Matrix* m, int scale, int* d_bad, bool want_band, bool want_band64);
 int solve(Matrix* m, const double* rhs, double* x, const rg_solver_opts* o, rg_diag* diag);
 // balance the matrix in place (first time) and build its solver data, the FP32 band copy
 // included when `band` (what rg_solve does before iterating)

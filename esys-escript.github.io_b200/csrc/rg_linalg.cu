@@ -128,7 +128,7 @@ __global__ void __launch_bounds__(256) k_row_balance(int64_t n, const int32_t* _
 // (SparseMatrix::invMain, paso/src/SparseMatrix.cpp:387-435): dinv_i = 1/a~_ii; a zero or
 // missing diagonal sets *bad.  With band != null the balanced row is also copied into the
 // tile-major FP32 band layout: band[((i/256)*nbands + b)*256 + i%256],
-// b = (dx+1) + 3(dy+1) (+ 9(dz+1)).
+// b = (dx+1) + 3(dy+1) (+ 9(dz+1)); with band64 != null the same in FP64.
 __global__ void __launch_bounds__(256) k_apply_balance(int64_t n, int nbands, int dim, int64_t NN0, int64_t NN1,
                                                        const int32_t* __restrict__ ptr,
                                                        const int32_t* __restrict__ idx,
@@ -136,7 +136,8 @@ __global__ void __launch_bounds__(256) k_apply_balance(int64_t n, int nbands, in
                                                        const double* __restrict__ bv, int scale,
                                                        double* __restrict__ dinv,
                                                        float* __restrict__ dinv32,
-                                                       float* __restrict__ band, int* bad)
+                                                       float* __restrict__ band, double* __restrict__ band64,
+                                                       int* bad)
 {
     const int lane = threadIdx.x & (kLpr - 1);
     const int64_t groups = (int64_t)gridDim.x * blockDim.x / kLpr;
@@ -161,11 +162,13 @@ __global__ void __launch_bounds__(256) k_apply_balance(int64_t n, int nbands, in
                     dg = a;
                     found = 1;
                 }
-                if (band) {
+                if (band || band64) {
                     const int64_t xj = j % NN0, yj = (j / NN0) % NN1, zj = j / plane;
                     int b = (int)(xj - xi + 1) + 3 * (int)(yj - yi + 1);
                     if (dim == 3) b += 9 * (int)(zj - zi + 1);
-                    band[((size_t)(row >> 8) * nbands + b) * 256 + (row & 255)] = (float)a;
+                    const size_t o = ((size_t)(row >> 8) * nbands + b) * 256 + (row & 255);
+                    if (band) band[o] = (float)a;
+                    if (band64) band64[o] = a;
                 }
             }
         }
@@ -215,7 +218,7 @@ int launch_nullify(Matrix* m, const double* mr, const double* mc, double diag)
     return RG_OK;
 }
 
-int launch_balance(Matrix* m, int scale, int* d_bad, bool want_band)
+int launch_balance(Matrix* m, int scale, int* d_bad, bool want_band, bool want_band64)
 {
     const Domain* d = m->dom;
     const int grid = grid_for(d->n, 256 / kLpr, 16);
@@ -224,9 +227,11 @@ int launch_balance(Matrix* m, int scale, int* d_bad, bool want_band)
         RG_CHECK_LAUNCH();
     }
     if (want_band) RG_CHECK_CUDA(cudaMemsetAsync(m->band32, 0, sizeof(float) * d->nbands * d->npad, stream()));
+    if (want_band64) RG_CHECK_CUDA(cudaMemsetAsync(m->band64, 0, sizeof(double) * d->nbands * d->npad, stream()));
     RG_TIMED(T_BALANCE, (k_apply_balance<<<grid, 256, 0, stream()>>>(d->n, d->nbands, d->dim, d->nn[0], d->nn[1], d->ptr, d->idx, m->val,
                                                 m->bv, scale, m->dinv, m->dinv32,
-                                                want_band ? m->band32 : nullptr, d_bad)));
+                                                want_band ? m->band32 : nullptr,
+                                                want_band64 ? m->band64 : nullptr, d_bad)));
     RG_CHECK_LAUNCH();
     return RG_OK;
 }

@@ -80,6 +80,8 @@ struct Workspace {
     int graph_sweeps[3] = {0, 0, 0};  // Jacobi sweeps the captured iterations apply
     long long graph_launches[3][T_COUNT] = {};
     int sweeps = 1;  // Jacobi sweeps of the current paso solve (Smoother.cpp:100-128)
+    bool band64 = false;              // paso FP64 SpMV on the FP64 band copy (RG_LAYOUT_BAND)
+    bool graph_band64[3] = {false, false, false};
     int spmv_cfg = -1;   // FP32 band SpMV pipeline: 0 = 3 stages x 1 CTA/SM, 1 = 2 stages x 2 CTAs/SM
     int grid_upd32 = 0;  // CTAs of k_f32_update (tuned with the SpMV; 0 = grid_vec)
     double spmv_us[2] = {0, 0};  // tuner's time per launch of each SpMV configuration
@@ -852,6 +854,169 @@ __global__ void __launch_bounds__(kTile + 32, 1) k_f32_spmv_tma(const float* __r
     }
 }
 
+// The FP64 band kernels of the paso PCG (RG_LAYOUT_BAND), warp-specialised and persistent
+// like k_f32_spmv_tma: lane 0 of warp kConsumerWarps streams, per tile, the tile's FP64 band
+// block (one bulk copy, L2 evict-first) and, for interior tiles, the NG windows of x its
+// stencil columns span (kTile+4 values from a 16-byte aligned start) into a kStages ring;
+// consumer warps compute row i0 + t from shared memory.  Tiles near the two ends read x with
+// clamped loads.  The bands are summed in column order.
+//   SWEEP = false: v = A x, delta = x.v, alpha = tau/delta, breakdown on delta == 0
+//                  (PCG.cpp:223-262), i.e. k_paso_spmv.
+//   SWEEP = true:  one Jacobi sweep out = x + dinv (b - A x) with k_jacobi_sweep's modes.
+// All waits are bounded: on timeout the kernel records ST_TIMEOUT and returns.
+constexpr int kWin64 = kTile + 4;
+
+template <int NB, int kStages>
+constexpr size_t band64_smem()
+{
+    return sizeof(double) * (size_t)kStages * (NB * kTile + (NB / 3) * kWin64);
+}
+
+template <int NB, int kStages, bool SWEEP>
+__global__ void __launch_bounds__(kTile + 32, 1) k_band64_bulk(const double* __restrict__ band,
+                                                               const __grid_constant__ TmaBandArgs ta,
+                                                               const double* __restrict__ x,
+                                                               double* __restrict__ out,
+                                                               const double* __restrict__ dinv,
+                                                               const double* __restrict__ b,
+                                                               double* __restrict__ pout, ReduceBuf rb, Scal* s,
+                                                               int mode)
+{
+    constexpr int NG = NB / 3;
+    constexpr int kBand = NB * kTile;
+    constexpr int kStage = kBand + NG * kWin64;
+    extern __shared__ __align__(128) double smem64[];
+    __shared__ __align__(8) uint64_t full[kStages], empty[kStages];
+    __shared__ int bad;
+    if (SWEEP ? (mode == 1 && s->done) : s->done) return;
+    const int t = threadIdx.x;
+    const int warp = t >> 5;
+    const int64_t n = ta.n;
+    const int64_t ntiles = (n + kTile - 1) / kTile;
+    const int64_t my_tiles = blockIdx.x < ntiles ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+    if (t == 0) {
+        for (int k = 0; k < kStages; ++k) {
+            mbar_init(&full[k], 1);
+            mbar_init(&empty[k], kConsumerWarps);
+        }
+        bad = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    auto interior = [&](int64_t i0) { return i0 - ta.halo - 8 >= 0 && i0 + kTile + ta.halo + 8 <= n; };
+
+    double v[1] = {0.0};
+    int64_t issued = 0;
+    if (warp == kConsumerWarps) {
+        // ---------------- producer
+        if ((t & 31) == 0) {
+            const uint64_t pol = evict_first_policy();
+            for (int64_t k = 0; k < my_tiles; ++k, issued = k) {
+                const int st = (int)(k % kStages);
+                if (k >= kStages && !mbar_wait(&empty[st], (uint32_t)(((k / kStages) - 1) & 1))) {
+                    bad = 1;
+                    break;
+                }
+                const int64_t tile = blockIdx.x + k * gridDim.x;
+                const int64_t i0 = tile * kTile;
+                double* dst = smem64 + (size_t)st * kStage;
+                const bool in = interior(i0);
+                mbar_expect_tx(&full[st], (kBand + (in ? NG * kWin64 : 0)) * 8);
+                bulk_g2s_hint(dst, band + (size_t)tile * kBand, kBand * 8, &full[st], pol);
+                if (in)
+                    for (int g = 0; g < NG; ++g) {
+                        const int64_t a = (i0 + ta.goff[g]) & ~(int64_t)1;
+                        bulk_g2s(dst + kBand + g * kWin64, x + a, kWin64 * 8, &full[st]);
+                    }
+            }
+        }
+    } else {
+        // ---------------- consumers: row i0 + t of every tile
+        for (int64_t k = 0; k < my_tiles; ++k) {
+            const int st = (int)(k % kStages);
+            if (!mbar_wait(&full[st], (uint32_t)((k / kStages) & 1))) {
+                bad = 1;
+                break;
+            }
+            const double* bs = smem64 + (size_t)st * kStage;
+            const int64_t i0 = (blockIdx.x + k * gridDim.x) * (int64_t)kTile;
+            const int64_t i = i0 + t;
+            double acc = 0.0, xi = 0.0;
+            if (interior(i0)) {
+                const double* xw = bs + kBand;
+#pragma unroll
+                for (int g = 0; g < NG; ++g) {
+                    const int base = (int)((i0 + ta.goff[g]) & 1) + t + g * kWin64;
+#pragma unroll
+                    for (int m = 0; m < 3; ++m) {
+                        const double xj = xw[base + m];
+                        acc = fma(bs[(3 * g + m) * kTile + t], xj, acc);
+                        if (3 * g + m == NB / 2) xi = xj;
+                    }
+                }
+            } else {
+#pragma unroll
+                for (int c = 0; c < NB; ++c) {
+                    const int64_t j = min(max(i + ta.off[c], (int64_t)0), n - 1);
+                    const double xj = __ldg(x + j);
+                    acc = fma(bs[c * kTile + t], xj, acc);
+                    if (c == NB / 2) xi = xj;
+                }
+            }
+            __syncwarp();
+            if ((t & 31) == 0) mbar_arrive(&empty[st]);
+            if (i < n) {
+                if (SWEEP) {
+                    const double bi = b[i];
+                    const double zi = xi + dinv[i] * (bi - acc);
+                    out[i] = zi;
+                    if (mode == 2) pout[i] = zi;
+                    v[0] += zi * bi;
+                } else {
+                    out[i] = acc;
+                    v[0] += acc * xi;
+                }
+            }
+        }
+    }
+    __syncthreads();
+    if (bad) {
+        // let the copies this CTA issued land (bounded) before its shared memory is released
+        if (warp == kConsumerWarps && (t & 31) == 0)
+            for (int64_t k = issued > kStages ? issued - kStages : 0; k < issued; ++k)
+                for (int tries = 0; tries < (1 << 20) && !mbar_try_wait(&full[k % kStages], (uint32_t)((k / kStages) & 1));
+                     ++tries) {
+                }
+        if (t == 0) {
+            s->status = ST_TIMEOUT;
+            s->done = 1;
+        }
+        return;
+    }
+    if (SWEEP && mode == 0) return;
+    double tt[1];
+    if (grid_reduce<1>(v, rb, tt) && threadIdx.x == 0) {
+        if (!SWEEP) {
+            s->delta = tt[0];
+            s->alpha = s->tau / tt[0];
+            if (fabs(tt[0]) <= 0.0) {  // breakFlag
+                s->iter += 1;
+                s->status = ST_BREAK;
+                s->done = 1;
+            }
+        } else if (mode == 1) {
+            s->tau_next = tt[0];
+            s->beta = tt[0] / s->tau;
+        } else {
+            s->tau = tt[0];
+        }
+    }
+}
+
+// stages of the FP64 band ring: 3 x 74 KB (27 bands) or 8 x 24 KB (9 bands), one CTA per SM
+template <int NB>
+constexpr int band64_stages() { return NB == 27 ? 3 : 8; }
+
 // d += alpha p; r -= alpha q; z = dinv r; rho_next = r.z and ||r||^2 in FP64; tests; beta
 __global__ void __launch_bounds__(kThreads) k_f32_update(int64_t n, float* __restrict__ d,
                                                          float* __restrict__ r,
@@ -1020,7 +1185,8 @@ int run_until_done(Matrix* m, int kind, IterFn step, int chunk, long long cap, l
         *status = w->hs->status;
         return RG_OK;
     }
-    if (!w->graph[kind] || w->graph_chunk[kind] != chunk || w->graph_sweeps[kind] != w->sweeps) {
+    if (!w->graph[kind] || w->graph_chunk[kind] != chunk || w->graph_sweeps[kind] != w->sweeps ||
+        w->graph_band64[kind] != w->band64) {
         if (w->graph[kind]) cudaGraphExecDestroy(w->graph[kind]);
         w->graph[kind] = nullptr;
         long long before[T_COUNT], after[T_COUNT];
@@ -1043,6 +1209,7 @@ int run_until_done(Matrix* m, int kind, IterFn step, int chunk, long long cap, l
         }
         w->graph_chunk[kind] = chunk;
         w->graph_sweeps[kind] = w->sweeps;
+        w->graph_band64[kind] = w->band64;
         timers_snapshot(after);
         long long undo[T_COUNT];
         for (int k = 0; k < T_COUNT; ++k) {
@@ -1083,16 +1250,57 @@ int run_until_done(Matrix* m, int kind, IterFn step, int chunk, long long cap, l
 // sweeps - 1 more Jacobi sweeps on the preconditioned vector z (of b), alternating between
 // z and `spare`; returns the buffer that holds the result.  mode of the last sweep as in
 // k_jacobi_sweep.
+TmaBandArgs band_offsets(const Domain* d)
+{
+    TmaBandArgs ta{};
+    for (int b = 0; b < d->nbands; ++b) {
+        ta.off[b] = (int)d->band_off[b];
+        ta.halo = std::max<int64_t>(ta.halo, std::abs(d->band_off[b]));
+    }
+    for (int g = 0; g < d->nbands / 3; ++g) ta.goff[g] = (int)d->band_off[3 * g];  // dx = -1 member
+    ta.n = d->n;
+    return ta;
+}
+
+int sm_count();
+
+// FP64 band kernel (SpMV or Jacobi sweep) over all tiles, one CTA per SM.  The vector x that
+// is bulk-copied is always a solver workspace array (cudaMalloc: 256-byte aligned).  Launch
+// errors are picked up by the caller's RG_CHECK_LAUNCH.
+template <bool SWEEP>
+void launch_band64(Matrix* m, const double* x, double* out, const double* b, double* pout, int mode)
+{
+    Workspace* w = m->ws;
+    const Domain* d = m->dom;
+    const TmaBandArgs ta = band_offsets(d);
+    const int64_t ntiles = (d->n + kTile - 1) / kTile;
+    const int grid = (int)std::min<int64_t>(ntiles, sm_count());
+    const int kind = SWEEP ? T_PASO_UPDATE1 : T_PASO_SPMV;
+    if (d->nbands == 27) {
+        constexpr int S = band64_stages<27>();
+        RG_TIMED(kind, (k_band64_bulk<27, S, SWEEP><<<grid, kTile + 32, band64_smem<27, S>(), stream()>>>(
+                           m->band64, ta, x, out, m->dinv, b, pout, rbuf(w), w->s, mode)));
+    } else {
+        constexpr int S = band64_stages<9>();
+        RG_TIMED(kind, (k_band64_bulk<9, S, SWEEP><<<grid, kTile + 32, band64_smem<9, S>(), stream()>>>(
+                           m->band64, ta, x, out, m->dinv, b, pout, rbuf(w), w->s, mode)));
+    }
+}
+
 double* jacobi_sweeps(Matrix* m, const double* b, double* z, double* spare, double* p, int last_mode)
 {
     Workspace* w = m->ws;
     const Domain* d = m->dom;
     double* src = z;
     double* dst = spare;
+    const bool band = w->band64 && m->band64;
     for (int k = 1; k < w->sweeps; ++k) {
         const int mode = k == w->sweeps - 1 ? last_mode : 0;
-        RG_TIMED(T_PASO_UPDATE1, (k_jacobi_sweep<<<w->grid_rows, kThreads, 0, stream()>>>(
-                                     d->n, d->ptr, d->idx, m->val, m->dinv, b, src, dst, p, rbuf(w), w->s, mode)));
+        if (band)
+            launch_band64<true>(m, src, dst, b, p, mode);
+        else
+            RG_TIMED(T_PASO_UPDATE1, (k_jacobi_sweep<<<w->grid_rows, kThreads, 0, stream()>>>(
+                                         d->n, d->ptr, d->idx, m->val, m->dinv, b, src, dst, p, rbuf(w), w->s, mode)));
         std::swap(src, dst);
     }
     return src;
@@ -1102,8 +1310,12 @@ int paso_step(Matrix* m)
 {
     Workspace* w = m->ws;
     const Domain* d = m->dom;
-    RG_TIMED(T_PASO_SPMV, (k_paso_spmv<<<w->grid_rows, kThreads, 0, stream()>>>(
-                              d->n, d->ptr, d->idx, m->val, w->p, w->q, rbuf(w), w->s)));
+    if (w->band64 && m->band64) {
+        launch_band64<false>(m, w->p, w->q, nullptr, nullptr, 0);
+    } else {
+        RG_TIMED(T_PASO_SPMV, (k_paso_spmv<<<w->grid_rows, kThreads, 0, stream()>>>(
+                                  d->n, d->ptr, d->idx, m->val, w->p, w->q, rbuf(w), w->s)));
+    }
     RG_TIMED(T_PASO_UPDATE1, (k_paso_update1<<<w->grid_vec, kThreads, 0, stream()>>>(
                                  d->n, w->r, w->q, w->rs, w->x2, w->p, m->dinv, w->z, rbuf(w), w->s)));
     // v = prec(r) with more than one Jacobi sweep: q (free after update1) is the spare buffer
@@ -1187,6 +1399,18 @@ int tma_attributes()
                                            (int)tma_smem<9, 3>()));
         RG_CHECK_CUDA(cudaFuncSetAttribute(k_f32_spmv_tma<9, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            (int)tma_smem<9, 2>()));
+        RG_CHECK_CUDA(cudaFuncSetAttribute(k_band64_bulk<27, band64_stages<27>(), false>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)band64_smem<27, band64_stages<27>()>()));
+        RG_CHECK_CUDA(cudaFuncSetAttribute(k_band64_bulk<27, band64_stages<27>(), true>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)band64_smem<27, band64_stages<27>()>()));
+        RG_CHECK_CUDA(cudaFuncSetAttribute(k_band64_bulk<9, band64_stages<9>(), false>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)band64_smem<9, band64_stages<9>()>()));
+        RG_CHECK_CUDA(cudaFuncSetAttribute(k_band64_bulk<9, band64_stages<9>(), true>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)band64_smem<9, band64_stages<9>()>()));
         done = true;
     }
     return RG_OK;
@@ -1292,24 +1516,27 @@ int f32_step(Matrix* m)
 }
 
 // balance (first solve only) and the preconditioner data (paso Solver.cpp:98,177)
-int prepare(Matrix* m, bool want_band)
+int prepare(Matrix* m, bool want_band, bool want_band64)
 {
     Domain* d = m->dom;
     Workspace* w = m->ws;
-    const bool need_band = want_band && !m->band32;
-    if (need_band) {
-        RG_CHECK_CUDA(cudaMalloc((void**)&m->band32, sizeof(float) * d->nbands * d->npad));
-        if (!m->dinv32) RG_CHECK_CUDA(cudaMalloc((void**)&m->dinv32, sizeof(float) * d->n));
-        m->solver_ready = false;
-    }
-    if (want_band) {
+    // a band copy is written once a solve reads it and kept current from then on; arrays
+    // adopted from a destroyed matrix are not written until then
+    if (want_band && !m->band32) RG_CHECK_CUDA(cudaMalloc((void**)&m->band32, sizeof(float) * d->nbands * d->npad));
+    if (want_band && !m->dinv32) RG_CHECK_CUDA(cudaMalloc((void**)&m->dinv32, sizeof(float) * d->n));
+    if (want_band64 && !m->band64)
+        RG_CHECK_CUDA(cudaMalloc((void**)&m->band64, sizeof(double) * d->nbands * d->npad));
+    if ((want_band && !m->band32_ok) || (want_band64 && !m->band64_ok)) m->solver_ready = false;
+    want_band = want_band || m->band32_ok;
+    want_band64 = want_band64 || m->band64_ok;
+    if (want_band || want_band64) {
         int rc = tma_attributes();
         if (rc) return rc;
     }
     if (m->balanced && m->solver_ready) return RG_OK;
     if (!m->dinv) RG_CHECK_CUDA(cudaMalloc((void**)&m->dinv, sizeof(double) * d->n));
     RG_CHECK_CUDA(cudaMemsetAsync(w->bad, 0, sizeof(int), stream()));
-    int rc = launch_balance(m, m->balanced ? 0 : 1, w->bad, m->band32 != nullptr);
+    int rc = launch_balance(m, m->balanced ? 0 : 1, w->bad, want_band, want_band64);
     if (rc) return rc;
     int bad = 0;
     RG_CHECK_CUDA(cudaMemcpyAsync(&bad, w->bad, sizeof(int), cudaMemcpyDeviceToHost, stream()));
@@ -1320,6 +1547,8 @@ int prepare(Matrix* m, bool want_band)
         return RG_INVALID_ARG;
     }
     m->solver_ready = true;
+    m->band32_ok = want_band;
+    m->band64_ok = want_band64;
     return RG_OK;
 }
 
@@ -1519,7 +1748,7 @@ int solver_prepare(Matrix* m, bool band)
 {
     int rc = ensure_workspace(m, band);
     if (rc) return rc;
-    return prepare(m, band);
+    return prepare(m, band, false);
 }
 
 std::mutex& pool_mutex()
@@ -1650,7 +1879,9 @@ int solve_impl(Matrix* m, const double* rhs, double* x, const rg_solver_opts* o,
     int rc = ensure_workspace(m, fp32);
     if (rc) return rc;
     Workspace* w = m->ws;
-    if ((rc = prepare(m, fp32))) return rc;
+    const bool band64 = paso && o->layout == RG_LAYOUT_BAND;
+    if ((rc = prepare(m, fp32, band64))) return rc;
+    w->band64 = band64;
     const double t_setup = now_s();
     dg.set_up_time = t_setup - t_start;
 
@@ -1713,7 +1944,7 @@ int solve_impl(Matrix* m, const double* rhs, double* x, const rg_solver_opts* o,
                         c_r = 2.0 * rho_n / delta;
                         rho = rho_n;
                     }
-                    if (m->band32) {
+                    if (m->band32 && m->band32_ok) {
                         // the FP32 band copy streams a third of the bytes of the FP64 CSR
                         TmaBandArgs ta{};
                         for (int b = 0; b < dm->nbands; ++b) ta.off[b] = (int)dm->band_off[b];

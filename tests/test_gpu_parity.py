@@ -340,6 +340,104 @@ def test_jacobi_sweeps_match_reference(cuda, golden, tag, sweeps):
     assert st == 0 and abs(int(dg1.num_iter) - int(golden[f"solve{tag}_iter"])) <= 1
 
 
+@pytest.mark.parametrize("tag", ["2d", "3d"])
+@pytest.mark.parametrize("sweeps", [1, 2])
+def test_paso_band_layout_matches_reference(cuda, golden, tag, sweeps):
+    """paso PCG in FP64 with RG_LAYOUT_BAND: the SpMV and the extra Jacobi sweeps read the
+    FP64 band copy of the balanced matrix instead of the CSR; iterations within one of the
+    reference's, solution within 1e-8.  A following CSR solve on the same matrix rebuilds the
+    captured iterations."""
+    d, m, rhs, _ = _system(golden, tag)
+    x = torch.zeros(d.n, dtype=torch.float64, device="cuda")
+    st, dg = R.solve(m, rhs, x, R.opts(tolerance=1e-10, sweeps=sweeps, layout=L.RG_LAYOUT_BAND))
+    assert st == 0 and dg.converged
+    key = f"solve{tag}" if sweeps == 1 else f"sweep{tag}_{sweeps}"
+    assert abs(int(dg.num_iter) - int(golden[f"{key}_iter"])) <= 1
+    ref = golden[f"{key}_x"]
+    assert np.linalg.norm(x.cpu().numpy() - ref) / np.linalg.norm(ref) < 1e-8
+    x1 = torch.zeros_like(x)
+    st, dg1 = R.solve(m, rhs, x1, R.opts(tolerance=1e-10, sweeps=sweeps))
+    assert st == 0 and abs(int(dg1.num_iter) - int(dg.num_iter)) <= 1
+    assert torch.linalg.norm(x1 - x) <= 1e-9 * torch.linalg.norm(x)
+
+
+@pytest.mark.parametrize("ne", [(40, 33, 27), (7, 5, 130), (300, 211)])
+def test_paso_band_layout_equals_csr(cuda, ne):
+    """The FP64 band SpMV on grids with ragged edge tiles (rows not a multiple of 256) and
+    long iteration counts (replayed graphs): the same iterations within one as the CSR
+    SpMV and the same solution to 1e-9."""
+    rng = np.random.default_rng(5)
+    dim = len(ne)
+    nel, nq = int(np.prod(ne)), 2 ** dim
+    kappa = np.exp(rng.standard_normal(nel))
+    A = np.zeros((nel, nq, dim, dim))
+    for i in range(dim):
+        A[:, :, i, i] = kappa[:, None]
+    Y = rng.standard_normal(nel * nq)
+    xs, its = [], []
+    for layout in (L.RG_LAYOUT_CSR, L.RG_LAYOUT_BAND):
+        d = R.Domain(dim, ne)
+        m = R.Matrix(d)
+        rhs = torch.zeros(d.n, dtype=torch.float64, device="cuda")
+        keep = []
+        R.assemble(m, rhs, keep, A=(A.reshape(-1), R.KINDS["exp"]), Y=(Y, R.KINDS["exp"]))
+        q = np.zeros(d.n)
+        q[: int(np.prod([v + 1 for v in ne[:-1]]))] = 1.0
+        R.insert_constraint(m, rhs, R.dev(q))
+        x = torch.zeros(d.n, dtype=torch.float64, device="cuda")
+        st, dg = R.solve(m, rhs, x, R.opts(tolerance=1e-10, layout=layout))
+        assert st == 0 and dg.converged
+        xs.append(x)
+        its.append(int(dg.num_iter))
+    assert abs(its[0] - its[1]) <= 1, its
+    assert torch.linalg.norm(xs[1] - xs[0]) <= 1e-9 * torch.linalg.norm(xs[0])
+
+
+def _kappa_problem(d, ne, seed):
+    """A = kappa I per element (log-normal kappa), Y random, u = 0 on the first face of the
+    last axis, assembled into a new matrix on domain d."""
+    rng = np.random.default_rng(seed)
+    dim = len(ne)
+    nel, nq = int(np.prod(ne)), 2 ** dim
+    kappa = np.exp(rng.standard_normal(nel))
+    A = np.zeros((nel, nq, dim, dim))
+    for i in range(dim):
+        A[:, :, i, i] = kappa[:, None]
+    m = R.Matrix(d)
+    rhs = torch.zeros(d.n, dtype=torch.float64, device="cuda")
+    keep = []
+    R.assemble(m, rhs, keep, A=(A.reshape(-1), R.KINDS["exp"]), Y=(rng.standard_normal(nel * nq), R.KINDS["exp"]))
+    q = np.zeros(d.n)
+    q[: int(np.prod([v + 1 for v in ne[:-1]]))] = 1.0
+    R.insert_constraint(m, rhs, R.dev(q))
+    return m, rhs
+
+
+def test_band_copies_follow_the_matrix(cuda):
+    """Band copies adopted from a destroyed matrix are rewritten before a solve reads them,
+    and a matrix whose values change (reset + assemble) gets fresh band copies: CSR, FP64
+    band and FP32 band solves of the second matrix all match a fresh matrix's solution."""
+    ne = (40, 33, 27)
+    d = R.Domain(3, ne)
+    m1, b1 = _kappa_problem(d, ne, seed=1)
+    x = torch.zeros(d.n, dtype=torch.float64, device="cuda")
+    assert R.solve(m1, b1, x, R.opts(tolerance=1e-10, layout=L.RG_LAYOUT_BAND))[0] == 0
+    assert R.solve(m1, b1, x, R.opts(tolerance=1e-10, precision=L.RG_PREC_FP32_REFINE))[0] == 0
+    R.lib().rg_matrix_destroy(m1.h)  # its arrays, band copies included, go to the domain's pool
+    m1.h = None
+    ref_d = R.Domain(3, ne)
+    mr, br = _kappa_problem(ref_d, ne, seed=2)
+    xr = torch.zeros(ref_d.n, dtype=torch.float64, device="cuda")
+    assert R.solve(mr, br, xr, R.opts(tolerance=1e-10))[0] == 0
+    m2, b2 = _kappa_problem(d, ne, seed=2)  # adopts m1's arrays
+    for o in (R.opts(tolerance=1e-10), R.opts(tolerance=1e-10, layout=L.RG_LAYOUT_BAND),
+              R.opts(tolerance=1e-10, precision=L.RG_PREC_FP32_REFINE)):
+        x2 = torch.zeros(d.n, dtype=torch.float64, device="cuda")
+        st, dg = R.solve(m2, b2, x2, o)
+        assert st == 0 and dg.converged and not dg.fp64_fallback
+        assert torch.linalg.norm(x2 - xr) <= 1e-7 * torch.linalg.norm(xr), (o.layout, o.precision)
+
+
 def test_matrix_keeps_its_domain_and_reuses_storage(cuda, golden):
     """A matrix keeps its domain alive: destroying the domain first (as a garbage collector
     may do) leaves the matrix usable; a matrix created after another on the same domain
