@@ -860,8 +860,9 @@ __global__ void __launch_bounds__(kTile + 32, 1) k_f32_spmv_tma(const float* __r
 // stencil columns span (kTile+4 values from a 16-byte aligned start) into a kStages ring;
 // consumer warps compute row i0 + t from shared memory.  Tiles near the two ends read x with
 // clamped loads.  The bands are summed in column order.
-//   SWEEP = false: v = A x, delta = x.v, alpha = tau/delta, breakdown on delta == 0
-//                  (PCG.cpp:223-262), i.e. k_paso_spmv.
+//   SWEEP = false: v = A x, delta = x.v; mode 0: alpha = tau/delta, breakdown on delta == 0
+//                  (PCG.cpp:223-262), i.e. k_paso_spmv; mode 1: alpha = rho/delta, i.e.
+//                  k_std_spmv (RG_MODE_STANDARD).
 //   SWEEP = true:  one Jacobi sweep out = x + dinv (b - A x) with k_jacobi_sweep's modes.
 // All waits are bounded: on timeout the kernel records ST_TIMEOUT and returns.
 constexpr int kWin64 = kTile + 4;
@@ -996,10 +997,18 @@ __global__ void __launch_bounds__(kTile + 32, 1) k_band64_bulk(const double* __r
     if (SWEEP && mode == 0) return;
     double tt[1];
     if (grid_reduce<1>(v, rb, tt) && threadIdx.x == 0) {
-        if (!SWEEP) {
+        if (!SWEEP && mode == 0) {
             s->delta = tt[0];
             s->alpha = s->tau / tt[0];
             if (fabs(tt[0]) <= 0.0) {  // breakFlag
+                s->iter += 1;
+                s->status = ST_BREAK;
+                s->done = 1;
+            }
+        } else if (!SWEEP) {
+            s->delta = tt[0];
+            s->alpha = s->rho / tt[0];
+            if (!(fabs(tt[0]) > 0.0)) {
                 s->iter += 1;
                 s->status = ST_BREAK;
                 s->done = 1;
@@ -1275,7 +1284,7 @@ void launch_band64(Matrix* m, const double* x, double* out, const double* b, dou
     const TmaBandArgs ta = band_offsets(d);
     const int64_t ntiles = (d->n + kTile - 1) / kTile;
     const int grid = (int)std::min<int64_t>(ntiles, sm_count());
-    const int kind = SWEEP ? T_PASO_UPDATE1 : T_PASO_SPMV;
+    const int kind = SWEEP ? T_PASO_UPDATE1 : (mode == 1 ? T_STD_SPMV : T_PASO_SPMV);
     if (d->nbands == 27) {
         constexpr int S = band64_stages<27>();
         RG_TIMED(kind, (k_band64_bulk<27, S, SWEEP><<<grid, kTile + 32, band64_smem<27, S>(), stream()>>>(
@@ -1330,8 +1339,11 @@ int std_step(Matrix* m)
 {
     Workspace* w = m->ws;
     const Domain* d = m->dom;
-    RG_TIMED(T_STD_SPMV, (k_std_spmv<<<w->grid_rows, kThreads, 0, stream()>>>(d->n, d->ptr, d->idx, m->val, w->p,
-                                                                              w->q, rbuf(w), w->s)));
+    if (w->band64 && m->band64)
+        launch_band64<false>(m, w->p, w->q, nullptr, nullptr, 1);
+    else
+        RG_TIMED(T_STD_SPMV, (k_std_spmv<<<w->grid_rows, kThreads, 0, stream()>>>(d->n, d->ptr, d->idx, m->val,
+                                                                                  w->p, w->q, rbuf(w), w->s)));
     RG_TIMED(T_STD_UPDATE, (k_std_update<<<w->grid_vec, kThreads, 0, stream()>>>(d->n, w->x, w->r, w->q, w->p,
                                                                                  m->dinv, w->z, rbuf(w), w->s)));
     RG_TIMED(T_VECTOR, (k_std_pupdate<<<w->grid_vec, kThreads, 0, stream()>>>(d->n, w->z, w->p, w->s)));
@@ -1879,7 +1891,7 @@ int solve_impl(Matrix* m, const double* rhs, double* x, const rg_solver_opts* o,
     int rc = ensure_workspace(m, fp32);
     if (rc) return rc;
     Workspace* w = m->ws;
-    const bool band64 = paso && o->layout == RG_LAYOUT_BAND;
+    const bool band64 = !fp32 && o->layout == RG_LAYOUT_BAND;
     if ((rc = prepare(m, fp32, band64))) return rc;
     w->band64 = band64;
     const double t_setup = now_s();

@@ -183,8 +183,9 @@ int rg_save_mm(rg_matrix* mat, const char* path);
 #define RG_PREC_FP32_REFINE 1     /* FP32 inner PCG, FP64 residual/update/stop test         */
 #define RG_LAYOUT_CSR 0           /* inner SpMV on the paso CSR values                       */
 #define RG_LAYOUT_BAND 1          /* SpMV on a 27-band (9 in 2D) structured copy: FP32_REFINE
-                                     always; paso FP64 with this layout streams an FP64 band
-                                     copy (8 bytes per coefficient against the CSR's 12)     */
+                                     always; FP64 solves (paso or standard mode) with this
+                                     layout stream an FP64 band copy (8 bytes per coefficient
+                                     against the CSR's 12)                                  */
 
 typedef struct {
     int method;                 /* RG_METHOD_PCG                                            */

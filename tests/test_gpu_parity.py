@@ -215,12 +215,13 @@ def test_paso_solve_matches_reference(cuda, golden, tag):
 
 
 @pytest.mark.parametrize("tag", ["2d", "3d"])
-@pytest.mark.parametrize("mode,precision", [(L.RG_MODE_STANDARD, L.RG_PREC_FP64),
-                                            (L.RG_MODE_STANDARD, L.RG_PREC_FP32_REFINE)])
-def test_fast_modes_match_reference(cuda, golden, tag, mode, precision):
+@pytest.mark.parametrize("mode,precision,layout", [(L.RG_MODE_STANDARD, L.RG_PREC_FP64, L.RG_LAYOUT_CSR),
+                                                   (L.RG_MODE_STANDARD, L.RG_PREC_FP64, L.RG_LAYOUT_BAND),
+                                                   (L.RG_MODE_STANDARD, L.RG_PREC_FP32_REFINE, L.RG_LAYOUT_BAND)])
+def test_fast_modes_match_reference(cuda, golden, tag, mode, precision, layout):
     d, m, rhs, _ = _system(golden, tag)
     x = torch.zeros(d.n, dtype=torch.float64, device="cuda")
-    st, dg = R.solve(m, rhs, x, R.opts(tolerance=1e-10, mode=mode, precision=precision))
+    st, dg = R.solve(m, rhs, x, R.opts(tolerance=1e-10, mode=mode, precision=precision, layout=layout))
     assert st == 0 and dg.converged
     ref = golden[f"solve{tag}_x"]
     err = np.linalg.norm(x.cpu().numpy() - ref) / np.linalg.norm(ref)
@@ -361,11 +362,13 @@ def test_paso_band_layout_matches_reference(cuda, golden, tag, sweeps):
     assert torch.linalg.norm(x1 - x) <= 1e-9 * torch.linalg.norm(x)
 
 
+@pytest.mark.parametrize("mode", [L.RG_MODE_PASO, L.RG_MODE_STANDARD])
 @pytest.mark.parametrize("ne", [(40, 33, 27), (7, 5, 130), (300, 211)])
-def test_paso_band_layout_equals_csr(cuda, ne):
-    """The FP64 band SpMV on grids with ragged edge tiles (rows not a multiple of 256) and
-    long iteration counts (replayed graphs): the same iterations within one as the CSR
-    SpMV and the same solution to 1e-9."""
+def test_paso_band_layout_equals_csr(cuda, ne, mode):
+    """The FP64 band SpMV (paso and standard PCG) on grids with ragged edge tiles (rows not a
+    multiple of 256) and long iteration counts (replayed graphs): the same iterations as the
+    CSR SpMV within one (paso) or 0.5 % (textbook CG, whose count over ~900 iterations moves
+    with the order in which the 27 products are added) and the same solution to 1e-9."""
     rng = np.random.default_rng(5)
     dim = len(ne)
     nel, nq = int(np.prod(ne)), 2 ** dim
@@ -385,11 +388,12 @@ def test_paso_band_layout_equals_csr(cuda, ne):
         q[: int(np.prod([v + 1 for v in ne[:-1]]))] = 1.0
         R.insert_constraint(m, rhs, R.dev(q))
         x = torch.zeros(d.n, dtype=torch.float64, device="cuda")
-        st, dg = R.solve(m, rhs, x, R.opts(tolerance=1e-10, layout=layout))
+        st, dg = R.solve(m, rhs, x, R.opts(tolerance=1e-10, layout=layout, mode=mode))
         assert st == 0 and dg.converged
         xs.append(x)
         its.append(int(dg.num_iter))
-    assert abs(its[0] - its[1]) <= 1, its
+    slack = 1 if mode == L.RG_MODE_PASO else max(1, int(0.005 * its[0]))
+    assert abs(its[0] - its[1]) <= slack, its
     assert torch.linalg.norm(xs[1] - xs[0]) <= 1e-9 * torch.linalg.norm(xs[0])
 
 
