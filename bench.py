@@ -186,8 +186,9 @@ def cpu_full_reference_iterations(inp, threads):
 # ----------------------------------------------------------------------------------------------
 
 # algorithmic bytes per launch of the dominant kernel, per DOF (n): the FP32 band SpMV reads
-# 27 band values (4 B each, padded bands count) + z and p_old, and writes p_new and q
-F32_SPMV_BYTES_PER_ROW = 27 * 4 + 4 * 4
+# 27 band values (4 B each, padded bands count) + z and p_old, writes p_new and q, and adds
+# the previous iteration's alpha p_old to the correction d (read + write)
+F32_SPMV_BYTES_PER_ROW = 27 * 4 + 6 * 4
 
 
 def max_over_ranks_of(v, dist=None, device="cpu"):

@@ -48,7 +48,8 @@ struct Scal {
     long long pk;              // FP32 path: parity counter of the two search-direction buffers
     double best;               // FP32 path: smallest recursive residual norm of the segment
     int since;                 // iterations since `best` last dropped by 5%
-    int done, status, pad0;
+    int done, status;
+    int dpend;                 // FP32 path: alpha p of the last SpMV is not yet added to d
 };
 
 enum { ST_RUN = 0, ST_CONV = 1, ST_MAXIT = 3, ST_BREAK = 4 };
@@ -715,6 +716,7 @@ __global__ void __launch_bounds__(kThreads) k_f32_init(int64_t n, const double* 
         }
         s->rho = t[0];
         s->norm = sqrt(t[1]);
+        s->dpend = 0;
     }
 }
 
@@ -730,7 +732,8 @@ __global__ void __launch_bounds__(kTile + 32, 1) k_f32_spmv_tma(const float* __r
                                                                 const __grid_constant__ TmaBandArgs ta,
                                                                 const float* __restrict__ z,
                                                                 float* __restrict__ P0, float* __restrict__ P1,
-                                                                float* __restrict__ q, ReduceBuf rb, Scal* s)
+                                                                float* __restrict__ q, float* __restrict__ d,
+                                                                ReduceBuf rb, Scal* s)
 {
     constexpr int NG = NB / 3;
     constexpr int kBand = NB * kTile;
@@ -741,6 +744,10 @@ __global__ void __launch_bounds__(kTile + 32, 1) k_f32_spmv_tma(const float* __r
     __shared__ int bad;
     if (s->done) return;
     const float beta = (float)s->beta;
+    // the previous iteration's d += alpha p, deferred from k_f32_update to here, where
+    // p_old is already in shared memory
+    const float alpha_prev = (float)s->alpha;
+    const bool dpend = s->dpend != 0;
     const float* __restrict__ pold = (s->pk & 1) ? P1 : P0;
     float* __restrict__ pnew = (s->pk & 1) ? P0 : P1;
     const int t = threadIdx.x;
@@ -796,7 +803,7 @@ __global__ void __launch_bounds__(kTile + 32, 1) k_f32_spmv_tma(const float* __r
             const float* bs = smem + (size_t)st * kStage;
             const int64_t i0 = (blockIdx.x + k * gridDim.x) * (int64_t)kTile;
             const int64_t i = i0 + t;
-            float acc = 0.f, pi = 0.f;
+            float acc = 0.f, pi = 0.f, po = 0.f;
             if (interior(i0)) {
                 const float* zw = bs + kBand;
                 const float* pw = bs + kBand + kWin;
@@ -807,7 +814,10 @@ __global__ void __launch_bounds__(kTile + 32, 1) k_f32_spmv_tma(const float* __r
                     for (int m = 0; m < 3; ++m) {
                         const float pj = fmaf(beta, pw[base + m], zw[base + m]);
                         acc = fmaf(bs[(3 * g + m) * kTile + t], pj, acc);
-                        if (3 * g + m == NB / 2) pi = pj;
+                        if (3 * g + m == NB / 2) {
+                            pi = pj;
+                            po = pw[base + m];
+                        }
                     }
                 }
             } else {
@@ -816,7 +826,10 @@ __global__ void __launch_bounds__(kTile + 32, 1) k_f32_spmv_tma(const float* __r
                     const int64_t j = min(max(i + ta.off[b], (int64_t)0), n - 1);
                     const float pj = fmaf(beta, __ldg(pold + j), __ldg(z + j));
                     acc = fmaf(bs[b * kTile + t], pj, acc);
-                    if (b == NB / 2) pi = pj;
+                    if (b == NB / 2) {
+                        pi = pj;
+                        po = __ldg(pold + j);
+                    }
                 }
             }
             __syncwarp();
@@ -824,6 +837,7 @@ __global__ void __launch_bounds__(kTile + 32, 1) k_f32_spmv_tma(const float* __r
             if (i < n) {
                 pnew[i] = pi;
                 q[i] = acc;
+                if (dpend) d[i] = fmaf(alpha_prev, po, d[i]);
                 v[0] += (double)acc * (double)pi;
             }
         }
@@ -846,10 +860,12 @@ __global__ void __launch_bounds__(kTile + 32, 1) k_f32_spmv_tma(const float* __r
     if (grid_reduce<1>(v, rb, tt) && threadIdx.x == 0) {
         s->delta = tt[0];
         s->alpha = s->rho / tt[0];
+        s->dpend = 1;  // d += alpha p happens in the next SpMV or in k_add_correction
         if (!(fabs(tt[0]) > 0.0)) {
             s->iter += 1;
             s->status = ST_BREAK;
             s->done = 1;
+            s->dpend = 0;
         }
     }
 }
@@ -1026,22 +1042,18 @@ __global__ void __launch_bounds__(kTile + 32, 1) k_band64_bulk(const double* __r
 template <int NB>
 constexpr int band64_stages() { return NB == 27 ? 3 : 8; }
 
-// d += alpha p; r -= alpha q; z = dinv r; rho_next = r.z and ||r||^2 in FP64; tests; beta
-__global__ void __launch_bounds__(kThreads) k_f32_update(int64_t n, float* __restrict__ d,
-                                                         float* __restrict__ r,
+// r -= alpha q; z = dinv r; rho_next = r.z and ||r||^2 in FP64; tests; beta.  (d += alpha p
+// of this iteration is done by the next SpMV, or by k_add_correction at the segment's end.)
+__global__ void __launch_bounds__(kThreads) k_f32_update(int64_t n, float* __restrict__ r,
                                                          const float* __restrict__ q,
-                                                         const float* P0, const float* P1,
                                                          const float* __restrict__ dinv,
                                                          float* __restrict__ z, ReduceBuf rb, Scal* s)
 {
     if (s->done) return;
     const float alpha = (float)s->alpha;
-    const float* __restrict__ p = (s->pk & 1) ? P0 : P1;  // the direction just formed
     double v[2] = {0.0, 0.0};
     const int64_t nv = n >> 2;
-    auto body = [&](int64_t k, float4 d0, float4 r0, float4 q0, float4 p0, float4 di) {
-        st4(d, k, make_float4(fmaf(alpha, p0.x, d0.x), fmaf(alpha, p0.y, d0.y), fmaf(alpha, p0.z, d0.z),
-                              fmaf(alpha, p0.w, d0.w)));
+    auto body = [&](int64_t k, float4 r0, float4 q0, float4 di) {
         const float4 rn = make_float4(fmaf(-alpha, q0.x, r0.x), fmaf(-alpha, q0.y, r0.y),
                                       fmaf(-alpha, q0.z, r0.z), fmaf(-alpha, q0.w, r0.w));
         st4(r, k, rn);
@@ -1050,21 +1062,20 @@ __global__ void __launch_bounds__(kThreads) k_f32_update(int64_t n, float* __res
         v[0] += (double)zn.x * rn.x + (double)zn.y * rn.y + (double)zn.z * rn.z + (double)zn.w * rn.w;
         v[1] += (double)rn.x * rn.x + (double)rn.y * rn.y + (double)rn.z * rn.z + (double)rn.w * rn.w;
     };
-    // two float4 groups per trip with all ten loads issued first: the inputs are mostly L2
-    // hits, and the kernel is bound by load latency rather than bandwidth
+    // two float4 groups per trip with all six loads issued first: the kernel is bound by load
+    // latency rather than bandwidth
     const int64_t st = gstride();
     int64_t k = gtid();
     for (; k + st < nv; k += 2 * st) {
         const int64_t k2 = k + st;
-        const float4 d0 = ld4(d, k), r0 = ld4(r, k), q0 = ld4(q, k), p0 = ld4(p, k), di0 = ld4(dinv, k);
-        const float4 d1 = ld4(d, k2), r1 = ld4(r, k2), q1 = ld4(q, k2), p1 = ld4(p, k2), di1 = ld4(dinv, k2);
-        body(k, d0, r0, q0, p0, di0);
-        body(k2, d1, r1, q1, p1, di1);
+        const float4 r0 = ld4(r, k), q0 = ld4(q, k), di0 = ld4(dinv, k);
+        const float4 r1 = ld4(r, k2), q1 = ld4(q, k2), di1 = ld4(dinv, k2);
+        body(k, r0, q0, di0);
+        body(k2, r1, q1, di1);
     }
-    if (k < nv) body(k, ld4(d, k), ld4(r, k), ld4(q, k), ld4(p, k), ld4(dinv, k));
+    if (k < nv) body(k, ld4(r, k), ld4(q, k), ld4(dinv, k));
     if (gtid() < (n & 3)) {
         const int64_t i = (nv << 2) + gtid();
-        d[i] = fmaf(alpha, p[i], d[i]);
         const float ri = fmaf(-alpha, q[i], r[i]);
         r[i] = ri;
         const float zi = ri * dinv[i];
@@ -1104,11 +1115,18 @@ __global__ void __launch_bounds__(kThreads) k_f32_update(int64_t n, float* __res
     }
 }
 
-// x64 += scale * d32; d32 = 0
-__global__ void k_add_correction(int64_t n, double* __restrict__ x, float* __restrict__ d, double scale)
+// x64 += scale * d32 (with the last SpMV's alpha p when it is still pending); d32 = 0.  The
+// pending flag is cleared by the next k_f32_init.
+__global__ void k_add_correction(int64_t n, double* __restrict__ x, float* __restrict__ d, const float* P0,
+                                 const float* P1, const Scal* s, double scale)
 {
+    const bool dpend = s->dpend != 0;
+    const float alpha = (float)s->alpha;
+    const float* __restrict__ p = (s->pk & 1) ? P1 : P0;  // the last direction formed
     for (int64_t i = gtid(); i < n; i += gstride()) {
-        x[i] += scale * (double)d[i];
+        float di = d[i];
+        if (dpend) di = fmaf(alpha, p[i], di);
+        x[i] += scale * (double)di;
         d[i] = 0.f;
     }
 }
@@ -1391,10 +1409,10 @@ int launch_f32_spmv_tma(Matrix* m, int cfg)
     const int grid = (int)std::min<int64_t>(ntiles, (int64_t)sm_count() * kSpmvCfg[cfg][1]);
     if (cfg == 0)
         RG_TIMED(T_F32_SPMV, (k_f32_spmv_tma<NB, 3><<<grid, kTile + 32, tma_smem<NB, 3>(), stream()>>>(
-                                 m->band32, ta, w->z32, w->p32[0], w->p32[1], w->q32, rbuf(w), w->s)));
+                                 m->band32, ta, w->z32, w->p32[0], w->p32[1], w->q32, w->d32, rbuf(w), w->s)));
     else
         RG_TIMED(T_F32_SPMV, (k_f32_spmv_tma<NB, 2><<<grid, kTile + 32, tma_smem<NB, 2>(), stream()>>>(
-                                 m->band32, ta, w->z32, w->p32[0], w->p32[1], w->q32, rbuf(w), w->s)));
+                                 m->band32, ta, w->z32, w->p32[0], w->p32[1], w->q32, w->d32, rbuf(w), w->s)));
     RG_CHECK_LAUNCH();
     return RG_OK;
 }
@@ -1491,8 +1509,7 @@ int tune_spmv(Matrix* m)
         RG_CHECK_CUDA(cudaEventRecord(e0, stream()));
         for (int k = 0; k < 8 && rc == RG_OK; ++k) {
             RG_TIMED(T_F32_UPDATE, (k_f32_update<<<g, kThreads, 0, stream()>>>(
-                                       w->n, w->d32, w->r32, w->q32, w->p32[0], w->p32[1], m->dinv32, w->z32,
-                                       rbuf(w), w->s)));
+                                       w->n, w->r32, w->q32, m->dinv32, w->z32, rbuf(w), w->s)));
             rc = cudaGetLastError() == cudaSuccess ? RG_OK : RG_CUDA_ERROR;
         }
         RG_CHECK_CUDA(cudaEventRecord(e1, stream()));
@@ -1521,7 +1538,7 @@ int f32_step(Matrix* m)
     int rc = launch_spmv_cfg(m, w->spmv_cfg < 0 ? 0 : w->spmv_cfg);
     if (rc) return rc;
     RG_TIMED(T_F32_UPDATE, (k_f32_update<<<w->grid_upd32 > 0 ? w->grid_upd32 : w->grid_vec, kThreads, 0, stream()>>>(
-                               d->n, w->d32, w->r32, w->q32, w->p32[0], w->p32[1], m->dinv32, w->z32, rbuf(w),
+                               d->n, w->r32, w->q32, m->dinv32, w->z32, rbuf(w),
                                w->s)));
     RG_CHECK_LAUNCH();
     return RG_OK;
@@ -1709,7 +1726,8 @@ int solve_f32(Matrix* m, const rg_solver_opts* o, OuterState& st, rg_diag& dg)
         st.totIter += it;
         done_iters += it;
         // fold the FP32 correction into x and test the FP64 true residual
-        RG_TIMED(T_VECTOR, (k_add_correction<<<eg, kThreads, 0, stream()>>>(n, w->x, w->d32, scale)));
+        RG_TIMED(T_VECTOR, (k_add_correction<<<eg, kThreads, 0, stream()>>>(n, w->x, w->d32, w->p32[0], w->p32[1],
+                                                                            w->s, scale)));
         RG_CHECK_LAUNCH();
         st.last2 = n2r;
         st.lastm = nmr;
