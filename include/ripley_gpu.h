@@ -185,7 +185,8 @@ int rg_save_mm(rg_matrix* mat, const char* path);
 #define RG_LAYOUT_BAND 1          /* SpMV on a 27-band (9 in 2D) structured copy: FP32_REFINE
                                      always; FP64 solves (paso or standard mode) with this
                                      layout stream an FP64 band copy (8 bytes per coefficient
-                                     against the CSR's 12)                                  */
+                                     against the CSR's 12).  Scalar PDEs only: systems
+                                     (block size 2, 3) always use the block CSR            */
 
 typedef struct {
     int method;                 /* RG_METHOD_PCG                                            */
