@@ -646,6 +646,12 @@ class SolverBuddy:
         return self.__precision
 
     def setMatrixLayout(self, layout):
+        """LAYOUT_CSR (default: the SpMV of FP64 solves reads the paso CSR values) or
+        LAYOUT_BAND (FP64 solves of scalar PDEs read an FP64 27-band copy of the balanced
+        matrix instead: the same arithmetic with fewer bytes).  FP32 refinement always uses
+        its FP32 band copy.  No reference counterpart."""
+        if layout not in (SolverOptions.LAYOUT_CSR, SolverOptions.LAYOUT_BAND):
+            raise ValueError("unknown matrix layout %r" % (layout,))
         self.__layout = layout
 
     def getMatrixLayout(self):
