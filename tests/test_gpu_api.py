@@ -265,6 +265,30 @@ def test_jacobi_sweeps_through_solver_options(domain):
 
 
 
+def test_matrix_layout_through_solver_options(domain):
+    """SolverOptions.setMatrixLayout(LAYOUT_BAND): FP64 solves (paso and standard mode) on
+    the FP64 band copy give the known answer u = 1 and, with Dirichlet data, the CSR
+    solution; an unknown layout is rejected."""
+    pde = LinearPDE(domain)
+    pde.setValue(A=kronecker(domain), D=1.0, Y=1.0)
+    pde.getSolverOptions().setMatrixLayout(SolverOptions.LAYOUT_BAND)
+    assert check(pde.getSolution(), 1.0)
+    x = Solution(domain).getX()
+    for mode in (SolverOptions.MODE_PASO, SolverOptions.MODE_STANDARD):
+        us = []
+        for layout in (SolverOptions.LAYOUT_CSR, SolverOptions.LAYOUT_BAND):
+            p = LinearPDE(domain)
+            p.setValue(A=kronecker(domain), Y=1.0, q=whereZero(x[0]))
+            so = p.getSolverOptions()
+            so.setSolverMode(mode)
+            so.setMatrixLayout(layout)
+            so.setTolerance(1e-10)
+            us.append(p.getSolution())
+        assert Lsup(us[1] - us[0]) <= 1e-8 * Lsup(us[0])
+    with pytest.raises(ValueError):
+        pde.getSolverOptions().setMatrixLayout(7)
+
+
 # ---- LinearPDE coefficient handling, after escriptcore/test/python/test_linearPDEs.py
 # (Test_LinearPDE: test_setCoefficient_*_Scalar / _System, test_reducedOn,
 # test_setCoefficient_WithIllegalFunctionSpace, test_resetCoefficient_WithWrongShape)
