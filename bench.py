@@ -243,6 +243,8 @@ def run_ours(args):
     n, nnz = n.value, nnz.value
     mat = C.c_void_p()
     L.check(lib.rg_matrix_create(dom, C.byref(mat)))
+    if args.spmv_config >= 0:  # profiling runs: a fixed FP32 SpMV pipeline instead of the tuner's
+        L.check(lib.rg_solver_set_config(mat, args.spmv_config))
     rhs = torch.zeros(n, dtype=torch.float64, device=dev)
     x = torch.zeros(n, dtype=torch.float64, device=dev)
 
@@ -639,6 +641,9 @@ def main():
     ap.add_argument("--sweeps", type=int, default=8, help="Chebyshev smoothing steps on the learned guess")
     ap.add_argument("--no-batched", dest="batched", action="store_false",
                     help="skip the batched 64-system workload")
+    ap.add_argument("--spmv-config", type=int, choices=[-1, 0, 1], default=-1,
+                    help="FP32 SpMV pipeline: -1 tuned (default), 0 = 3 stages x 1 CTA/SM, "
+                         "1 = 2 stages x 2 CTAs/SM")
     ap.add_argument("--only", choices=["all", "fast", "plain", "plain_band"], default="all",
                     help="profiling runs: only the fast path, or only the plain FP64 paso solve "
                          "(CSR, or the FP64 band copy)")
