@@ -39,10 +39,13 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
     return ok != 0;
 }
 
+// polls of a bounded wait unless the caller gives another limit
+constexpr int kDefaultPolls = 1 << 22;
+
 // bounded wait; false when it gave up
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity)
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int polls = kDefaultPolls)
 {
-    for (int tries = 0; tries < (1 << 22); ++tries)
+    for (int tries = 0; tries < polls; ++tries)
         if (mbar_try_wait(bar, parity)) return true;
     return false;
 }

@@ -241,6 +241,9 @@ int solver_prepare(Matrix* m, bool band);
 int solver_config(const Matrix* m, int* spmv_cfg, int* update_grid, double* spmv_us);
 // fixes the FP32 SpMV configuration (-1: tune at the next FP32 solve)
 int solver_set_config(Matrix* m, int spmv_cfg);
+// poll limit of the band kernels' bounded waits (0: default) and whether their producer
+// withholds its copies (rg_test_wait_limit)
+int set_wait_control(int polls, int withhold);
 void free_workspace(Matrix* m);
 // hands the matrix's solver vectors to its domain for the next matrix there (one is kept; a
 // further one is freed), instead of freeing them: a fresh matrix on the same grid then

@@ -650,6 +650,24 @@ constexpr int kPWin = kTile + 8;
 constexpr int kConsumerWarps = kTile / 32;
 enum { ST_TIMEOUT = 6 };
 
+// Limits of the bounded waits of the warp-specialised kernels below, read once per CTA.
+// polls = 0 keeps the default limit; withhold != 0 makes the producer issue no copies, so
+// that every consumer wait runs out without any copy in flight (the test of the timeout
+// path sets both through rg_test_wait_limit).
+struct WaitCtl {
+    int polls;
+    int withhold;
+};
+__device__ WaitCtl g_wait_ctl = {0, 0};
+
+// A CTA whose wait gave up records the timeout; status codes are ordered so that the
+// most severe one wins when several CTAs report at once (ST_TIMEOUT > ST_BREAK > ...).
+__device__ __forceinline__ void report_status(Scal* s, int st)
+{
+    atomicMax(&s->status, st);
+    s->done = 1;
+}
+
 struct TmaBandArgs {
     int off[27];   // column offset of band b
     int goff[9];   // column offset of stencil column g = (dy,dz) at dx = -1
@@ -768,13 +786,15 @@ __global__ void __launch_bounds__(kTile + 32, 1) k_f32_spmv_tma(const float* __r
 
     double v[1] = {0.0};
     int64_t issued = 0;
+    const WaitCtl wc = g_wait_ctl;
+    const int polls = wc.polls > 0 ? wc.polls : kDefaultPolls;
     if (warp == kConsumerWarps) {
         // ---------------- producer
-        if ((t & 31) == 0) {
+        if ((t & 31) == 0 && !wc.withhold) {
             const uint64_t pol = evict_first_policy();
             for (int64_t k = 0; k < my_tiles; ++k, issued = k) {
                 const int st = (int)(k % kStages);
-                if (k >= kStages && !mbar_wait(&empty[st], (uint32_t)(((k / kStages) - 1) & 1))) {
+                if (k >= kStages && !mbar_wait(&empty[st], (uint32_t)(((k / kStages) - 1) & 1), polls)) {
                     bad = 1;
                     break;
                 }
@@ -796,7 +816,7 @@ __global__ void __launch_bounds__(kTile + 32, 1) k_f32_spmv_tma(const float* __r
         // ---------------- consumers: row i0 + t of every tile
         for (int64_t k = 0; k < my_tiles; ++k) {
             const int st = (int)(k % kStages);
-            if (!mbar_wait(&full[st], (uint32_t)((k / kStages) & 1))) {
+            if (!mbar_wait(&full[st], (uint32_t)((k / kStages) & 1), polls)) {
                 bad = 1;
                 break;
             }
@@ -850,11 +870,10 @@ __global__ void __launch_bounds__(kTile + 32, 1) k_f32_spmv_tma(const float* __r
                 for (int tries = 0; tries < (1 << 20) && !mbar_try_wait(&full[k % kStages], (uint32_t)((k / kStages) & 1));
                      ++tries) {
                 }
-        if (t == 0) {
-            s->status = ST_TIMEOUT;
-            s->done = 1;
-        }
-        return;
+        if (t == 0) report_status(s, ST_TIMEOUT);
+        // the CTA still takes its turn in the grid reduction (with nothing to add), so the
+        // reduction counter ends the launch at zero for the kernels that follow
+        v[0] = 0.0;
     }
     double tt[1];
     if (grid_reduce<1>(v, rb, tt) && threadIdx.x == 0) {
@@ -863,8 +882,7 @@ __global__ void __launch_bounds__(kTile + 32, 1) k_f32_spmv_tma(const float* __r
         s->dpend = 1;  // d += alpha p happens in the next SpMV or in k_add_correction
         if (!(fabs(tt[0]) > 0.0)) {
             s->iter += 1;
-            s->status = ST_BREAK;
-            s->done = 1;
+            report_status(s, ST_BREAK);
             s->dpend = 0;
         }
     }
@@ -924,13 +942,15 @@ __global__ void __launch_bounds__(kTile + 32, 1) k_band64_bulk(const double* __r
 
     double v[1] = {0.0};
     int64_t issued = 0;
+    const WaitCtl wc = g_wait_ctl;
+    const int polls = wc.polls > 0 ? wc.polls : kDefaultPolls;
     if (warp == kConsumerWarps) {
         // ---------------- producer
-        if ((t & 31) == 0) {
+        if ((t & 31) == 0 && !wc.withhold) {
             const uint64_t pol = evict_first_policy();
             for (int64_t k = 0; k < my_tiles; ++k, issued = k) {
                 const int st = (int)(k % kStages);
-                if (k >= kStages && !mbar_wait(&empty[st], (uint32_t)(((k / kStages) - 1) & 1))) {
+                if (k >= kStages && !mbar_wait(&empty[st], (uint32_t)(((k / kStages) - 1) & 1), polls)) {
                     bad = 1;
                     break;
                 }
@@ -951,7 +971,7 @@ __global__ void __launch_bounds__(kTile + 32, 1) k_band64_bulk(const double* __r
         // ---------------- consumers: row i0 + t of every tile
         for (int64_t k = 0; k < my_tiles; ++k) {
             const int st = (int)(k % kStages);
-            if (!mbar_wait(&full[st], (uint32_t)((k / kStages) & 1))) {
+            if (!mbar_wait(&full[st], (uint32_t)((k / kStages) & 1), polls)) {
                 bad = 1;
                 break;
             }
@@ -1004,11 +1024,10 @@ __global__ void __launch_bounds__(kTile + 32, 1) k_band64_bulk(const double* __r
                 for (int tries = 0; tries < (1 << 20) && !mbar_try_wait(&full[k % kStages], (uint32_t)((k / kStages) & 1));
                      ++tries) {
                 }
-        if (t == 0) {
-            s->status = ST_TIMEOUT;
-            s->done = 1;
-        }
-        return;
+        if (t == 0) report_status(s, ST_TIMEOUT);
+        // the CTA still takes its turn in the grid reduction (with nothing to add), so the
+        // reduction counter ends the launch at zero for the kernels that follow
+        v[0] = 0.0;
     }
     if (SWEEP && mode == 0) return;
     double tt[1];
@@ -1018,16 +1037,14 @@ __global__ void __launch_bounds__(kTile + 32, 1) k_band64_bulk(const double* __r
             s->alpha = s->tau / tt[0];
             if (fabs(tt[0]) <= 0.0) {  // breakFlag
                 s->iter += 1;
-                s->status = ST_BREAK;
-                s->done = 1;
+                report_status(s, ST_BREAK);
             }
         } else if (!SWEEP) {
             s->delta = tt[0];
             s->alpha = s->rho / tt[0];
             if (!(fabs(tt[0]) > 0.0)) {
                 s->iter += 1;
-                s->status = ST_BREAK;
-                s->done = 1;
+                report_status(s, ST_BREAK);
             }
         } else if (mode == 1) {
             s->tau_next = tt[0];
@@ -1635,6 +1652,10 @@ int status_from(int st, long long it, const rg_solver_opts* o, long long totIter
         set_error("Solver: maximum number of iteration steps reached.\nReturned solution does not fulfil stopping criterion.");
         return RG_MAXITER;
     }
+    if (st == ST_TIMEOUT) {
+        set_error("solver: a bounded device wait of the band SpMV pipeline gave up");
+        return RG_TIMEOUT;
+    }
     if (st == ST_BREAK) {
         if (it <= 1) {
             if (o->verbose) printf("Solver: Uncurable break down!\n");
@@ -1725,6 +1746,10 @@ int solve_f32(Matrix* m, const rg_solver_opts* o, OuterState& st, rg_diag& dg)
         if ((rc = run_until_done(m, 2, f32_step, chunk, cap, &it, &dst))) return rc;
         st.totIter += it;
         done_iters += it;
+        if (dst == ST_TIMEOUT) {
+            bool restart = false;
+            return status_from(dst, it, o, st.totIter, &restart);
+        }
         // fold the FP32 correction into x and test the FP64 true residual
         RG_TIMED(T_VECTOR, (k_add_correction<<<eg, kThreads, 0, stream()>>>(n, w->x, w->d32, w->p32[0], w->p32[1],
                                                                             w->s, scale)));
@@ -1771,6 +1796,19 @@ int solver_set_config(Matrix* m, int spmv_cfg)
     }
     m->force_spmv = spmv_cfg;
     if (m->ws) m->ws->spmv_cfg = -1;  // re-tune (and apply) at the next FP32 solve
+    return RG_OK;
+}
+
+int set_wait_control(int polls, int withhold)
+{
+    if (polls < 0) {
+        set_error("rg_test_wait_limit: max_polls must be >= 0");
+        return RG_INVALID_ARG;
+    }
+    const WaitCtl c = {polls, withhold ? 1 : 0};
+    // no solver kernel may be running while the limits change
+    RG_CHECK_CUDA(cudaDeviceSynchronize());
+    RG_CHECK_CUDA(cudaMemcpyToSymbol(g_wait_ctl, &c, sizeof(c)));
     return RG_OK;
 }
 
@@ -1909,6 +1947,9 @@ int solve_impl(Matrix* m, const double* rhs, double* x, const rg_solver_opts* o,
     int rc = ensure_workspace(m, fp32);
     if (rc) return rc;
     Workspace* w = m->ws;
+    // every grid reduction leaves the counter at zero; clearing it here as well keeps one
+    // solve independent of anything an earlier, interrupted one left behind
+    RG_CHECK_CUDA(cudaMemsetAsync(w->counter, 0, sizeof(unsigned), stream()));
     const bool band64 = !fp32 && o->layout == RG_LAYOUT_BAND;
     if ((rc = prepare(m, fp32, band64))) return rc;
     w->band64 = band64;

@@ -1,0 +1,90 @@
+"""Failure detection on the GPU without a GPU fault: the bounded waits of the band SpMV
+kernels are made to run out (their producer withholds every copy, so nothing is ever in
+flight), the solve must return RG_TIMEOUT, and the next solve on the same matrix and domain
+must match the oracle, i.e. nothing the interrupted launch left behind (the grid-reduction
+counter, the device scalars, the captured iteration graphs) leaks into later work.
+
+The paso status mapping the library follows is paso/src/solve.cpp:119-142 (a solver status
+becomes an exception); RG_TIMEOUT has no paso counterpart because paso has no device waits.
+"""
+import numpy as np
+import pytest
+import torch
+
+from oracle import oracle as O
+import rgcapi as R
+from esys_b200 import _lib as L
+
+pytestmark = pytest.mark.gpu
+
+
+def _problem(ne, seed):
+    rng = np.random.default_rng(seed)
+    nel = int(np.prod(ne))
+    kappa = np.exp(rng.standard_normal(nel))
+    A = np.zeros((nel, 8, 3, 3))
+    for i in range(3):
+        A[:, :, i, i] = kappa[:, None]
+    A = A.reshape(-1)
+    Y = rng.standard_normal(nel * 8)
+    d = R.Domain(3, ne)
+    m = R.Matrix(d)
+    rhs = torch.zeros(d.n, dtype=torch.float64, device="cuda")
+    keep = []
+    R.assemble(m, rhs, keep, A=(A, R.KINDS["exp"]), Y=(Y, R.KINDS["exp"]))
+    q = np.zeros(d.n)
+    q[-(ne[0] + 1) * (ne[1] + 1):] = 1.0  # top face
+    R.insert_constraint(m, rhs, R.dev(q))
+    pat = O.pattern(3, ne)
+    val, rr = O.assemble(3, ne, d.dx, pat, A=(O.EXPANDED, A), Y=(O.EXPANDED, Y))
+    O.insert_constraint(pat, val, rr, q)
+    return d, m, rhs, keep, (pat, val, rr)
+
+
+@pytest.mark.parametrize("mode,precision,tol", [
+    (L.RG_MODE_PASO, L.RG_PREC_FP64, 1e-8),        # k_band64_bulk (paso PCG on the FP64 band copy)
+    (L.RG_MODE_STANDARD, L.RG_PREC_FP32_REFINE, 1e-7),  # k_f32_spmv_tma (FP32 inner PCG)
+])
+def test_band_kernel_wait_timeout_is_reported_and_recoverable(cuda, mode, precision, tol):
+    d, m, rhs, _keep, (pat, val, rr) = _problem((24, 20, 18), 31)
+    ref = O.solve_paso(pat, val.copy(), rr, tol=1e-10)  # balances its copy in place
+    assert ref.converged
+    o = R.opts(tolerance=1e-10, mode=mode, precision=precision, layout=L.RG_LAYOUT_BAND)
+    x = torch.zeros(d.n, dtype=torch.float64, device="cuda")
+    # a normal solve first: the FP32 tuner and the captured iteration graphs exist before the
+    # waits are shortened, so the interrupted solve replays graphs captured earlier
+    st, dg = R.solve(m, rhs, x, o)
+    assert st == 0 and dg.converged
+    first = x.clone()
+    lib = R.lib()
+    x.fill_(7.0)
+    L.check(lib.rg_test_wait_limit(64, 1))
+    try:
+        st, dg = R.solve(m, rhs, x, o)
+    finally:
+        L.check(lib.rg_test_wait_limit(0, 0))
+    assert st == L.RG_TIMEOUT, (st, L.last_error())
+    assert "wait" in L.last_error()
+    assert not dg.converged
+    # the library, the matrix and its domain stay usable, and nothing from the interrupted
+    # launch leaks into the next solve
+    x.zero_()
+    st, dg = R.solve(m, rhs, x, o)
+    assert st == 0 and dg.converged
+    err = np.linalg.norm(x.cpu().numpy() - ref.x) / np.linalg.norm(ref.x)
+    assert err < tol, err
+    assert torch.allclose(x, first, rtol=0, atol=1e-12 * float(first.abs().max()))
+    if precision == L.RG_PREC_FP64:
+        assert abs(int(dg.num_iter) - ref.num_iter) <= 1
+    # an unrelated reduction on the same workspace (the residual norms) is exact as well
+    import ctypes
+    l2, lm = ctypes.c_double(), ctypes.c_double()
+    L.check(lib.rg_residual_norms(m.h, R.ptr(rhs), R.ptr(x), ctypes.byref(l2), ctypes.byref(lm)))
+    res = rr - O.spmv(pat, val, x.cpu().numpy())
+    assert abs(l2.value - np.linalg.norm(res)) <= 1e-9 * np.linalg.norm(rr)
+
+
+def test_wait_limit_arguments_are_checked(cuda):
+    lib = R.lib()
+    assert lib.rg_test_wait_limit(-1, 0) == L.RG_INVALID_ARG
+    L.check(lib.rg_test_wait_limit(0, 0))
