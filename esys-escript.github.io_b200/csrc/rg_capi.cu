@@ -544,14 +544,16 @@ int rg_save_mm(rg_matrix* mat, const char* path)
         set_error(std::string("rg_save_mm: cannot open ") + path);
         return RG_INVALID_ARG;
     }
-    // scalar coordinates: block entry (ir, ic) of node pair (i, j) is row i nb + ir, column j nb + ic
+    // SparseMatrix<double>::saveMM (paso/src/SparseMatrix.cpp:180-240): banner, size line, then
+    // per node pair (i, j) of the pattern its block entries (ir, ic), row-block index outer, as
+    // scalar coordinates (i nb + ir, j nb + ic), 1-based, values with 15 significant digits
     fprintf(f, "%%%%MatrixMarket matrix coordinate real general\n");
     fprintf(f, "%lld %lld %lld\n", (long long)d.n * nb, (long long)d.n * nb, (long long)d.nnz * nb * nb);
     for (int64_t i = 0; i < d.n; ++i)
-        for (int ir = 0; ir < nb; ++ir)
-            for (int32_t k = ptr[i]; k < ptr[i + 1]; ++k)
+        for (int32_t k = ptr[i]; k < ptr[i + 1]; ++k)
+            for (int ir = 0; ir < nb; ++ir)
                 for (int ic = 0; ic < nb; ++ic)
-                    fprintf(f, "%lld %lld %.17g\n", (long long)(i * nb + ir + 1), (long long)idx[k] * nb + ic + 1,
+                    fprintf(f, "%lld %lld %.15g\n", (long long)(i * nb + ir + 1), (long long)idx[k] * nb + ic + 1,
                             val[(size_t)k * nb * nb + ir + nb * ic]);
     fclose(f);
     return RG_OK;
@@ -584,6 +586,11 @@ int rg_solver_set_config(rg_matrix* mat, int spmv_config)
 {
     RG_REQUIRE(mat, "rg_solver_set_config: NULL matrix");
     return rg::solver_set_config(&mat->m, spmv_config);
+}
+
+int rg_test_wait_limit(int max_polls, int withhold_copies)
+{
+    return rg::set_wait_control(max_polls, withhold_copies);
 }
 
 int rg_solve(rg_matrix* mat, const double* rhs, double* x, const rg_solver_opts* opts, rg_diag* diag)

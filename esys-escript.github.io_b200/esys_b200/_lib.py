@@ -102,6 +102,7 @@ _SIGNATURES = {
     "rg_residual_norms": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_double),
                                     C.POINTER(C.c_double)]),
     "rg_solver_set_config": (C.c_int, [C.c_void_p, C.c_int]),
+    "rg_test_wait_limit": (C.c_int, [C.c_int, C.c_int]),
     "rg_residual_norms_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_double),
                                             C.POINTER(C.c_double)]),
     "rg_solver_opts_default": (None, [C.POINTER(rg_solver_opts)]),
@@ -129,6 +130,8 @@ _SIGNATURES = {
     "rg_ws_field_stats": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int64, C.c_double, C.c_void_p,
                                     C.c_void_p]),
     "rg_ws_pack_input": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.POINTER(rg_act), C.c_void_p]),
+    "rg_ws_element_fields": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_int64, C.c_void_p,
+                                       C.c_void_p]),
     "rg_ws_nodes_to_cells": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p,
                                        C.c_void_p]),
     "rg_ws_cells_to_nodes": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int,

@@ -165,11 +165,17 @@ int rg_residual_norms(rg_matrix* mat, const double* rhs, const double* x, double
    device memory, or a latency-critical loop that cannot absorb the implicit
    synchronisation of cudaMalloc/cudaFree).  All calls share the array: calls that overlap
    on the GPU race and must be serialised.  The first call on a device looks up the array's
-   address (make it before any stream capture).  Sizes whose reduction would need more
-   partial sums than the array holds are rejected with RG_INVALID_ARG. */
+   address (make it before any stream capture); a call whose device work fails forgets it,
+   so a call after cudaDeviceReset looks it up again.  The reduction grid is capped at 1184
+   CTAs for any size, so every size fits the array; should that cap ever exceed it, the call
+   returns RG_INVALID_ARG instead of writing past the array.  PDE systems (block size > 1):
+   RG_NOT_SUPPORTED. */
 int rg_residual_norms_noalloc(rg_matrix* mat, const double* rhs, const double* x,
                               double* l2_host, double* linf_host);
-/* MatrixMarket coordinate real general, 1-based (SystemMatrix::saveMM) */
+/* SystemMatrix::saveMM (paso/src/SystemMatrix.h:70-80 -> SparseMatrix<double>::saveMM,
+   paso/src/SparseMatrix.cpp:180-240): MatrixMarket coordinate real general, 1-based, the
+   values as they are now (balanced in place after a solve, as in paso), entries in paso's
+   order: node rows, their pattern entries, then block row and block column. */
 int rg_save_mm(rg_matrix* mat, const char* path);
 
 /* ---- solver: SolverBuddy subset + paso Options (escriptcore/src/SolverOptions.cpp:40-70) */
@@ -243,6 +249,16 @@ int rg_solver_config(const rg_matrix* mat, int* spmv_config, int* update_grid, d
    tuner's choice).  The tuner still times both configurations, so rg_solver_config reports
    them. */
 int rg_solver_set_config(rg_matrix* mat, int spmv_config);
+
+/* Test hook for the timeout path of the band SpMV kernels (no reference counterpart; paso
+   has no device waits).  max_polls > 0 caps the polls of each bounded wait of the
+   warp-specialised band kernels (FP32_REFINE, and FP64 with RG_LAYOUT_BAND); 0 restores the
+   default limit.  withhold_copies != 0 makes their producer issue no copies, so every
+   consumer wait runs out with nothing in flight: the solve then returns RG_TIMEOUT and the
+   matrix, its domain and the library stay usable.  Applies to all matrices on the current
+   device from the next launch on; it waits for the device to be idle first.  Not for use
+   in production code. */
+int rg_test_wait_limit(int max_polls, int withhold_copies);
 
 /* ---- batched solves (no reference counterpart: many independent systems at once) ------- */
 /* A batch holds assembled matrices of the same dimension (any sizes) that are solved
@@ -348,6 +364,12 @@ int rg_ws_weights_bf16(const float* w, void* w_fwd, void* w_dgrad, int c_out, in
 int rg_ws_field_stats(const float* kappa, const float* y, int nsamples, int64_t per_sample, double h_net,
                       float* stats, double* work);
 int rg_ws_pack_input(const float* kappa, const float* y, int factor, rg_act* x, const float* stats);
+/* The per-element fields the network reads, from the PDE's coefficient arrays (device
+   pointers): kappa[e] = A[e a_stride] (A's first entry: a_stride 9 for A per element, 72
+   for A on the Gauss points, whose first point is taken), y[e] = mean of Y[e y_points ..
+   e y_points + y_points - 1]; fp32 outputs, nel elements. */
+int rg_ws_element_fields(const double* A, int a_stride, const double* Y, int y_points, int64_t nel, float* kappa,
+                         float* y);
 /* training target per network cell: mean of the nodal solution u (fp64, (f d+1)(f h+1)(f w+1)
    nodes per sample) over the cell, in units of u_unit */
 int rg_ws_nodes_to_cells(const double* u, int factor, int nsamples, int d, int h, int w, const float* stats,
