@@ -15,7 +15,12 @@
 //    the caller;
 //  * the first call on a device looks up the array's device address with the device
 //    current (cudaGetSymbolAddress) and caches it; make that first call before any
-//    stream capture.
+//    stream capture.  The cached address does not survive cudaDeviceReset: a call whose
+//    device work fails drops it, so the next call looks it up again.
+//
+// The reduction grid of k_residual_norms is capped at residual::kMaxBlocks CTAs for every
+// size, so the array always holds enough partial sums; the size check below guards that
+// invariant should the cap ever change.
 #include <cmath>
 #include <mutex>
 
@@ -25,6 +30,8 @@ namespace rg {
 namespace {
 
 constexpr int kMaxPartialBlocks = residual::kMaxBlocks;          // 1184 CTAs
+static_assert(residual::kMaxBlocks >= kNumSMs * 8,
+              "the residual grid (grid_for caps it at kNumSMs * 8 CTAs) must fit the static scratch");
 constexpr int kScratchDoubles = 2 * kMaxPartialBlocks + 4;       // partials, result, counter
 constexpr int kOutSlot = 2 * kMaxPartialBlocks;                  // 2 doubles
 constexpr int kCounterSlot = 2 * kMaxPartialBlocks + 2;          // an unsigned in a double slot
@@ -58,6 +65,35 @@ int scratch_address(double** out)
     return RG_OK;
 }
 
+// forgets the current device's address after failed device work (e.g. after a device reset)
+void drop_address()
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return;
+    std::lock_guard<std::mutex> lk(g_mu);
+    g_addr[dev] = nullptr;
+}
+
+// the reduction on the static scratch: clear the counter, launch, read the two results
+int norms_with_scratch(Matrix* m, double* scratch, int grid, const double* rhs, const double* x, double* l2_host,
+                       double* linf_host)
+{
+    const Domain* d = m->dom;
+    unsigned* counter = reinterpret_cast<unsigned*>(scratch + kCounterSlot);
+    double* out = scratch + kOutSlot;
+    RG_CHECK_CUDA(cudaMemsetAsync(counter, 0, sizeof(unsigned), stream()));
+    RG_TIMED(T_NORMS, (residual::k_residual_norms<<<grid, residual::kThreads, 0, stream()>>>(
+                          d->n, d->ptr, d->idx, m->val, m->balanced ? m->bv : nullptr, rhs, x,
+                          ReduceBuf{scratch, counter}, out)));
+    RG_CHECK_LAUNCH();
+    double h[2];
+    RG_CHECK_CUDA(cudaMemcpyAsync(h, out, sizeof(h), cudaMemcpyDeviceToHost, stream()));
+    RG_CHECK_CUDA(cudaStreamSynchronize(stream()));
+    if (l2_host) *l2_host = std::sqrt(h[0]);
+    if (linf_host) *linf_host = h[1];
+    return RG_OK;
+}
+
 }  // namespace
 }  // namespace rg
 
@@ -82,17 +118,7 @@ extern "C" int rg_residual_norms_noalloc(rg_matrix* mat, const double* rhs, cons
     double* scratch = nullptr;
     int rc = scratch_address(&scratch);
     if (rc) return rc;
-    unsigned* counter = reinterpret_cast<unsigned*>(scratch + kCounterSlot);
-    double* out = scratch + kOutSlot;
-    RG_CHECK_CUDA(cudaMemsetAsync(counter, 0, sizeof(unsigned), stream()));
-    RG_TIMED(T_NORMS, (residual::k_residual_norms<<<grid, residual::kThreads, 0, stream()>>>(
-                          d->n, d->ptr, d->idx, m->val, m->balanced ? m->bv : nullptr, rhs, x,
-                          ReduceBuf{scratch, counter}, out)));
-    RG_CHECK_LAUNCH();
-    double h[2];
-    RG_CHECK_CUDA(cudaMemcpyAsync(h, out, sizeof(h), cudaMemcpyDeviceToHost, stream()));
-    RG_CHECK_CUDA(cudaStreamSynchronize(stream()));
-    if (l2_host) *l2_host = std::sqrt(h[0]);
-    if (linf_host) *linf_host = h[1];
-    return RG_OK;
+    rc = norms_with_scratch(m, scratch, grid, rhs, x, l2_host, linf_host);
+    if (rc == RG_CUDA_ERROR) drop_address();
+    return rc;
 }
