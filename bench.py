@@ -121,19 +121,13 @@ class ClockSampler:
 # CPU baseline: the reference's own assembler + paso solver (oracle/_ref), else the oracle port
 # ----------------------------------------------------------------------------------------------
 
-def cpu_reference_sample(inp, n_iter_full: int | None, threads: int):
-    """Times, on the host cores, the reference's assembly of the full input, the constraint,
-    and paso's solve for 10 and for 40 iterations; the time-to-solution is extrapolated as
-    assemble + constrain + setup + n_iter * (time per iteration).  Returns a dict."""
+def _reference_system(inp, use_ref):
+    """The reference's assembly (DefaultAssembler3D with A expanded to the Gauss points, the
+    form escript hands it) and insertConstraint of the full input.  Returns the pattern,
+    values, right hand side and the two times."""
     from oracle import oracle as O
     ne = inp["ne"]
     nel = ne ** 3
-    kind = "reference" if O.have_ref() else "port"
-    use_ref = kind == "reference"
-    if use_ref:
-        O.set_threads(threads)
-    else:
-        os.environ["OMP_NUM_THREADS"] = str(threads)
     A = np.zeros((nel, 8, 3, 3))
     for i in range(3):
         A[:, :, i, i] = inp["kappa"][:, None]
@@ -145,40 +139,46 @@ def cpu_reference_sample(inp, n_iter_full: int | None, threads: int):
     t1 = time.perf_counter()
     O.insert_constraint(pat, val, rhs, inp["q"])
     t2 = time.perf_counter()
-    times = {}
-    for its in (10, 40):
-        v = val.copy()
-        s0 = time.perf_counter()
-        r = O.solve_paso(pat, v, rhs, tol=RTOL, iter_max=its, use_ref=use_ref)
-        times[its] = (time.perf_counter() - s0, r.num_iter)
-    (ta, ia), (tb, ib) = times[10], times[40]
-    per_iter = (tb - ta) / max(ib - ia, 1)
-    setup = ta - ia * per_iter
-    out = {"assemble_s": t1 - t0, "constraint_s": t2 - t1, "setup_s": setup, "per_iter_s": per_iter,
-           "kind": kind, "cores": threads}
-    if n_iter_full:
-        out["time_to_solution_s"] = (t1 - t0) + (t2 - t1) + setup + n_iter_full * per_iter
+    return pat, val, rhs, t1 - t0, t2 - t1
+
+
+def cpu_reference_solve(inp, threads, rtol=RTOL, oracle_rtol=None):
+    """One complete time-to-solution of the reference on the host cores: its own assembly,
+    the constraint and paso's Solver/PCG to rtol (oracle/_ref, the reference's sources
+    compiled in place; the oracle port where that library is absent).  With oracle_rtol it
+    also solves the same system to that tolerance (untimed) and returns that solution as
+    the FP64 oracle the GPU solutions are measured against."""
+    from oracle import oracle as O
+    use_ref = O.have_ref()
+    kind = "reference" if use_ref else "port"
+    if use_ref:
+        O.set_threads(threads)
+    else:
+        os.environ["OMP_NUM_THREADS"] = str(threads)
+    pat, val, rhs, t_asm, t_con = _reference_system(inp, use_ref)
+    val0 = val.copy() if oracle_rtol else None
+    s0 = time.perf_counter()
+    r = O.solve_paso(pat, val, rhs, tol=rtol, use_ref=use_ref)
+    t_sol = time.perf_counter() - s0
+    out = {"kind": kind, "cores": threads, "assemble_s": t_asm, "constraint_s": t_con, "solve_s": t_sol,
+           "time_to_solution_s": t_asm + t_con + t_sol, "iterations": int(r.num_iter),
+           "converged": bool(r.converged), "x": r.x}
+    if oracle_rtol:
+        ro = O.solve_paso(pat, val0, rhs, tol=oracle_rtol, use_ref=use_ref)
+        out["x_oracle"] = ro.x
+        out["oracle_iterations"] = int(ro.num_iter)
     return out
 
 
-def cpu_full_reference_iterations(inp, threads):
-    """One complete paso solve with the reference code (gives paso's iteration count)."""
+def cpu_reference_warmup(inp, threads):
+    """A bounded warm-up of the reference on the host: assembly, constraint and 10 paso
+    iterations (pages the code and the arrays in)."""
     from oracle import oracle as O
-    ne = inp["ne"]
-    nel = ne ** 3
     use_ref = O.have_ref()
     if use_ref:
         O.set_threads(threads)
-    A = np.zeros((nel, 8, 3, 3))
-    for i in range(3):
-        A[:, :, i, i] = inp["kappa"][:, None]
-    pat = O.pattern(3, (ne, ne, ne))
-    val, rhs = O.assemble(3, (ne, ne, ne), [1.0 / ne] * 3, pat, A=(O.EXPANDED, A.reshape(-1)),
-                          Y=(O.EXPANDED, inp["Y"]), use_ref=use_ref)
-    O.insert_constraint(pat, val, rhs, inp["q"])
-    t0 = time.perf_counter()
-    r = O.solve_paso(pat, val, rhs, tol=RTOL, use_ref=use_ref)
-    return r.num_iter, time.perf_counter() - t0
+    pat, val, rhs, _, _ = _reference_system(inp, use_ref)
+    O.solve_paso(pat, val, rhs, tol=RTOL, iter_max=10, use_ref=use_ref)
 
 
 # ----------------------------------------------------------------------------------------------
@@ -291,8 +291,9 @@ def run_ours(args):
             Yd = Y_d if Y_dev is None else Y_dev
             side.wait_stream(stream)
             with torch.cuda.stream(side):
-                kap32.view(-1).copy_(Ad.view(-1, 9)[:, 0])
-                y32.view(-1).copy_(Yd.view(-1, 8).mean(dim=1))
+                L.set_stream_from_torch()
+                L.check(lib.rg_ws_element_fields(C.c_void_p(Ad.data_ptr()), 9, C.c_void_p(Yd.data_ptr()), 8,
+                                                 nel, C.c_void_p(kap32.data_ptr()), C.c_void_p(y32.data_ptr())))
                 warm.guess(kap32, y32, (ne, ne, ne), q=qq, out=guess)
             L.set_stream_from_torch()  # library work back on the main stream
         L.check(lib.rg_matrix_reset(mat))
@@ -348,6 +349,7 @@ def run_ours(args):
     ev1.record(stream)
     torch.cuda.synchronize()
     plain_ms = max_over_ranks(ev0.elapsed_time(ev1) / n_plain)
+    x_plain = x.clone()
 
     # --- the same FP64 paso PCG with its SpMV on the FP64 band copy (RG_LAYOUT_BAND)
     plain_band = opts(L.RG_MODE_PASO, L.RG_PREC_FP64)
@@ -360,6 +362,21 @@ def run_ours(args):
     ev1.record(stream)
     torch.cuda.synchronize()
     plain_band_ms = max_over_ranks(ev0.elapsed_time(ev1) / n_plain)
+    x_plain_band = x.clone()
+
+    # --- textbook Jacobi-PCG in FP64 (RG_MODE_STANDARD) on the FP64 band copy: the fastest
+    # FP64 solve of the library, the baseline the mixed-precision speed-up is quoted against
+    std_band = opts(L.RG_MODE_STANDARD, L.RG_PREC_FP64)
+    std_band.layout = L.RG_LAYOUT_BAND
+    d_sb = step(std_band)
+    barrier()
+    ev0.record(stream)
+    for _ in range(n_plain):
+        d_sb = step(std_band)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    std_band_ms = max_over_ranks(ev0.elapsed_time(ev1) / n_plain)
+    x_std_band = x.clone()
 
     # --- the FP32-refinement path without the learned guess, for comparison
     for _ in range(2):
@@ -372,6 +389,7 @@ def run_ours(args):
     ev1.record(stream)
     torch.cuda.synchronize()
     f32_ms = max_over_ranks(ev0.elapsed_time(ev1) / n_f)
+    x_f32 = x.clone()
 
     # --- the same with A given expanded (its 9 values repeated at the 8 Gauss points, the form
     # escript's general assembler reads): the assembly reads 1.2 GB of A instead of 151 MB
@@ -396,7 +414,7 @@ def run_ours(args):
     ev1.record(stream)
     torch.cuda.synchronize()
     f32x_ms = max_over_ranks(ev0.elapsed_time(ev1) / n_f)
-    del A_x
+    A_x_host = A_x.cpu().pin_memory()
 
     # --- warm-up of the timed path
     for _ in range(args.warmup):
@@ -486,18 +504,73 @@ def run_ours(args):
     torch.cuda.synchronize()
     e2e_ms = max_over_ranks(ev0.elapsed_time(ev1) / args.steps)
 
+    # --- the same end to end with A handed over the way escript's LinearPDE does when kappa
+    # lives on Function: expanded to the 8 Gauss points (72 doubles per element, 1.2 GB at
+    # 128^3), copied from pinned host memory every step; the learned path reads kappa from it
+    def step_expanded_e2e():
+        A_x.copy_(A_x_host, non_blocking=True)
+        Y_e.copy_(Y_host, non_blocking=True)
+        q_e.copy_(q_host, non_blocking=True)
+        cax = L.rg_coef(A_x.data_ptr(), L.RG_COEF_EXPANDED)
+        if timed is learned:
+            side.wait_stream(stream)
+            with torch.cuda.stream(side):
+                L.set_stream_from_torch()
+                L.check(lib.rg_ws_element_fields(C.c_void_p(A_x.data_ptr()), 72, C.c_void_p(Y_e.data_ptr()), 8,
+                                                 nel, C.c_void_p(kap32.data_ptr()), C.c_void_p(y32.data_ptr())))
+                warm.guess(kap32, y32, (ne, ne, ne), q=q_e, out=guess)
+            L.set_stream_from_torch()
+        L.check(lib.rg_matrix_reset(mat))
+        rhs.zero_()
+        L.check(lib.rg_assemble_single(mat, C.c_void_p(rhs.data_ptr()), C.byref(cax), C.byref(empty),
+                                       C.byref(empty), C.byref(empty), C.byref(empty),
+                                       C.byref(L.rg_coef(Y_e.data_ptr(), L.RG_COEF_EXPANDED))))
+        L.check(lib.rg_insert_constraint(mat, C.c_void_p(rhs.data_ptr()), C.c_void_p(q_e.data_ptr()), None, 0))
+        if timed is learned:
+            stream.wait_stream(side)
+        d = L.rg_diag()
+        L.check(lib.rg_solve(mat, C.c_void_p(rhs.data_ptr()), C.c_void_p(x.data_ptr()), C.byref(timed), C.byref(d)))
+        x_host.copy_(x, non_blocking=True)
+        return d
+
+    step_expanded_e2e()
+    barrier()
+    n_x = max(2, min(args.steps, 3))
+    ev0.record(stream)
+    for _ in range(n_x):
+        step_expanded_e2e()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    e2e_x_ms = max_over_ranks(ev0.elapsed_time(ev1) / n_x)
+    bi_x = A_x_host.numel() * 8 + Y_host.numel() * 8 + q_host.numel() * 8
+    del A_x, A_x_host
+
     # --- CPU baseline (rank 0, one GPU): the reference's own code on a bounded sample
     cpu = None
+    errors = None
     if rank == 0 and world == 1 and not args.no_cpu:
         threads = os.cpu_count() or 1
-        s = cpu_reference_sample(inp, plain_iters, threads)
+        oracle_rtol = min(1e-10, rtol / 100)
+        s = cpu_reference_solve(inp, threads, rtol=rtol, oracle_rtol=oracle_rtol)
         cpu = {"value": round(s["time_to_solution_s"] * 1e3, 1), "unit": "ms", "cores": threads,
                "kind": s["kind"],
-               "sample": (f"reference DefaultAssembler3D + insertConstraint on the full {ne}^3 input, "
-                          f"paso Solver/PCG run for 10 and 40 iterations; time-to-solution = "
-                          f"assemble + constrain + setup + {plain_iters} (GPU paso iteration count) "
-                          f"x {s['per_iter_s'] * 1e3:.2f} ms/iteration"),
-               "assemble_s": round(s["assemble_s"], 3), "per_iter_ms": round(s["per_iter_s"] * 1e3, 3)}
+               "sample": (f"one complete time-to-solution of the reference on the full {ne}^3 input: its "
+                          f"DefaultAssembler3D (A on the Gauss points) + insertConstraint + paso Solver/PCG "
+                          f"to rtol {rtol:g} ({s['iterations']} iterations)"),
+               "assemble_s": round(s["assemble_s"], 3), "constraint_s": round(s["constraint_s"], 3),
+               "solve_s": round(s["solve_s"], 3), "iterations": s["iterations"]}
+        xo = s["x_oracle"]
+        nrm = float(np.linalg.norm(xo))
+
+        def err_of(v):
+            return float(np.linalg.norm(v.cpu().numpy() - xo) / nrm)
+
+        errors = {"oracle": (f"{s['kind']} paso Solver/PCG in FP64 on the host, rtol {oracle_rtol:g} "
+                             f"({s['oracle_iterations']} iterations)"),
+                  "timed_path": err_of(x_fast), "fp32_refine_no_guess": err_of(x_f32),
+                  "plain_fp64_paso_csr": err_of(x_plain), "plain_fp64_paso_band": err_of(x_plain_band),
+                  "fp64_standard_band": err_of(x_std_band),
+                  "reference_at_rtol": float(np.linalg.norm(s["x"] - xo) / nrm)}
 
     kernels = {k: {"launches_per_step": v[0] // n_prof, "ms_per_step": round(v[2] / n_prof, 3)}
                for k, v in tm.items() if v[0]}
@@ -554,13 +627,19 @@ def run_ours(args):
         "iterations": int(d_fast.num_iter), "outer_steps": int(d_fast.num_outer),
         "rel_residual": float(d_fast.residual_norm / d_fast.rhs_norm),
         "error_vs_fp64": err,
+        "error_vs_oracle": errors["timed_path"] if errors else None,
+        "errors_vs_oracle": errors,
         "plain_fp64": {"ms": round(plain_ms, 3), "iterations": plain_iters,
                        "algorithm": "paso PCG with residual smoothing, balanced CSR FP64",
                        "band_layout_ms": round(plain_band_ms, 3),
-                       "band_layout_iterations": int(d_pb.num_iter)},
-        "speedup_vs_plain_fp64": round(plain_ms / ms, 3),
+                       "band_layout_iterations": int(d_pb.num_iter),
+                       "standard_band_ms": round(std_band_ms, 3),
+                       "standard_band_iterations": int(d_sb.num_iter),
+                       "fastest_ms": round(min(plain_ms, plain_band_ms, std_band_ms), 3)},
+        "speedup_vs_plain_fp64": round(min(plain_ms, plain_band_ms, std_band_ms) / ms, 3),
+        "speedup_vs_paso_csr": round(plain_ms / ms, 3),
         "fp32_refine_no_guess": {"ms": round(f32_ms, 3), "iterations": int(d_f32.num_iter),
-                                 "speedup_vs_plain_fp64": round(plain_ms / f32_ms, 3),
+                                 "speedup_vs_plain_fp64": round(min(plain_ms, plain_band_ms, std_band_ms) / f32_ms, 3),
                                  "with_A_expanded_ms": round(f32x_ms, 3),
                                  "with_A_expanded_iterations": int(d_fx.num_iter)},
         "learned_guess": ({"rejected": bool(d_fast.guess_rejected),
@@ -572,6 +651,9 @@ def run_ours(args):
         "std_fp64_iterations": int(d_std.num_iter),
         "roofline": roofline, "cpu_baseline": cpu,
         "e2e": {"value": round(e2e_ms, 3), "unit": "ms", "h2d_bytes_per_step": bi, "d2h_bytes_per_step": bo},
+        "e2e_A_expanded": {"value": round(e2e_x_ms, 3), "unit": "ms", "h2d_bytes_per_step": bi_x,
+                           "d2h_bytes_per_step": bo,
+                           "note": "A as escript hands it for kappa on Function: 72 doubles per element"},
         "gpu_launches": launches, "clocks": clk, "kernels": kernels,
         "batched": batched,
     }
@@ -589,36 +671,43 @@ def run_ours(args):
 # ----------------------------------------------------------------------------------------------
 
 def run_reference(args):
+    """The reference's own CPU implementation of the path on the host cores: every timed step
+    is one complete time-to-solution of the same workload (DefaultAssembler3D with A on the
+    Gauss points, insertConstraint, paso Solver/PCG to rtol), the reference's sources
+    compiled in place (oracle/_ref).  Warm-up steps are bounded (assembly, constraint and
+    10 paso iterations).  Under torchrun only rank 0 works."""
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     if rank != 0:
         return
-    from oracle import oracle as O
     threads = os.cpu_count() or 1
     inp = make_inputs(args.ne, args.seed, 8.0 * args.ne / 128.0)
-    # warm-up 1: one complete solve gives paso's iteration count for the extrapolation
-    n_iter, full_s = cpu_full_reference_iterations(inp, threads)
-    for _ in range(max(args.warmup - 1, 0)):
-        cpu_reference_sample(inp, n_iter, threads)
-    vals = []
+    for _ in range(args.warmup):
+        cpu_reference_warmup(inp, threads)
+    vals, iters, kind = [], [], None
+    t_run = time.perf_counter()
     for _ in range(args.steps):
-        s = cpu_reference_sample(inp, n_iter, threads)
+        s = cpu_reference_solve(inp, threads, rtol=args.rtol)
         vals.append(s["time_to_solution_s"] * 1e3)
+        iters.append(s["iterations"])
+        kind = s["kind"]
+    run_s = time.perf_counter() - t_run
     v = statistics.mean(vals)
-    kind = "reference" if O.have_ref() else "port"
     out = {
         "impl": "reference", "metric": METRIC, "value": round(v, 1), "unit": "ms", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(v, 1), "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic, seeded: kappa=exp(GRF corr 8 cells, std 1), 4 Gaussian blobs",
         "config": {"workload": f"Brick {args.ne}^3 variable-coefficient Poisson, u=0 on top face, "
-                               f"PCG+Jacobi rtol {RTOL:g} (assemble+constrain+solve per step)",
-                   "ne": [args.ne] * 3, "seed": args.seed, "full_solve_s": round(full_s, 2),
-                   "iterations": n_iter},
+                               f"PCG+Jacobi rtol {args.rtol:g} (assemble+constrain+solve per step)",
+                   "ne": [args.ne] * 3, "seed": args.seed, "iterations": iters[0],
+                   "step_ms": {"min": round(min(vals), 1), "max": round(max(vals), 1)},
+                   "timed_steps_wall_s": round(run_s, 2)},
         "cpu_baseline": {"value": round(v, 1), "unit": "ms", "cores": threads, "kind": kind,
-                         "sample": ("reference DefaultAssembler3D + insertConstraint on the full input, "
-                                    f"paso Solver/PCG for 10 and 40 iterations, extrapolated to the "
-                                    f"{n_iter} iterations of one full reference solve (warm-up)")},
+                         "sample": ("every step one complete time-to-solution on the full input: the reference's "
+                                    "DefaultAssembler3D (A on the Gauss points) + insertConstraint + paso "
+                                    f"Solver/PCG to rtol {args.rtol:g}; warm-up steps: assembly, constraint "
+                                    "and 10 iterations")},
         "e2e": {"value": round(v, 1), "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(out), flush=True)

@@ -4,6 +4,7 @@
 // head, bias gradients, the mean-squared-error loss, the Adam update with bf16 weight
 // refresh (forward and flipped/transposed data-gradient layouts), and the packing of
 // (log kappa, Y) into the network input.  Activations use the layout of rg_act.
+#include <algorithm>
 #include <cuda_bf16.h>
 
 #include "rg_internal.cuh"
@@ -295,6 +296,20 @@ __global__ void k_weights_bf16(const float* __restrict__ w, __nv_bfloat16* __res
 // u / u_unit (the solution scales with Y h^2 / kappa).  Fields are fp32 per element of the
 // fine grid (fd, fh, fw), x fastest.
 constexpr int kStatBlocks = 64;
+
+// the network's per-element inputs from the PDE's coefficient arrays: kappa_e = A's first
+// entry of element e (a_stride doubles per element: 9 for A per element, 72 for A expanded
+// to the Gauss points, whose first point is read), y_e = mean of Y's y_points values
+__global__ void k_element_fields(const double* __restrict__ A, int a_stride, const double* __restrict__ Y,
+                                 int y_points, size_t nel, float* __restrict__ kappa, float* __restrict__ y)
+{
+    for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < nel; e += (size_t)gridDim.x * blockDim.x) {
+        kappa[e] = (float)__ldcs(A + e * a_stride);
+        double s = 0.0;
+        for (int q = 0; q < y_points; ++q) s += __ldcs(Y + e * y_points + q);
+        y[e] = (float)(s / y_points);
+    }
+}
 
 __global__ void k_field_stats(const float* __restrict__ kappa, const float* __restrict__ y, size_t per_sample,
                               double* __restrict__ part)
@@ -601,6 +616,17 @@ int rg_ws_field_stats(const float* kappa, const float* y, int nsamples, int64_t 
     RG_CHECK_LAUNCH();
     RG_TIMED(T_WS_OPS, (k_field_stats_finish<<<(nsamples + 63) / 64, 64, 0, stream()>>>(work, kStatBlocks, (size_t)per_sample, nsamples,
                                                                      h_net, stats)));
+    RG_CHECK_LAUNCH();
+    return RG_OK;
+}
+
+int rg_ws_element_fields(const double* A, int a_stride, const double* Y, int y_points, int64_t nel, float* kappa,
+                         float* y)
+{
+    RG_REQUIRE(A && Y && kappa && y && a_stride >= 1 && y_points >= 1 && nel > 0,
+               "rg_ws_element_fields: invalid argument");
+    const int grid = (int)std::min<int64_t>((nel + 255) / 256, 148 * 8);
+    RG_TIMED(T_WS_OPS, (k_element_fields<<<grid, 256, 0, stream()>>>(A, a_stride, Y, y_points, (size_t)nel, kappa, y)));
     RG_CHECK_LAUNCH();
     return RG_OK;
 }
