@@ -185,10 +185,11 @@ def cpu_reference_warmup(inp, threads):
 # our arm
 # ----------------------------------------------------------------------------------------------
 
-# algorithmic bytes per launch of the dominant kernel, per DOF (n): the FP32 band SpMV reads
-# 27 band values (4 B each, padded bands count) + z and p_old, writes p_new and q, and adds
-# the previous iteration's alpha p_old to the correction d (read + write)
-F32_SPMV_BYTES_PER_ROW = 27 * 4 + 6 * 4
+# algorithmic bytes per launch of the dominant kernel, per DOF (n): one fused FP32 PCG
+# iteration reads the row's 27 band values (4 B each, padded bands count) and its 16-byte
+# iteration state {u, D^-1 A u, D^-1 A p, p}, writes the new state, and updates the
+# correction d (read + write)
+F32_SPMV_BYTES_PER_ROW = 27 * 4 + 16 + 16 + 8
 
 
 def max_over_ranks_of(v, dist=None, device="cpu"):
@@ -475,7 +476,7 @@ def run_ours(args):
         tr = json.load(open(tr_path)).get("f32_spmv")
         if tr and tr.get("ne") == ne:
             traffic = tr.get("bytes_per_launch")
-    roofline = {"bound": "hbm", "kernel": "k_f32_spmv_tma<27> (FP32 27-band SpMV + p.q, TMA-pipelined)",
+    roofline = {"bound": "hbm", "kernel": "k_f32_cg<27> (one fused FP32 PCG iteration: 27-band SpMV, vector updates, one reduction)",
                 "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
                 "frac": round(achieved / hbm, 4), "peak_source": peak_note,
                 "algorithmic_bytes_per_launch": algo_bytes, "avg_launch_us": round(avg_s * 1e6, 2),
@@ -577,7 +578,7 @@ def run_ours(args):
     cfg, ug = C.c_int(), C.c_int()
     spmv_us = (C.c_double * 2)()
     lib.rg_solver_config(mat, C.byref(cfg), C.byref(ug), spmv_us)
-    spmv_names = {0: "k_f32_spmv_tma<27, 3 stages>", 1: "k_f32_spmv_tma<27, 2 stages x 2 CTAs/SM>"}
+    spmv_names = {0: "k_f32_cg<27, 3 stages x 1 CTA/SM>", 1: "k_f32_cg<27, 2 stages x 2 CTAs/SM>"}
     roofline["kernel"] = spmv_names.get(cfg.value, roofline["kernel"])
     roofline["tuned"] = {"spmv_config": cfg.value, "update_grid": ug.value,
                          "spmv_us_per_config": [round(v, 2) for v in spmv_us]}

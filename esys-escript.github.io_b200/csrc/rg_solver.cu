@@ -10,8 +10,10 @@
 //    recursive FP32 residual has dropped by `inner_tolerance` the true residual is
 //    recomputed in FP64 on the CSR values, tested with paso's dual-norm criterion and
 //    written back into the FP32 recurrence (the Krylov direction is kept, no restart).
+//    One FP32 iteration is one kernel (k_f32_cg, the one-reduction recurrence of
+//    Chronopoulos and Gear).
 //
-// One PCG iteration is three kernels: a pure SpMV of the search direction with its
+// One FP64 PCG iteration is three kernels: a pure SpMV of the search direction with its
 // p.q reduction, an elementwise update with the iteration's reductions, and an
 // elementwise kernel that forms the next search direction (in paso mode it also does
 // the smoothing step).  Scalars (alpha, beta, tau, ...) live in device memory: the last
@@ -49,7 +51,6 @@ struct Scal {
     double best;               // FP32 path: smallest recursive residual norm of the segment
     int since;                 // iterations since `best` last dropped by 5%
     int done, status;
-    int dpend;                 // FP32 path: alpha p of the last SpMV is not yet added to d
 };
 
 enum { ST_RUN = 0, ST_CONV = 1, ST_MAXIT = 3, ST_BREAK = 4 };
@@ -61,8 +62,8 @@ struct Workspace {
     double *r = nullptr, *x = nullptr, *rs = nullptr, *x2 = nullptr, *q = nullptr, *z = nullptr;
     double* p = nullptr;
     double* bb = nullptr;  // balanced rhs
-    float *r32 = nullptr, *d32 = nullptr, *q32 = nullptr, *z32 = nullptr;
-    float* p32[2] = {nullptr, nullptr};
+    float* d32 = nullptr;                // FP32 path: correction accumulated over a segment
+    float4* v4[2] = {nullptr, nullptr};  // FP32 iteration state {u, D^-1 A u, D^-1 A p_prev, p_prev}
     double* partials = nullptr;
     unsigned* counter = nullptr;
     Scal* s = nullptr;   // device scalars
@@ -83,8 +84,8 @@ struct Workspace {
     int sweeps = 1;  // Jacobi sweeps of the current paso solve (Smoother.cpp:100-128)
     bool band64 = false;              // paso FP64 SpMV on the FP64 band copy (RG_LAYOUT_BAND)
     bool graph_band64[3] = {false, false, false};
-    int spmv_cfg = -1;   // FP32 band SpMV pipeline: 0 = 3 stages x 1 CTA/SM, 1 = 2 stages x 2 CTAs/SM
-    int grid_upd32 = 0;  // CTAs of k_f32_update (tuned with the SpMV; 0 = grid_vec)
+    int spmv_cfg = -1;   // FP32 iteration pipeline: 0 = 3 stages x 1 CTA/SM, 1 = 2 stages x 2 CTAs/SM
+    int grid_upd32 = 0;  // kept for rg_solver_config: the FP32 iteration has no separate update kernel
     double spmv_us[2] = {0, 0};  // tuner's time per launch of each SpMV configuration
 };
 
@@ -134,11 +135,9 @@ int ensure_workspace(Matrix* m, bool fp32)
         RG_CHECK_CUDA(cudaMemsetAsync(w->counter, 0, sizeof(unsigned), stream()));
     }
     Workspace* w = m->ws;
-    if (fp32 && !w->r32) {
+    if (fp32 && !w->d32) {
         int rc;
-        if ((rc = dalloc(&w->r32, n)) || (rc = dalloc(&w->d32, n)) || (rc = dalloc(&w->q32, n)) ||
-            (rc = dalloc(&w->z32, n)) || (rc = dalloc(&w->p32[0], n)) || (rc = dalloc(&w->p32[1], n)))
-            return rc;
+        if ((rc = dalloc(&w->d32, n)) || (rc = dalloc(&w->v4[0], n)) || (rc = dalloc(&w->v4[1], n))) return rc;
     }
     return RG_OK;
 }
@@ -638,15 +637,8 @@ __global__ void __launch_bounds__(kThreads) k_std_pupdate(int64_t n, const doubl
 // Tile-major band layout: rows are grouped in tiles of kTile; tile T's coefficients are
 // band[(T*NB + b)*kTile + t] for row T*kTile + t and band b (neighbour i + off_b; 0 where
 // there is none, and in padding rows), so one tile's whole matrix slice is one contiguous
-// NB*kTile*4-byte block.
-//
-// Iteration (two kernels): the SpMV kernel forms the search direction p = z + beta p_old
-// (beta = 0 on a fresh start) from staged windows of z and p_old, writes p to the other
-// buffer, and computes q = A p and p.q; the update kernel does d += alpha p, r -= alpha q,
-// z = dinv r and the FP64 reductions r.z and r.r.  p alternates between two buffers by
-// the parity counter s->pk.
+// NB*kTile*4-byte block.  One FP32 PCG iteration is one kernel (k_f32_cg below).
 constexpr int kTile = 256;
-constexpr int kPWin = kTile + 8;
 constexpr int kConsumerWarps = kTile / 32;
 enum { ST_TIMEOUT = 6 };
 
@@ -702,194 +694,8 @@ __global__ void __launch_bounds__(kThreads) k_cheb_step_band(const __grid_consta
     }
 }
 
-// r32 = r64 * inv_scale, z = dinv r, rho = r.z, ||r||.  fresh: d = 0, p_old = 0, beta = 0,
-// pk = 0 (a new recurrence).  Otherwise (residual replacement) the direction continues:
-// beta is rescaled to the replaced rho.
-__global__ void __launch_bounds__(kThreads) k_f32_init(int64_t n, const double* __restrict__ r64,
-                                                       const float* __restrict__ dinv32,
-                                                       float* __restrict__ r32, float* __restrict__ z32,
-                                                       float* __restrict__ p0, float* __restrict__ d32,
-                                                       int fresh, ReduceBuf rb, Scal* s, double inv_scale)
-{
-    double v[2] = {0.0, 0.0};
-    for (int64_t i = gtid(); i < n; i += gstride()) {
-        const float ri = (float)(r64[i] * inv_scale);
-        r32[i] = ri;
-        const float zi = ri * dinv32[i];
-        z32[i] = zi;
-        if (fresh) {
-            p0[i] = 0.f;
-            d32[i] = 0.f;
-        }
-        v[0] += (double)zi * (double)ri;
-        v[1] += (double)ri * (double)ri;
-    }
-    double t[2];
-    if (grid_reduce<2>(v, rb, t) && threadIdx.x == 0) {
-        if (fresh) {
-            s->beta = 0.0;
-            s->pk = 0;
-        } else {
-            s->beta = s->rho > 0 ? s->beta * (t[0] / s->rho) : 0.0;
-        }
-        s->rho = t[0];
-        s->norm = sqrt(t[1]);
-        s->dpend = 0;
-    }
-}
-
-// Warp-specialised, persistent (one CTA per SM): warp kConsumerWarps is the producer, its
-// lane 0 streams, per tile, the tile's band block (one bulk copy, L2 evict-first) and, for
-// interior tiles, the 2*NG windows of z and p_old its stencil columns span (kTile+8 values
-// from a 16-byte aligned start) into a kStages ring; consumer warps compute one row per
-// thread from shared memory and release the stage through an `empty` mbarrier.  Tiles near
-// the two ends read z and p_old with clamped loads.  All waits are bounded: on timeout the
-// kernel records ST_TIMEOUT and returns.
-template <int NB, int kStages>
-__global__ void __launch_bounds__(kTile + 32, 1) k_f32_spmv_tma(const float* __restrict__ band,
-                                                                const __grid_constant__ TmaBandArgs ta,
-                                                                const float* __restrict__ z,
-                                                                float* __restrict__ P0, float* __restrict__ P1,
-                                                                float* __restrict__ q, float* __restrict__ d,
-                                                                ReduceBuf rb, Scal* s)
-{
-    constexpr int NG = NB / 3;
-    constexpr int kBand = NB * kTile;
-    constexpr int kWin = NG * kPWin;
-    constexpr int kStage = kBand + 2 * kWin;
-    extern __shared__ __align__(128) float smem[];
-    __shared__ __align__(8) uint64_t full[kStages], empty[kStages];
-    __shared__ int bad;
-    if (s->done) return;
-    const float beta = (float)s->beta;
-    // the previous iteration's d += alpha p, deferred from k_f32_update to here, where
-    // p_old is already in shared memory
-    const float alpha_prev = (float)s->alpha;
-    const bool dpend = s->dpend != 0;
-    const float* __restrict__ pold = (s->pk & 1) ? P1 : P0;
-    float* __restrict__ pnew = (s->pk & 1) ? P0 : P1;
-    const int t = threadIdx.x;
-    const int warp = t >> 5;
-    const int64_t n = ta.n;
-    const int64_t ntiles = (n + kTile - 1) / kTile;
-    const int64_t my_tiles = blockIdx.x < ntiles ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
-    if (t == 0) {
-        for (int k = 0; k < kStages; ++k) {
-            mbar_init(&full[k], 1);
-            mbar_init(&empty[k], kConsumerWarps);
-        }
-        bad = 0;
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    __syncthreads();
-    auto interior = [&](int64_t i0) { return i0 - ta.halo - 8 >= 0 && i0 + kTile + ta.halo + 8 <= n; };
-
-    double v[1] = {0.0};
-    int64_t issued = 0;
-    const WaitCtl wc = g_wait_ctl;
-    const int polls = wc.polls > 0 ? wc.polls : kDefaultPolls;
-    if (warp == kConsumerWarps) {
-        // ---------------- producer
-        if ((t & 31) == 0 && !wc.withhold) {
-            const uint64_t pol = evict_first_policy();
-            for (int64_t k = 0; k < my_tiles; ++k, issued = k) {
-                const int st = (int)(k % kStages);
-                if (k >= kStages && !mbar_wait(&empty[st], (uint32_t)(((k / kStages) - 1) & 1), polls)) {
-                    bad = 1;
-                    break;
-                }
-                const int64_t tile = blockIdx.x + k * gridDim.x;
-                const int64_t i0 = tile * kTile;
-                float* dst = smem + (size_t)st * kStage;
-                const bool in = interior(i0);
-                mbar_expect_tx(&full[st], kBand * 4 + (in ? 2 * kWin * 4 : 0));
-                bulk_g2s_hint(dst, band + (size_t)tile * kBand, kBand * 4, &full[st], pol);
-                if (in)
-                    for (int g = 0; g < NG; ++g) {
-                        const int64_t a = (i0 + ta.goff[g]) & ~(int64_t)3;
-                        bulk_g2s(dst + kBand + g * kPWin, z + a, kPWin * 4, &full[st]);
-                        bulk_g2s(dst + kBand + kWin + g * kPWin, pold + a, kPWin * 4, &full[st]);
-                    }
-            }
-        }
-    } else {
-        // ---------------- consumers: row i0 + t of every tile
-        for (int64_t k = 0; k < my_tiles; ++k) {
-            const int st = (int)(k % kStages);
-            if (!mbar_wait(&full[st], (uint32_t)((k / kStages) & 1), polls)) {
-                bad = 1;
-                break;
-            }
-            const float* bs = smem + (size_t)st * kStage;
-            const int64_t i0 = (blockIdx.x + k * gridDim.x) * (int64_t)kTile;
-            const int64_t i = i0 + t;
-            float acc = 0.f, pi = 0.f, po = 0.f;
-            if (interior(i0)) {
-                const float* zw = bs + kBand;
-                const float* pw = bs + kBand + kWin;
-#pragma unroll
-                for (int g = 0; g < NG; ++g) {
-                    const int base = (int)((i0 + ta.goff[g]) & 3) + t + g * kPWin;
-#pragma unroll
-                    for (int m = 0; m < 3; ++m) {
-                        const float pj = fmaf(beta, pw[base + m], zw[base + m]);
-                        acc = fmaf(bs[(3 * g + m) * kTile + t], pj, acc);
-                        if (3 * g + m == NB / 2) {
-                            pi = pj;
-                            po = pw[base + m];
-                        }
-                    }
-                }
-            } else {
-#pragma unroll
-                for (int b = 0; b < NB; ++b) {
-                    const int64_t j = min(max(i + ta.off[b], (int64_t)0), n - 1);
-                    const float pj = fmaf(beta, __ldg(pold + j), __ldg(z + j));
-                    acc = fmaf(bs[b * kTile + t], pj, acc);
-                    if (b == NB / 2) {
-                        pi = pj;
-                        po = __ldg(pold + j);
-                    }
-                }
-            }
-            __syncwarp();
-            if ((t & 31) == 0) mbar_arrive(&empty[st]);
-            if (i < n) {
-                pnew[i] = pi;
-                q[i] = acc;
-                if (dpend) d[i] = fmaf(alpha_prev, po, d[i]);
-                v[0] += (double)acc * (double)pi;
-            }
-        }
-    }
-    __syncthreads();
-    if (bad) {
-        // let the copies this CTA issued land (bounded) before its shared memory is released
-        if (warp == kConsumerWarps && (t & 31) == 0)
-            for (int64_t k = issued > kStages ? issued - kStages : 0; k < issued; ++k)
-                for (int tries = 0; tries < (1 << 20) && !mbar_try_wait(&full[k % kStages], (uint32_t)((k / kStages) & 1));
-                     ++tries) {
-                }
-        if (t == 0) report_status(s, ST_TIMEOUT);
-        // the CTA still takes its turn in the grid reduction (with nothing to add), so the
-        // reduction counter ends the launch at zero for the kernels that follow
-        v[0] = 0.0;
-    }
-    double tt[1];
-    if (grid_reduce<1>(v, rb, tt) && threadIdx.x == 0) {
-        s->delta = tt[0];
-        s->alpha = s->rho / tt[0];
-        s->dpend = 1;  // d += alpha p happens in the next SpMV or in k_add_correction
-        if (!(fabs(tt[0]) > 0.0)) {
-            s->iter += 1;
-            report_status(s, ST_BREAK);
-            s->dpend = 0;
-        }
-    }
-}
-
 // The FP64 band kernels of the paso PCG (RG_LAYOUT_BAND), warp-specialised and persistent
-// like k_f32_spmv_tma: lane 0 of warp kConsumerWarps streams, per tile, the tile's FP64 band
+// like k_f32_cg: lane 0 of warp kConsumerWarps streams, per tile, the tile's FP64 band
 // block (one bulk copy, L2 evict-first) and, for interior tiles, the NG windows of x its
 // stencil columns span (kTile+4 values from a 16-byte aligned start) into a kStages ring;
 // consumer warps compute row i0 + t from shared memory.  Tiles near the two ends read x with
@@ -1059,91 +865,284 @@ __global__ void __launch_bounds__(kTile + 32, 1) k_band64_bulk(const double* __r
 template <int NB>
 constexpr int band64_stages() { return NB == 27 ? 3 : 8; }
 
-// r -= alpha q; z = dinv r; rho_next = r.z and ||r||^2 in FP64; tests; beta.  (d += alpha p
-// of this iteration is done by the next SpMV, or by k_add_correction at the segment's end.)
-__global__ void __launch_bounds__(kThreads) k_f32_update(int64_t n, float* __restrict__ r,
-                                                         const float* __restrict__ q,
-                                                         const float* __restrict__ dinv,
-                                                         float* __restrict__ z, ReduceBuf rb, Scal* s)
+// ------------------------------------------------------------------ FP32 PCG, one kernel per iteration
+// Jacobi-PCG in the one-reduction form of Chronopoulos and Gear ("s-step iterative methods
+// for symmetric linear systems", J. Comput. Appl. Math. 25, 1989): besides the search
+// direction p the recurrences carry s = A p and w = A u (u = D^-1 r, the preconditioned
+// residual), so that the SpMV of an iteration is applied to u_{i+1}, which every tile can
+// form itself from the previous vectors:
+//     p_i = u_i + b_i p_{i-1}          s_i = w_i + b_i s_{i-1}          d += a_i p_i
+//     u_{i+1} = u_i - a_i D^-1 s_i     w_{i+1} = A u_{i+1}
+// and all scalars of the next iteration come from ONE grid reduction over the rows:
+//     g = r.u = sum diag u^2,  |r|^2 = sum (diag u)^2,  u.w,  u.s,  p.w,  p.s
+//     b_{i+1} = g_{i+1} / g_i,
+//     a_{i+1} = g_{i+1} / (p_{i+1}.A p_{i+1})  with  p_{i+1}.s_{i+1} = u.w + b (u.s + p.w) + b^2 p.s
+// (the expansion of p.Ap gives the step length from the stored vectors instead of the
+// orthogonality relations of the original recurrence for a).  D^-1 s and D^-1 w are stored,
+// so that u_{i+1} at a neighbour needs no diagonal there; the diagonal comes from the band.
+// (The pipelined variant of Ghysels and Vanroose, whose SpMV input is complete before the
+// iteration, was measured too: its auxiliary recurrences drift too far in FP32 for the FP64
+// refinement, which then stalls.)
+//
+// Per row the vector state is one float4 {u, D^-1 w, D^-1 s_prev, p_prev}, double-buffered
+// by the parity counter s->pk: every tile reads the previous state in the windows its stencil
+// spans (one window per stencil plane when its rows overlap, i.e. x-lines shorter than about
+// a tile, else one per stencil column), bulk-copied into shared memory with the tile's band
+// block by a producer warp (one bulk copy each, the band with an L2 evict-first policy), and
+// writes its own rows' new state.  All waits are bounded.  A
+// consumer thread forms u_{i+1} once per stencil column, at its own dx = 0 position, and takes
+// the dx = -1 / +1 values from the neighbouring lanes (warp shuffles; lanes 0 and 31 form their
+// outer neighbour themselves): 9 state loads per row instead of 27.  Per row the kernel moves
+// the 108 band bytes, 16 bytes of state in and out and the correction d (8 bytes): 148 B, in
+// one launch with one reduction.
+//
+// mode 0: iteration.  mode 1/2: start of a segment (fresh / continuing direction): u was just
+// seeded from the FP64 residual; both A u and A p_prev are formed from the windows (no
+// recurrence), d is not touched, and the reduction sets the first a, b (b = 0 when fresh;
+// when continuing, b divides by r.u of the residual the kept direction came from).
+constexpr int kMaxWin = 9;
+
+struct CgArgs {
+    int bpos[27];          // shared-memory float4 index of band b's neighbour for consumer row 0
+    int off[27];           // column offset of band b
+    int woff[kMaxWin];     // row offset of window w's first row relative to the tile's first row
+    int nwin, wlen;        // windows per tile and rows per window
+    int64_t n;
+    int64_t lo, hi;        // a tile is interior when i0 + lo >= 0 and i0 + hi <= n
+};
+
+// u_{i+1} at a neighbour from its state: u - a (D^-1 w + b D^-1 s_prev)
+__device__ __forceinline__ float next_u(float4 v, float alpha, float beta)
 {
-    if (s->done) return;
-    const float alpha = (float)s->alpha;
-    double v[2] = {0.0, 0.0};
-    const int64_t nv = n >> 2;
-    auto body = [&](int64_t k, float4 r0, float4 q0, float4 di) {
-        const float4 rn = make_float4(fmaf(-alpha, q0.x, r0.x), fmaf(-alpha, q0.y, r0.y),
-                                      fmaf(-alpha, q0.z, r0.z), fmaf(-alpha, q0.w, r0.w));
-        st4(r, k, rn);
-        const float4 zn = make_float4(rn.x * di.x, rn.y * di.y, rn.z * di.z, rn.w * di.w);
-        st4(z, k, zn);
-        v[0] += (double)zn.x * rn.x + (double)zn.y * rn.y + (double)zn.z * rn.z + (double)zn.w * rn.w;
-        v[1] += (double)rn.x * rn.x + (double)rn.y * rn.y + (double)rn.z * rn.z + (double)rn.w * rn.w;
-    };
-    // two float4 groups per trip with all six loads issued first: the kernel is bound by load
-    // latency rather than bandwidth
-    const int64_t st = gstride();
-    int64_t k = gtid();
-    for (; k + st < nv; k += 2 * st) {
-        const int64_t k2 = k + st;
-        const float4 r0 = ld4(r, k), q0 = ld4(q, k), di0 = ld4(dinv, k);
-        const float4 r1 = ld4(r, k2), q1 = ld4(q, k2), di1 = ld4(dinv, k2);
-        body(k, r0, q0, di0);
-        body(k2, r1, q1, di1);
-    }
-    if (k < nv) body(k, ld4(r, k), ld4(q, k), ld4(dinv, k));
-    if (gtid() < (n & 3)) {
-        const int64_t i = (nv << 2) + gtid();
-        const float ri = fmaf(-alpha, q[i], r[i]);
-        r[i] = ri;
-        const float zi = ri * dinv[i];
-        z[i] = zi;
-        v[0] += (double)zi * ri;
-        v[1] += (double)ri * ri;
-    }
-    double t[2];
-    if (grid_reduce<2>(v, rb, t) && threadIdx.x == 0) {
-        const long long it = s->iter + 1;
-        s->iter = it;
-        s->pk += 1;
-        const double norm = sqrt(t[1]);
-        s->norm = norm;
-        s->beta = t[0] / s->rho;
-        const bool brk = !(fabs(t[0]) > 0.0);
-        s->rho = t[0];
-        // the FP32 recurrence has stagnated when no new minimum (5% below the best)
-        // appeared for 200 iterations: end the segment so that the FP64 residual is
-        // recomputed and fed back
-        if (norm < 0.95 * s->best) {
-            s->best = norm;
-            s->since = 0;
-        } else {
-            s->since += 1;
+    return fmaf(-alpha, fmaf(beta, v.z, v.y), v.x);
+}
+
+template <int NB, int kStages, int kCtas>
+__global__ void __launch_bounds__(kTile + 32, kCtas) k_f32_cg(const float* __restrict__ band,
+                                                              const __grid_constant__ CgArgs ca,
+                                                              const float4* V0, const float4* V1,
+                                                              float4* W0, float4* W1,
+                                                              float* __restrict__ d, ReduceBuf rb, Scal* s, int mode)
+{
+    constexpr int kBand = NB * kTile;
+    constexpr int kCenter = NB / 2;
+    constexpr int NG = NB / 3;
+    extern __shared__ __align__(128) float smem[];
+    __shared__ __align__(8) uint64_t full[kStages], empty[kStages];
+    __shared__ int bad;
+    if (mode == 0 && s->done) return;
+    const float alpha = mode == 0 ? (float)s->alpha : 0.f;
+    const float beta = mode == 0 ? (float)s->beta : 0.f;
+    const bool odd = (s->pk & 1) != 0;
+    const float4* __restrict__ vin = odd ? V1 : V0;   // state of this iteration
+    float4* __restrict__ vout = odd ? W0 : W1;        // state of the next one
+    const int t = threadIdx.x;
+    const int lane = t & 31;
+    const int warp = t >> 5;
+    const int64_t n = ca.n;
+    const int64_t ntiles = (n + kTile - 1) / kTile;
+    const int64_t my_tiles = blockIdx.x < ntiles ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+    const int stage_floats = kBand + 4 * ca.nwin * ca.wlen;
+    if (t == 0) {
+        for (int k = 0; k < kStages; ++k) {
+            mbar_init(&full[k], 1);
+            mbar_init(&empty[k], kConsumerWarps);
         }
-        if (norm <= s->tol || s->since > 200) {
-            s->status = ST_CONV;
-            s->done = 1;
-        } else if (it >= s->maxit) {
-            s->status = ST_MAXIT;
-            s->done = 1;
-        } else if (brk) {
-            s->status = ST_BREAK;
-            s->done = 1;
+        bad = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    auto interior = [&](int64_t i0) { return i0 + ca.lo >= 0 && i0 + ca.hi <= n; };
+
+    // sums: g = r.u, |r|^2, u.w, u.s, p.w, p.s (u, w of the next iteration; p, s of this one)
+    double v[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    int64_t issued = 0;
+    const WaitCtl wc = g_wait_ctl;
+    const int polls = wc.polls > 0 ? wc.polls : kDefaultPolls;
+    if (warp == kConsumerWarps) {
+        // ---------------- producer: band block and state windows of each tile
+        if (lane == 0 && !wc.withhold) {
+            const uint64_t pol = evict_first_policy();
+            const uint32_t wbytes = (uint32_t)ca.wlen * 16u;
+            for (int64_t k = 0; k < my_tiles; ++k, issued = k) {
+                const int st = (int)(k % kStages);
+                if (k >= kStages && !mbar_wait(&empty[st], (uint32_t)(((k / kStages) - 1) & 1), polls)) {
+                    bad = 1;
+                    break;
+                }
+                const int64_t tile = blockIdx.x + k * gridDim.x;
+                const int64_t i0 = tile * kTile;
+                float* dst = smem + (size_t)st * stage_floats;
+                const bool in = interior(i0);
+                mbar_expect_tx(&full[st], kBand * 4 + (in ? (uint32_t)ca.nwin * wbytes : 0u));
+                bulk_g2s_hint(dst, band + (size_t)tile * kBand, kBand * 4, &full[st], pol);
+                if (in)
+                    for (int w = 0; w < ca.nwin; ++w)
+                        bulk_g2s(dst + kBand + 4 * w * ca.wlen, vin + (i0 + ca.woff[w]), wbytes, &full[st]);
+            }
+        }
+    } else {
+        // ---------------- consumers: row i0 + t of every tile
+        for (int64_t k = 0; k < my_tiles; ++k) {
+            const int st = (int)(k % kStages);
+            const int64_t i0 = (blockIdx.x + k * gridDim.x) * (int64_t)kTile;
+            const int64_t i = i0 + t;
+            // the correction is only read and written by this row: load it while the stage fills
+            const float dold = (mode == 0 && i < n) ? __ldcs(d + i) : 0.f;
+            if (!mbar_wait(&full[st], (uint32_t)((k / kStages) & 1), polls)) {
+                bad = 1;
+                break;
+            }
+            const float* bs = smem + (size_t)st * stage_floats;
+            const float4* win = reinterpret_cast<const float4*>(bs + kBand);
+            float acc_u = 0.f, acc_p = 0.f;
+            float4 c = make_float4(0.f, 0.f, 0.f, 0.f);  // this row's state
+            if (interior(i0) && mode == 0) {
+#pragma unroll
+                for (int g = 0; g < NG; ++g) {
+                    // u_{i+1} at this lane's dx = 0 neighbour of stencil column g; dx = -1 / +1
+                    // from the lanes beside it, lanes 0 / 31 form that outer value themselves
+                    const int pc = ca.bpos[3 * g + 1] + t;
+                    const float4 vc = win[pc];
+                    const float uc = next_u(vc, alpha, beta);
+                    float ue = 0.f;
+                    if (lane == 0 || lane == 31) ue = next_u(win[lane == 0 ? pc - 1 : pc + 1], alpha, beta);
+                    float ul = __shfl_up_sync(0xffffffffu, uc, 1);
+                    float ur = __shfl_down_sync(0xffffffffu, uc, 1);
+                    if (lane == 0) ul = ue;
+                    if (lane == 31) ur = ue;
+                    acc_u = fmaf(bs[(3 * g) * kTile + t], ul, acc_u);
+                    acc_u = fmaf(bs[(3 * g + 1) * kTile + t], uc, acc_u);
+                    acc_u = fmaf(bs[(3 * g + 2) * kTile + t], ur, acc_u);
+                    if (3 * g + 1 == kCenter) c = vc;
+                }
+            } else {
+                const bool in = interior(i0);
+#pragma unroll
+                for (int b = 0; b < NB; ++b) {
+                    float4 nb;
+                    if (in) {
+                        nb = win[ca.bpos[b] + t];
+                    } else {
+                        const int64_t j = min(max(i + ca.off[b], (int64_t)0), n - 1);
+                        nb = __ldg(vin + j);
+                    }
+                    const float a = bs[b * kTile + t];
+                    if (mode == 0) {
+                        acc_u = fmaf(a, next_u(nb, alpha, beta), acc_u);
+                    } else {
+                        acc_u = fmaf(a, nb.x, acc_u);
+                        acc_p = fmaf(a, nb.w, acc_p);
+                    }
+                    if (b == kCenter) c = nb;
+                }
+            }
+            const float diag = bs[kCenter * kTile + t];
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&empty[st]);
+            if (i < n) {
+                float un, spn, pn;
+                if (mode == 0) {
+                    pn = fmaf(beta, c.w, c.x);      // p_i = u_i + beta p_{i-1}
+                    spn = fmaf(beta, c.z, c.y);     // D^-1 s_i = D^-1 w_i + beta D^-1 s_{i-1}
+                    un = fmaf(-alpha, spn, c.x);    // u_{i+1}, as next_u forms it
+                    d[i] = fmaf(alpha, pn, dold);   // d += alpha p_i
+                } else {
+                    pn = c.w;                       // the kept direction (0 when fresh)
+                    spn = acc_p / diag;             // D^-1 A p, formed afresh
+                    un = c.x;
+                }
+                const float w = acc_u;              // (A u_{i+1})_i
+                vout[i] = make_float4(un, w / diag, spn, pn);
+                const double du = un, dd = diag, ds = (double)spn * dd;
+                v[0] += dd * du * du;
+                v[1] += (dd * du) * (dd * du);
+                v[2] += du * (double)w;
+                v[3] += du * ds;
+                v[4] += (double)pn * (double)w;
+                v[5] += (double)pn * ds;
+            }
+        }
+    }
+    __syncthreads();
+    if (bad) {
+        // let the copies this CTA issued land (bounded) before its shared memory is released
+        if (warp == kConsumerWarps && lane == 0)
+            for (int64_t k = issued > kStages ? issued - kStages : 0; k < issued; ++k)
+                for (int tries = 0; tries < (1 << 20) && !mbar_try_wait(&full[k % kStages], (uint32_t)((k / kStages) & 1));
+                     ++tries) {
+                }
+        if (t == 0) report_status(s, ST_TIMEOUT);
+        // the CTA still takes its turn in the grid reduction (with nothing to add)
+#pragma unroll
+        for (int j = 0; j < 6; ++j) v[j] = 0.0;
+    }
+    double tt[6];
+    if (grid_reduce<6>(v, rb, tt) && threadIdx.x == 0) {
+        // s->rho holds r.u of the current u, s->tau that of the u the kept direction was
+        // formed from: a continuing segment start replaces the current u, so its b divides
+        // by the older one
+        const double g = tt[0];
+        const double beta_n = mode == 1 ? 0.0 : g / (mode == 2 ? s->tau : s->rho);
+        const double pap = tt[2] + beta_n * (tt[3] + tt[4]) + beta_n * beta_n * tt[5];
+        s->beta = beta_n;
+        s->alpha = g / pap;
+        if (mode == 0) s->tau = s->rho;
+        s->rho = g;
+        s->pk += 1;
+        const double norm = sqrt(tt[1]);
+        s->norm = norm;
+        if (mode == 0) {
+            const long long it = s->iter + 1;
+            s->iter = it;
+            // the FP32 recurrence has stagnated when no new minimum (5% below the best)
+            // appeared for 200 iterations: end the segment so that the FP64 residual is
+            // recomputed and fed back
+            if (norm < 0.95 * s->best) {
+                s->best = norm;
+                s->since = 0;
+            } else {
+                s->since += 1;
+            }
+            if (norm <= s->tol || s->since > 200) {
+                report_status(s, ST_CONV);
+            } else if (it >= s->maxit) {
+                report_status(s, ST_MAXIT);
+            } else if (!(g > 0.0) || !(pap > 0.0)) {
+                report_status(s, ST_BREAK);
+            }
+        } else if (!(g > 0.0) || !(pap > 0.0)) {
+            atomicMax(&s->status, (int)ST_BREAK);  // read by the host after the start pass
         }
     }
 }
 
-// x64 += scale * d32 (with the last SpMV's alpha p when it is still pending); d32 = 0.  The
-// pending flag is cleared by the next k_f32_init.
-__global__ void k_add_correction(int64_t n, double* __restrict__ x, float* __restrict__ d, const float* P0,
-                                 const float* P1, const Scal* s, double scale)
+// u = D^-1 (r64 / scale) into the current state (p_prev = 0 and d = 0 when fresh): the start
+// of a segment of k_f32_cg
+__global__ void __launch_bounds__(kThreads) k_f32_cg_seed(int64_t n, const double* __restrict__ r64,
+                                                          const float* __restrict__ dinv32, float4* V0, float4* V1,
+                                                          float* __restrict__ d, int fresh, const Scal* s,
+                                                          double inv_scale)
 {
-    const bool dpend = s->dpend != 0;
-    const float alpha = (float)s->alpha;
-    const float* __restrict__ p = (s->pk & 1) ? P1 : P0;  // the last direction formed
+    float4* __restrict__ v = (s->pk & 1) ? V1 : V0;
     for (int64_t i = gtid(); i < n; i += gstride()) {
-        float di = d[i];
-        if (dpend) di = fmaf(alpha, p[i], di);
-        x[i] += scale * (double)di;
+        float4 c = v[i];
+        c.x = (float)(r64[i] * inv_scale) * dinv32[i];
+        if (fresh) {
+            c.y = 0.f;
+            c.z = 0.f;
+            c.w = 0.f;
+            d[i] = 0.f;
+        }
+        v[i] = c;
+    }
+}
+
+// x64 += scale * d32; d32 = 0
+__global__ void k_fold_correction(int64_t n, double* __restrict__ x, float* __restrict__ d, double scale)
+{
+    for (int64_t i = gtid(); i < n; i += gstride()) {
+        x[i] += scale * (double)d[i];
         d[i] = 0.f;
     }
 }
@@ -1398,39 +1397,77 @@ int sm_count()
     return count;
 }
 
-template <int NB, int STAGES>
-size_t tma_smem()
-{
-    return sizeof(float) * STAGES * (NB * kTile + 2 * (NB / 3) * kPWin);
-}
-
-// configurations of the FP32 band SpMV pipeline: (stages, CTAs per SM)
+// configurations of the FP32 iteration pipeline: (stages, CTAs per SM)
 constexpr int kSpmvCfg[2][2] = {{3, 1}, {2, 2}};
 
-template <int NB>
-int launch_f32_spmv_tma(Matrix* m, int cfg)
+// Window geometry of k_f32_cg for a domain: one window per stencil plane (dz) covering the
+// rows [i0 - NN0 - 1, i0 + kTile + NN0 + 1) when that is shorter than three windows of
+// kTile + 2 rows (x-lines shorter than about a tile), else one window per stencil column
+// (dy, dz) of kTile + 2 rows; bpos[b] locates band b's neighbour of consumer row 0 in shared
+// memory (float4 elements).
+CgArgs cg_args(const Domain* d)
 {
-    Workspace* w = m->ws;
-    const Domain* d = m->dom;
-    constexpr int NG = NB / 3;
-    TmaBandArgs ta;
-    int64_t h = 0;
-    for (int b = 0; b < NB; ++b) {
-        ta.off[b] = (int)d->band_off[b];
-        h = std::max<int64_t>(h, std::abs(d->band_off[b]));
+    CgArgs ca{};
+    const int64_t nn0 = d->nn[0], nn01 = d->nn[0] * d->nn[1];
+    const bool three = d->dim == 3;
+    const bool merged = 2 * nn0 + kTile + 2 <= 3 * (kTile + 2);
+    const int planes = three ? 3 : 1;
+    int64_t nominal[kMaxWin];
+    int64_t len;
+    if (merged) {
+        ca.nwin = planes;
+        len = kTile + 2 * nn0 + 2;
+        for (int z = 0; z < planes; ++z) nominal[z] = (three ? (z - 1) * nn01 : 0) - nn0 - 1;
+    } else {
+        ca.nwin = 3 * planes;
+        len = kTile + 2;
+        for (int z = 0; z < planes; ++z)
+            for (int y = 0; y < 3; ++y) nominal[3 * z + y] = (three ? (z - 1) * nn01 : 0) + (y - 1) * nn0 - 1;
     }
-    for (int g = 0; g < NG; ++g) ta.goff[g] = (int)d->band_off[3 * g];  // dx = -1 member
-    ta.n = d->n;
-    ta.halo = h;
-    const int64_t ntiles = (d->n + kTile - 1) / kTile;
-    const int grid = (int)std::min<int64_t>(ntiles, (int64_t)sm_count() * kSpmvCfg[cfg][1]);
-    if (cfg == 0)
-        RG_TIMED(T_F32_SPMV, (k_f32_spmv_tma<NB, 3><<<grid, kTile + 32, tma_smem<NB, 3>(), stream()>>>(
-                                 m->band32, ta, w->z32, w->p32[0], w->p32[1], w->q32, w->d32, rbuf(w), w->s)));
-    else
-        RG_TIMED(T_F32_SPMV, (k_f32_spmv_tma<NB, 2><<<grid, kTile + 32, tma_smem<NB, 2>(), stream()>>>(
-                                 m->band32, ta, w->z32, w->p32[0], w->p32[1], w->q32, w->d32, rbuf(w), w->s)));
-    RG_CHECK_LAUNCH();
+    ca.wlen = (int)len;  // the state is 16 bytes per row: every window start is 16-byte aligned
+    int64_t lo = 0, hi = 0;
+    for (int w = 0; w < ca.nwin; ++w) {
+        ca.woff[w] = (int)nominal[w];
+        lo = std::min<int64_t>(lo, nominal[w]);
+        hi = std::max<int64_t>(hi, nominal[w] + ca.wlen);
+    }
+    ca.lo = lo;
+    ca.hi = hi;
+    for (int b = 0; b < d->nbands; ++b) {
+        const int dy = (b / 3) % 3, dz = three ? b / 9 : 0;  // 0..2
+        const int w = merged ? dz : 3 * dz + dy;
+        ca.off[b] = (int)d->band_off[b];
+        ca.bpos[b] = w * ca.wlen + (int)(d->band_off[b] - ca.woff[w]);
+    }
+    ca.n = d->n;
+    return ca;
+}
+
+size_t cg_smem(const Domain* d, const CgArgs& ca, int stages)
+{
+    return sizeof(float) * (size_t)stages * ((size_t)d->nbands * kTile + 4 * (size_t)ca.nwin * ca.wlen);
+}
+
+// largest dynamic shared memory a launch of `kernel` may ask for: the device's opt-in limit
+// per CTA less the kernel's static shared memory
+int max_dyn_smem(const void* kernel, int* out)
+{
+    int dev = 0, optin = 0;
+    RG_CHECK_CUDA(cudaGetDevice(&dev));
+    RG_CHECK_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    cudaFuncAttributes fa{};
+    RG_CHECK_CUDA(cudaFuncGetAttributes(&fa, kernel));
+    *out = optin - (int)fa.sharedSizeBytes;
+    return RG_OK;
+}
+
+template <int NB, int S, int CPS>
+int cg_attribute()
+{
+    int lim = 0;
+    int rc = max_dyn_smem((const void*)k_f32_cg<NB, S, CPS>, &lim);
+    if (rc) return rc;
+    RG_CHECK_CUDA(cudaFuncSetAttribute(k_f32_cg<NB, S, CPS>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
     return RG_OK;
 }
 
@@ -1438,14 +1475,10 @@ int tma_attributes()
 {
     static bool done = false;
     if (!done) {
-        RG_CHECK_CUDA(cudaFuncSetAttribute(k_f32_spmv_tma<27, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)tma_smem<27, 3>()));
-        RG_CHECK_CUDA(cudaFuncSetAttribute(k_f32_spmv_tma<27, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)tma_smem<27, 2>()));
-        RG_CHECK_CUDA(cudaFuncSetAttribute(k_f32_spmv_tma<9, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)tma_smem<9, 3>()));
-        RG_CHECK_CUDA(cudaFuncSetAttribute(k_f32_spmv_tma<9, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)tma_smem<9, 2>()));
+        int rc;
+        if ((rc = cg_attribute<27, 3, 1>()) || (rc = cg_attribute<27, 2, 2>()) || (rc = cg_attribute<9, 3, 1>()) ||
+            (rc = cg_attribute<9, 2, 2>()))
+            return rc;
         RG_CHECK_CUDA(cudaFuncSetAttribute(k_band64_bulk<27, band64_stages<27>(), false>,
                                            cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            (int)band64_smem<27, band64_stages<27>()>()));
@@ -1463,43 +1496,102 @@ int tma_attributes()
     return RG_OK;
 }
 
-int launch_spmv_cfg(Matrix* m, int cfg)
+template <int NB, int S, int CPS>
+const void* cg_kernel() { return (const void*)k_f32_cg<NB, S, CPS>; }
+
+const void* cg_kernel_for(int nb, int cfg)
 {
-    return m->dom->nbands == 27 ? launch_f32_spmv_tma<27>(m, cfg) : launch_f32_spmv_tma<9>(m, cfg);
+    if (nb == 27) return cfg == 0 ? cg_kernel<27, 3, 1>() : cg_kernel<27, 2, 2>();
+    return cfg == 0 ? cg_kernel<9, 3, 1>() : cg_kernel<9, 2, 2>();
 }
 
-// Picks the faster SpMV pipeline for this matrix once per workspace: a few timed launches of
-// each configuration before the first FP32 segment seeds the recursion (their outputs are
-// overwritten by that seed).
+// whether configuration cfg reaches its CTAs per SM with this domain's windows
+bool cg_config_fits(const Domain* d, int cfg)
+{
+    const CgArgs ca = cg_args(d);
+    const size_t smem = cg_smem(d, ca, kSpmvCfg[cfg][0]);
+    int lim = 0;
+    if (max_dyn_smem(cg_kernel_for(d->nbands, cfg), &lim) != RG_OK || smem > (size_t)lim) return false;
+    int blocks = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, cg_kernel_for(d->nbands, cfg), kTile + 32, smem) !=
+        cudaSuccess)
+        return false;
+    return blocks >= kSpmvCfg[cfg][1];
+}
+
+// one launch of the fused FP32 iteration (mode 0) or of a segment start (mode 1, 2)
+template <int NB>
+int launch_cg(Matrix* m, int cfg, int mode)
+{
+    Workspace* w = m->ws;
+    const Domain* d = m->dom;
+    const CgArgs ca = cg_args(d);
+    const int64_t ntiles = (d->n + kTile - 1) / kTile;
+    const int grid = (int)std::min<int64_t>(ntiles, (int64_t)sm_count() * kSpmvCfg[cfg][1]);
+    const size_t smem = cg_smem(d, ca, kSpmvCfg[cfg][0]);
+    if (cfg == 0)
+        RG_TIMED(T_F32_SPMV, (k_f32_cg<NB, 3, 1><<<grid, kTile + 32, smem, stream()>>>(
+                                 m->band32, ca, w->v4[0], w->v4[1], w->v4[0], w->v4[1], w->d32, rbuf(w), w->s, mode)));
+    else
+        RG_TIMED(T_F32_SPMV, (k_f32_cg<NB, 2, 2><<<grid, kTile + 32, smem, stream()>>>(
+                                 m->band32, ca, w->v4[0], w->v4[1], w->v4[0], w->v4[1], w->d32, rbuf(w), w->s, mode)));
+    RG_CHECK_LAUNCH();
+    return RG_OK;
+}
+
+int launch_spmv_cfg(Matrix* m, int cfg, int mode = 0)
+{
+    return m->dom->nbands == 27 ? launch_cg<27>(m, cfg, mode) : launch_cg<9>(m, cfg, mode);
+}
+
+__global__ void k_fill_state(int64_t n, float4* __restrict__ v0, float4* __restrict__ v1, float* __restrict__ d)
+{
+    for (int64_t i = gtid(); i < n; i += gstride()) {
+        v0[i] = make_float4(1.f, 0.f, 0.f, 0.f);
+        v1[i] = make_float4(1.f, 0.f, 0.f, 0.f);
+        d[i] = 0.f;
+    }
+}
+
+// Picks the faster iteration pipeline for this matrix once per workspace: a few timed
+// iterations of each configuration that fits, from the state u = 1, before the first FP32
+// segment seeds the recursion (which overwrites what these launches wrote).
 int tune_spmv(Matrix* m)
 {
     Workspace* w = m->ws;
     if (w->spmv_cfg >= 0) return RG_OK;
-    if (timers_on()) {  // keep the timed launch counts clean: default configuration
-        w->spmv_cfg = m->force_spmv >= 0 ? m->force_spmv : 0;
+    bool fits[2] = {cg_config_fits(m->dom, 0), cg_config_fits(m->dom, 1)};
+    if (!fits[0] && !fits[1]) {
+        set_error("FP32 iteration: no pipeline configuration fits the shared memory of one SM");
+        return RG_NOT_SUPPORTED;
+    }
+    if (m->force_spmv >= 0 && !fits[m->force_spmv]) {
+        set_error("rg_solver_set_config: that configuration does not fit this grid's windows");
+        return RG_INVALID_ARG;
+    }
+    const int fallback = fits[1] ? 1 : 0;
+    if (timers_on()) {  // keep the timed launch counts clean: no tuning launches
+        w->spmv_cfg = m->force_spmv >= 0 ? m->force_spmv : fallback;
         return RG_OK;
     }
-    // every timed launch does the full work: z = 1, p = 0, beta = 0 (q = A 1, p.q > 0)
-    k_fill32<<<w->grid_vec, kThreads, 0, stream()>>>(w->n, w->z32, 1.0f);
-    RG_CHECK_LAUNCH();
-    RG_CHECK_CUDA(cudaMemsetAsync(w->p32[0], 0, sizeof(float) * w->n, stream()));
-    RG_CHECK_CUDA(cudaMemsetAsync(w->p32[1], 0, sizeof(float) * w->n, stream()));
-    // and for the update kernel: r = 1, d = 0, finite scalars
-    k_fill32<<<w->grid_vec, kThreads, 0, stream()>>>(w->n, w->r32, 1.0f);
-    RG_CHECK_LAUNCH();
-    RG_CHECK_CUDA(cudaMemsetAsync(w->d32, 0, sizeof(float) * w->n, stream()));
-    w->hs->beta = 0.0;
-    w->hs->pk = 0;
-    w->hs->rho = 1.0;
-    w->hs->norm = 1.0;
+    w->spmv_us[0] = w->spmv_us[1] = 0.0;
     int rc = RG_OK;
     cudaEvent_t e0, e1;
     RG_CHECK_CUDA(cudaEventCreate(&e0));
     RG_CHECK_CUDA(cudaEventCreate(&e1));
     float best = 1e30f;
-    int best_cfg = 0;
-    for (int cfg = 0; cfg < 2; ++cfg) {
-        if ((rc = write_scal_fields(w, 0.0, 1, 0))) break;  // done = 0
+    int best_cfg = fallback;
+    for (int cfg = 0; cfg < 2 && rc == RG_OK; ++cfg) {
+        if (!fits[cfg]) continue;
+        k_fill_state<<<w->grid_vec, kThreads, 0, stream()>>>(w->n, w->v4[0], w->v4[1], w->d32);
+        RG_CHECK_LAUNCH();
+        w->hs->alpha = 0.0;
+        w->hs->beta = 0.0;
+        w->hs->rho = 1.0;
+        w->hs->tau = 1.0;
+        w->hs->pk = 0;
+        w->hs->norm = 1.0;
+        if ((rc = write_scal_fields(w, 0.0, 1LL << 40, 0))) break;  // done = 0, no iteration cap
         for (int k = 0; k < 2 && rc == RG_OK; ++k) rc = launch_spmv_cfg(m, cfg);
         RG_CHECK_CUDA(cudaEventRecord(e0, stream()));
         for (int k = 0; k < 8 && rc == RG_OK; ++k) rc = launch_spmv_cfg(m, cfg);
@@ -1513,52 +1605,18 @@ int tune_spmv(Matrix* m)
             best_cfg = cfg;
         }
     }
-    // the update kernel's grid: fewer CTAs shorten its reduction tail, more hide latency
-    w->spmv_cfg = best_cfg;
-    if (m->force_spmv >= 0) w->spmv_cfg = m->force_spmv;
-    const int64_t nv = (w->n + 3) / 4;
-    float best_u = 1e30f;
-    int best_grid = w->grid_vec;
-    for (int per_sm : {2, 4, 8}) {
-        const int g = grid_for(nv, kThreads, per_sm);
-        if ((rc = write_scal_fields(w, 0.0, 1LL << 40, 0))) break;  // done = 0, no iteration cap
-        w->grid_upd32 = g;
-        RG_CHECK_CUDA(cudaEventRecord(e0, stream()));
-        for (int k = 0; k < 8 && rc == RG_OK; ++k) {
-            RG_TIMED(T_F32_UPDATE, (k_f32_update<<<g, kThreads, 0, stream()>>>(
-                                       w->n, w->r32, w->q32, m->dinv32, w->z32, rbuf(w), w->s)));
-            rc = cudaGetLastError() == cudaSuccess ? RG_OK : RG_CUDA_ERROR;
-        }
-        RG_CHECK_CUDA(cudaEventRecord(e1, stream()));
-        RG_CHECK_CUDA(cudaEventSynchronize(e1));
-        float ms = 0;
-        cudaEventElapsedTime(&ms, e0, e1);
-        if (rc == RG_OK && ms < best_u) {
-            best_u = ms;
-            best_grid = g;
-        }
-    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    if (rc) {
-        set_error("FP32 update tuning launch failed");
-        return rc;
-    }
-    w->grid_upd32 = best_grid;
+    if (rc) return rc;
+    w->spmv_cfg = m->force_spmv >= 0 ? m->force_spmv : best_cfg;
+    w->grid_upd32 = 0;  // the iteration has no separate update kernel
     return RG_OK;
 }
 
 int f32_step(Matrix* m)
 {
     Workspace* w = m->ws;
-    const Domain* d = m->dom;
-    int rc = launch_spmv_cfg(m, w->spmv_cfg < 0 ? 0 : w->spmv_cfg);
-    if (rc) return rc;
-    RG_TIMED(T_F32_UPDATE, (k_f32_update<<<w->grid_upd32 > 0 ? w->grid_upd32 : w->grid_vec, kThreads, 0, stream()>>>(
-                               d->n, w->r32, w->q32, m->dinv32, w->z32, rbuf(w),
-                               w->s)));
-    RG_CHECK_LAUNCH();
-    return RG_OK;
+    return launch_spmv_cfg(m, w->spmv_cfg < 0 ? 0 : w->spmv_cfg, 0);
 }
 
 // balance (first solve only) and the preconditioner data (paso Solver.cpp:98,177)
@@ -1715,7 +1773,7 @@ int solve_f32(Matrix* m, const rg_solver_opts* o, OuterState& st, rg_diag& dg)
     Workspace* w = m->ws;
     const int64_t n = m->dom->n;
     const int eg = grid_for(n, kThreads, 8);
-    const int chunk = chunk_for(n, 4 * 27 + 60);
+    const int chunk = chunk_for(n, 4 * 27 + 40);
     // segment reduction factor: 1e-2 keeps the FP32 recurrence within a few ulps of the
     // true residual (smaller factors let it drift and cost iterations)
     const double seg = std::fmin(std::fmax(o->inner_tolerance > 0 ? o->inner_tolerance : 1e-2, 1e-4), 0.5);
@@ -1728,12 +1786,19 @@ int solve_f32(Matrix* m, const rg_solver_opts* o, OuterState& st, rg_diag& dg)
     bool first = true;
     long long done_iters = 0;
     for (;;) {
-        // (re)seed the FP32 recurrence from the FP64 residual; keep p after the first time
-        RG_TIMED(T_VECTOR, (k_f32_init<<<eg, kThreads, 0, stream()>>>(n, w->r, m->dinv32, w->r32, w->z32,
-                                                                      w->p32[0], w->d32, first ? 1 : 0, rbuf(w),
-                                                                      w->s, 1.0 / scale)));
+        // (re)seed the FP32 recurrence from the FP64 residual, keeping the search direction
+        // after the first time; the start pass forms A u and A p and the first step length
+        RG_TIMED(T_VECTOR, (k_f32_cg_seed<<<eg, kThreads, 0, stream()>>>(n, w->r, m->dinv32, w->v4[0], w->v4[1],
+                                                                         w->d32, first ? 1 : 0, w->s, 1.0 / scale)));
         RG_CHECK_LAUNCH();
+        w->hs->status = ST_RUN;
+        RG_CHECK_CUDA(cudaMemcpyAsync(&w->s->status, &w->hs->status, sizeof(int), cudaMemcpyHostToDevice, stream()));
+        if ((rc = launch_spmv_cfg(m, w->spmv_cfg < 0 ? 0 : w->spmv_cfg, first ? 1 : 2))) return rc;
         if ((rc = read_scal(w))) return rc;
+        if (w->hs->status == ST_BREAK || w->hs->status == ST_TIMEOUT) {
+            bool restart = false;
+            return status_from(w->hs->status, 0, o, st.totIter, &restart);
+        }
         const double norm0 = w->hs->norm;  // ||r32||
         // stop this segment when the recursive residual has dropped by `seg`, or below
         // what the dual-norm test needs (with a margin for the FP32 recurrence)
@@ -1751,8 +1816,7 @@ int solve_f32(Matrix* m, const rg_solver_opts* o, OuterState& st, rg_diag& dg)
             return status_from(dst, it, o, st.totIter, &restart);
         }
         // fold the FP32 correction into x and test the FP64 true residual
-        RG_TIMED(T_VECTOR, (k_add_correction<<<eg, kThreads, 0, stream()>>>(n, w->x, w->d32, w->p32[0], w->p32[1],
-                                                                            w->s, scale)));
+        RG_TIMED(T_VECTOR, (k_fold_correction<<<eg, kThreads, 0, stream()>>>(n, w->x, w->d32, scale)));
         RG_CHECK_LAUNCH();
         st.last2 = n2r;
         st.lastm = nmr;
@@ -1864,8 +1928,9 @@ void free_workspace(Matrix* m)
     if (!w) return;
     double* dd[] = {w->r, w->x, w->rs, w->x2, w->q, w->z, w->p, w->bb, w->partials};
     for (double* p : dd) cudaFree(p);
-    float* ff[] = {w->r32, w->d32, w->q32, w->z32, w->p32[0], w->p32[1]};
-    for (float* p : ff) cudaFree(p);
+    cudaFree(w->d32);
+    cudaFree(w->v4[0]);
+    cudaFree(w->v4[1]);
     cudaFree(w->counter);
     cudaFree(w->s);
     cudaFree(w->bad);

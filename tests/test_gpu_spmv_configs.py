@@ -1,6 +1,7 @@
-"""Both FP32 SpMV pipeline configurations of the FP32_REFINE solve, forced one at a time
-through rg_solver_set_config (0: 3 stages x 1 CTA/SM, 1: 2 stages x 2 CTAs/SM), on Bricks
-and Rectangles with interior and ragged edge tiles.  Each solution is within 1e-7 relative
+"""Both pipeline configurations of the fused FP32 iteration of the FP32_REFINE solve, forced
+one at a time through rg_solver_set_config (0: 3 stages x 1 CTA/SM, 1: 2 stages x 2
+CTAs/SM), on Bricks and Rectangles with interior and ragged edge tiles, with one window per
+stencil plane (short x-lines) and one per stencil column (x-lines longer than a tile).  Each solution is within 1e-7 relative
 of the FP64 PCG solution at tol 1e-10, the forced configuration is the one used, and the
 iteration counts agree within 3% (an inner operator that differed from A would show as
 extra iterations or an FP64 fallback, since the FP64 refinement still drives the true
@@ -60,7 +61,7 @@ def test_forced_spmv_configs_agree(cuda, ne):
         st, dg = R.solve(m, b, x, R.opts(tolerance=1e-10, precision=L.RG_PREC_FP32_REFINE))
         assert st == 0 and dg.converged and not dg.fp64_fallback
         used, ug, us = _config(m)
-        assert used == cfg and ug > 0
+        assert used == cfg and ug == 0  # one kernel per iteration: no separate update grid
         assert all(v > 0 for v in us)  # the tuner timed both configurations
         err = np.linalg.norm(x.cpu().numpy() - ref) / np.linalg.norm(ref)
         assert err < 1e-7, (cfg, err)
