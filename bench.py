@@ -186,9 +186,11 @@ def cpu_reference_warmup(inp, threads):
 # ----------------------------------------------------------------------------------------------
 
 # algorithmic bytes per launch of the dominant kernel, per DOF (n): one fused FP32 PCG
-# iteration reads the row's 27 band values (4 B each, padded bands count) and its 16-byte
-# iteration state {u, D^-1 A u, D^-1 A p, p}, writes the new state, and updates the
-# correction d (read + write)
+# iteration reads the row's operator data and its 16-byte iteration state {u, D^-1 A u,
+# D^-1 A p, p}, writes the new state, and updates the correction d (read + write).  Operator
+# data: the element coefficient of the row's node (4 B, RG_LAYOUT_COEF, the timed path), or
+# the row's 27 band values (4 B each, padded bands count, RG_LAYOUT_BAND)
+F32_COEF_BYTES_PER_ROW = 4 + 16 + 16 + 8
 F32_SPMV_BYTES_PER_ROW = 27 * 4 + 16 + 16 + 8
 
 
@@ -258,10 +260,12 @@ def run_ours(args):
         o.tolerance = tol
         o.mode = mode
         o.precision = precision
-        o.layout = L.RG_LAYOUT_BAND if precision == L.RG_PREC_FP32_REFINE else L.RG_LAYOUT_CSR
+        o.layout = L.RG_LAYOUT_COEF if precision == L.RG_PREC_FP32_REFINE else L.RG_LAYOUT_CSR
         return o
 
     fast = opts(L.RG_MODE_STANDARD, L.RG_PREC_FP32_REFINE)
+    if args.inner_tol > 0:
+        fast.inner_tolerance = args.inner_tol
     plain = opts(L.RG_MODE_PASO, L.RG_PREC_FP64)
     empty = L.rg_coef(None, 0)
     cA = L.rg_coef(A_d.data_ptr(), L.RG_COEF_PER_ELEMENT)
@@ -276,6 +280,8 @@ def run_ours(args):
     y32 = torch.empty_like(kap32)
     learned = opts(L.RG_MODE_STANDARD, L.RG_PREC_FP32_REFINE)
     learned.initial_guess = guess.data_ptr()
+    if args.inner_tol > 0:
+        learned.inner_tolerance = args.inner_tol
     learned.guess_sweeps = args.sweeps
     timed = learned if args.path == "learned" else fast
     side = torch.cuda.Stream(device=dev)
@@ -327,10 +333,26 @@ def run_ours(args):
         print(json.dumps({"only": args.only, "iterations": int(step(o).num_iter)}), flush=True)
         return
     if args.only == "fast":
-        for _ in range(args.warmup + args.steps):
+        for _ in range(args.warmup):
             d = step(timed)
         torch.cuda.synchronize()
-        print(json.dumps({"only": "fast", "path": args.path, "iterations": int(d.num_iter)}), flush=True)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            d = step(timed)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        # the iteration kernel's average launch time (events around every launch, one step)
+        lib.rg_timers_reset()
+        lib.rg_timers_enable(1)
+        step(timed)
+        torch.cuda.synchronize()
+        lib.rg_timers_enable(0)
+        _, kt, kms = L.timers()["f32_spmv"]
+        print(json.dumps({"only": "fast", "path": args.path, "iterations": int(d.num_iter),
+                          "outer_steps": int(d.num_outer), "inner_operator": int(d.inner_operator),
+                          "fp64_fallback": int(d.fp64_fallback), "ms_per_step": e0.elapsed_time(e1) / args.steps,
+                          "iteration_kernel_us": kms / max(kt, 1) * 1e3}), flush=True)
         return
 
     # --- FP64 reference solution for the error statement (paso algorithm, rtol 1e-10, or
@@ -391,6 +413,28 @@ def run_ours(args):
     torch.cuda.synchronize()
     f32_ms = max_over_ranks(ev0.elapsed_time(ev1) / n_f)
     x_f32 = x.clone()
+
+    # --- the same FP32 refinement with the operator streamed from the FP32 band copy
+    # (RG_LAYOUT_BAND) instead of evaluated from the element coefficients
+    fast_band = opts(L.RG_MODE_STANDARD, L.RG_PREC_FP32_REFINE)
+    fast_band.layout = L.RG_LAYOUT_BAND
+    step(fast_band)
+    barrier()
+    ev0.record(stream)
+    for _ in range(n_f):
+        d_fb = step(fast_band)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    f32_band_ms = max_over_ranks(ev0.elapsed_time(ev1) / n_f)
+    x_f32_band = x.clone()
+    # its iteration kernel's average launch time (events around every launch, one step)
+    lib.rg_timers_reset()
+    lib.rg_timers_enable(1)
+    step(fast_band)
+    torch.cuda.synchronize()
+    lib.rg_timers_enable(0)
+    _, bt, bms = L.timers()["f32_spmv"]
+    band_us = bms / max(bt, 1) * 1e3
 
     # --- the same with A given expanded (its 9 values repeated at the 8 Gauss points, the form
     # escript's general assembler reads): the assembly reads 1.2 GB of A instead of 151 MB
@@ -458,10 +502,11 @@ def run_ours(args):
     ms_events = ev0.elapsed_time(ev1) / n_prof
     tm = L.timers()
 
-    # dominant kernel: FP32 band SpMV (+ p.q); average launch time from the live events
+    # dominant kernel: the fused FP32 iteration; average launch time from the live events
     spmv_n, spmv_t, spmv_ms = tm["f32_spmv"]
     avg_s = spmv_ms / max(spmv_t, 1) / 1e3
-    algo_bytes = F32_SPMV_BYTES_PER_ROW * n
+    coef_used = bool(d_fast.inner_operator)
+    algo_bytes = (F32_COEF_BYTES_PER_ROW if coef_used else F32_SPMV_BYTES_PER_ROW) * n
     peaks = {}
     pk_path = os.path.join(REPO, "MEASURED_PEAKS.json")
     if os.path.exists(pk_path):
@@ -476,7 +521,11 @@ def run_ours(args):
         tr = json.load(open(tr_path)).get("f32_spmv")
         if tr and tr.get("ne") == ne:
             traffic = tr.get("bytes_per_launch")
-    roofline = {"bound": "hbm", "kernel": "k_f32_cg<27> (one fused FP32 PCG iteration: 27-band SpMV, vector updates, one reduction)",
+    roofline = {"bound": "hbm",
+                "kernel": ("k_f32_cg<27, element coefficients> (one fused FP32 PCG iteration: operator from kappa per "
+                           "element, vector updates, one reduction)" if coef_used else
+                           "k_f32_cg<27, band> (one fused FP32 PCG iteration: 27-band SpMV, vector updates, one "
+                           "reduction)"),
                 "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
                 "frac": round(achieved / hbm, 4), "peak_source": peak_note,
                 "algorithmic_bytes_per_launch": algo_bytes, "avg_launch_us": round(avg_s * 1e6, 2),
@@ -569,6 +618,7 @@ def run_ours(args):
         errors = {"oracle": (f"{s['kind']} paso Solver/PCG in FP64 on the host, rtol {oracle_rtol:g} "
                              f"({s['oracle_iterations']} iterations)"),
                   "timed_path": err_of(x_fast), "fp32_refine_no_guess": err_of(x_f32),
+                  "fp32_refine_band": err_of(x_f32_band),
                   "plain_fp64_paso_csr": err_of(x_plain), "plain_fp64_paso_band": err_of(x_plain_band),
                   "fp64_standard_band": err_of(x_std_band),
                   "reference_at_rtol": float(np.linalg.norm(s["x"] - xo) / nrm)}
@@ -578,8 +628,15 @@ def run_ours(args):
     cfg, ug = C.c_int(), C.c_int()
     spmv_us = (C.c_double * 2)()
     lib.rg_solver_config(mat, C.byref(cfg), C.byref(ug), spmv_us)
-    spmv_names = {0: "k_f32_cg<27, 3 stages x 1 CTA/SM>", 1: "k_f32_cg<27, 2 stages x 2 CTAs/SM>"}
+    spmv_names = ({0: "k_f32_cg<27, element coefficients, 3 stages x 2 CTAs/SM>",
+                   1: "k_f32_cg<27, element coefficients, 2 stages x 2 CTAs/SM>"} if coef_used else
+                  {0: "k_f32_cg<27, band, 3 stages x 1 CTA/SM>", 1: "k_f32_cg<27, band, 2 stages x 2 CTAs/SM>"})
     roofline["kernel"] = spmv_names.get(cfg.value, roofline["kernel"])
+    band_bytes = F32_SPMV_BYTES_PER_ROW * n
+    roofline_band = {"kernel": "k_f32_cg<27, band> (the same iteration streaming the FP32 band copy)",
+                     "algorithmic_bytes_per_launch": band_bytes, "avg_launch_us": round(band_us, 2),
+                     "achieved": round(band_bytes / (band_us * 1e-6) / 1e9, 1), "peak": hbm, "unit": "GB/s",
+                     "frac": round(band_bytes / (band_us * 1e-6) / 1e9 / hbm, 4), "peak_source": peak_note}
     roofline["tuned"] = {"spmv_config": cfg.value, "update_grid": ug.value,
                          "spmv_us_per_config": [round(v, 2) for v in spmv_us]}
 
@@ -619,9 +676,11 @@ def run_ours(args):
                                f"PCG+Jacobi rtol {rtol:g} (assemble+constrain+solve per step)",
                    "ne": [ne, ne, ne], "n_dof": n, "nnz": nnz, "seed": args.seed,
                    "path": ("learned warm start (U-Net on tcgen05, fields coarsened to 64^3, Chebyshev-"
-                            f"smoothed x{args.sweeps}) + FP32 27-band PCG with FP64 residual replacement"
+                            f"smoothed x{args.sweeps}) + FP32 PCG (operator from the element coefficients, one "
+                            "fused kernel per iteration) with FP64 residual replacement"
                             if args.path == "learned" else
-                            "FP32 27-band PCG with FP64 residual replacement"),
+                            "FP32 PCG (operator from the element coefficients, one fused kernel per iteration) with "
+                            "FP64 residual replacement"),
                    "l2": (f"inputs larger than L2 (FP64 CSR values {nnz * 8 / 1e6:.0f} MB, band copy "
                           f"{27 * 4 * n / 1e6:.0f} MB per step)"),
                    "parallelism": f"{world} independent replicas" if world > 1 else "1 GPU"},
@@ -630,6 +689,7 @@ def run_ours(args):
         "error_vs_fp64": err,
         "error_vs_oracle": errors["timed_path"] if errors else None,
         "errors_vs_oracle": errors,
+        "inner_operator": "element coefficients" if coef_used else "band copy",
         "plain_fp64": {"ms": round(plain_ms, 3), "iterations": plain_iters,
                        "algorithm": "paso PCG with residual smoothing, balanced CSR FP64",
                        "band_layout_ms": round(plain_band_ms, 3),
@@ -640,9 +700,12 @@ def run_ours(args):
         "speedup_vs_plain_fp64": round(min(plain_ms, plain_band_ms, std_band_ms) / ms, 3),
         "speedup_vs_paso_csr": round(plain_ms / ms, 3),
         "fp32_refine_no_guess": {"ms": round(f32_ms, 3), "iterations": int(d_f32.num_iter),
+                                 "inner_operator": "element coefficients" if d_f32.inner_operator else "band copy",
                                  "speedup_vs_plain_fp64": round(min(plain_ms, plain_band_ms, std_band_ms) / f32_ms, 3),
                                  "with_A_expanded_ms": round(f32x_ms, 3),
                                  "with_A_expanded_iterations": int(d_fx.num_iter)},
+        "fp32_refine_band": {"ms": round(f32_band_ms, 3), "iterations": int(d_fb.num_iter),
+                             "inner_operator": "band copy (RG_LAYOUT_BAND)", "roofline": roofline_band},
         "learned_guess": ({"rejected": bool(d_fast.guess_rejected),
                            "guess_rel_residual": float(d_fast.guess_residual / d_fast.rhs_norm),
                            "smoothing_steps": args.sweeps,
@@ -729,6 +792,8 @@ def main():
     ap.add_argument("--path", choices=["learned", "fp32"], default="learned",
                     help="timed path: learned warm start + FP32 refinement, or FP32 refinement alone")
     ap.add_argument("--sweeps", type=int, default=8, help="Chebyshev smoothing steps on the learned guess")
+    ap.add_argument("--inner-tol", type=float, default=0.0,
+                    help="FP32 segment reduction factor of the refinement (0: the library's default)")
     ap.add_argument("--no-batched", dest="batched", action="store_false",
                     help="skip the batched 64-system workload")
     ap.add_argument("--spmv-config", type=int, choices=[-1, 0, 1], default=-1,

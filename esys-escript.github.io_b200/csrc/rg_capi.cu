@@ -70,6 +70,7 @@ void free_domain(Domain* d)
 
 void free_matrix(Matrix* m)
 {
+    free_coef(m);
     release_workspace(m);
     free_residual_scratch(m);
     free_system_workspace(m);
@@ -365,6 +366,7 @@ int rg_matrix_reset(rg_matrix* mat)
     RG_CHECK_CUDA(cudaMemsetAsync(m.val, 0, sizeof(double) * m.dom->nnz * m.nb * m.nb, stream()));
     m.balanced = false;
     m.solver_ready = false;
+    coef_reset(&m);
     return RG_OK;
 }
 
@@ -406,6 +408,7 @@ int rg_assemble_single(rg_matrix* mat, double* rhs, const rg_coef* A, const rg_c
         int rc = require_unbalanced(&mat->m, "rg_assemble_single");
         if (rc) return rc;
         mat->m.solver_ready = false;
+        if ((rc = coef_on_assemble(&mat->m, c, false))) return rc;
     }
     return assemble_single_impl(mat->m.dom, mat->m.val, rhs, c, false);
 }
@@ -425,6 +428,7 @@ int rg_assemble_single_reduced(rg_matrix* mat, double* rhs, const rg_coef* A, co
         int rc = require_unbalanced(&mat->m, "rg_assemble_single_reduced");
         if (rc) return rc;
         mat->m.solver_ready = false;
+        if ((rc = coef_on_assemble(&mat->m, c, true))) return rc;
     }
     return assemble_single_impl(mat->m.dom, mat->m.val, rhs, c, true);
 }
@@ -440,6 +444,7 @@ int rg_assemble_system(rg_matrix* mat, double* rhs, const rg_coef* A, const rg_c
         int rc = require_unbalanced(&mat->m, "rg_assemble_system");
         if (rc) return rc;
         mat->m.solver_ready = false;
+        if ((rc = coef_on_assemble(&mat->m, c, false))) return rc;
     }
     if (mat->m.nb == 1) return assemble_single_impl(mat->m.dom, mat->m.val, rhs, c, false);
     return assemble_system_impl(mat->m.dom, mat->m.nb, mat->m.val, rhs, c, false);
@@ -456,6 +461,7 @@ int rg_assemble_system_reduced(rg_matrix* mat, double* rhs, const rg_coef* A, co
         int rc = require_unbalanced(&mat->m, "rg_assemble_system_reduced");
         if (rc) return rc;
         mat->m.solver_ready = false;
+        if ((rc = coef_on_assemble(&mat->m, c, true))) return rc;
     }
     if (mat->m.nb == 1) return assemble_single_impl(mat->m.dom, mat->m.val, rhs, c, true);
     return assemble_system_impl(mat->m.dom, mat->m.nb, mat->m.val, rhs, c, true);
@@ -476,6 +482,7 @@ static int assemble_boundary_any(rg_matrix* mat, double* rhs, const rg_coef* d, 
         int rc = require_unbalanced(&mat->m, who);
         if (rc) return rc;
         mat->m.solver_ready = false;
+        coef_invalidate(&mat->m);  // face terms are not part of the coefficient operator
     }
     return assemble_boundary_impl(mat->m.dom, mat->m.nb, reduced, mat->m.val, rhs, d, y);
 }
@@ -497,6 +504,7 @@ int rg_insert_constraint(rg_matrix* mat, double* rhs, const double* q, const dou
         int rc = require_unbalanced(&mat->m, "rg_insert_constraint");
         if (rc) return rc;
         mat->m.solver_ready = false;
+        if ((rc = coef_on_constraint(&mat->m, q))) return rc;
     }
     if (mat->m.nb != 1) return launch_system_constraint(&mat->m, rhs, q, r, rhs_only);
     return launch_insert_constraint(&mat->m, rhs, q, r, rhs_only);
@@ -509,6 +517,7 @@ int rg_nullify_rows_and_cols(rg_matrix* mat, const double* mask_row, const doubl
     int rc = require_unbalanced(&mat->m, "rg_nullify_rows_and_cols");
     if (rc) return rc;
     mat->m.solver_ready = false;
+    coef_invalidate(&mat->m);
     if (mat->m.nb != 1) return launch_system_nullify(&mat->m, mask_row, mask_col, main_diagonal_value);
     return launch_nullify(&mat->m, mask_row, mask_col, main_diagonal_value);
 }

@@ -79,6 +79,22 @@ struct Workspace;        // solver vectors, allocated lazily (rg_solver.cu)
 struct SysWorkspace;     // vectors of the block (PDE system) solver (rg_system.cu)
 struct ResidualScratch;  // reduction scratch of rg_residual_norms (rg_residual.cu)
 
+// What the values of a scalar matrix were built from, so that the FP32 inner solve can
+// evaluate the operator from the element coefficients instead of streaming stored values
+// (RG_LAYOUT_COEF, rg_coef.cu).  Representable: the sum of interior assemblies with A = kappa I
+// per element (CONSTANT, PER_ELEMENT, or EXPANDED with the same value at every Gauss point)
+// and no B, C, D, followed by at most insertConstraint.  khat is node-indexed: khat[i] =
+// kappa of the element whose upper corner is node i (0 where there is no such element), with
+// the sign bit set on nodes the constraint fixes; it holds n + NN0 NN1 + NN0 + kCoefPad floats
+// so that every element a node touches (i + {0,1} + NN0 {0,1} + NN0 NN1 {0,1}) is in range.
+constexpr int64_t kCoefPad = 1024;
+struct CoefRecord {
+    int state = 0;              // 0: values are zero, 1: khat describes them, -1: not representable
+    bool constrained = false;   // a constraint was recorded (a later assembly is not representable)
+    float* khat = nullptr;
+    int* bad = nullptr;         // set on the device when an element's A is not kappa I with kappa >= 0
+};
+
 struct Matrix {
     Domain* dom;
     int nb = 1;                // block size (numEq = numComp of a PDE system; 1 = scalar)
@@ -97,6 +113,7 @@ struct Matrix {
     Workspace* ws = nullptr;
     ResidualScratch* rs = nullptr;
     SysWorkspace* sws = nullptr;
+    CoefRecord coef;
 };
 
 // ---------------------------------------------------------------- deterministic reductions
@@ -260,6 +277,14 @@ int solve_system(Matrix* m, const double* rhs, double* x, const rg_solver_opts* 
 int residual_norms_system(Matrix* m, const double* b, const double* x, double* l2, double* linf);
 void free_system_workspace(Matrix* m);
 void free_residual_scratch(Matrix* m);
+// coefficient record of a scalar matrix (rg_coef.cu)
+void coef_reset(Matrix* m);                                                // values zeroed
+void coef_invalidate(Matrix* m);                                           // values no longer representable
+int coef_on_assemble(Matrix* m, const rg_coef* c[6], bool reduced);        // before an interior assembly
+int coef_on_constraint(Matrix* m, const double* q);                        // insertConstraint (not rhs_only)
+// whether the record describes the values (reads the device flag: synchronises the stream)
+int coef_usable(Matrix* m, bool* usable);
+void free_coef(Matrix* m);
 // l2 norm of b - A x with the matrix's values as they are (unbalance: undo an in-place
 // balancing on the fly); synchronises the stream
 int residual_l2(Matrix* m, const double* b, const double* x, bool unbalance, double* l2);

@@ -80,11 +80,14 @@ struct Workspace {
     cudaGraphExec_t graph[3] = {nullptr, nullptr, nullptr};
     int graph_chunk[3] = {0, 0, 0};
     int graph_sweeps[3] = {0, 0, 0};  // Jacobi sweeps the captured iterations apply
+    bool graph_coef[3] = {false, false, false};  // the captured FP32 iterations' operator
     long long graph_launches[3][T_COUNT] = {};
     int sweeps = 1;  // Jacobi sweeps of the current paso solve (Smoother.cpp:100-128)
     bool band64 = false;              // paso FP64 SpMV on the FP64 band copy (RG_LAYOUT_BAND)
     bool graph_band64[3] = {false, false, false};
-    int spmv_cfg = -1;   // FP32 iteration pipeline: 0 = 3 stages x 1 CTA/SM, 1 = 2 stages x 2 CTAs/SM
+    int spmv_cfg = -1;   // FP32 iteration pipeline of the band operator (kSpmvCfg; -1: not tuned)
+    int coef_cfg = -1;   // the same for the element-coefficient operator (kCoefCfg)
+    bool coef_op = false;  // the current FP32 solve evaluates the operator from the coefficients
     int grid_upd32 = 0;  // kept for rg_solver_config: the FP32 iteration has no separate update kernel
     double spmv_us[2] = {0, 0};  // tuner's time per launch of each SpMV configuration
 };
@@ -109,6 +112,7 @@ int ensure_workspace(Matrix* m, bool fp32)
             m->ws = m->dom->spare_ws;
             m->dom->spare_ws = nullptr;
             m->ws->spmv_cfg = -1;
+            m->ws->coef_cfg = -1;
             m->ws->grid_upd32 = 0;
         }
     }
@@ -909,6 +913,12 @@ struct CgArgs {
     int nwin, wlen;        // windows per tile and rows per window
     int64_t n;
     int64_t lo, hi;        // a tile is interior when i0 + lo >= 0 and i0 + hi <= n
+    // element-coefficient operator (RG_LAYOUT_COEF): khat windows and the Q1 table
+    int kwoff[4];          // khat window offsets (multiples of 4: 16-byte aligned starts)
+    int nkw, kwlen;        // khat windows per tile and floats per window (a multiple of 4)
+    int kpos[8];           // shared-memory float index of corner element j = a + 2b + 4c for row 0
+    int kdelta[8];         // khat offset of corner element j: a + NN0 b + NN0 NN1 c
+    float T[8];            // Q1 stiffness entry for nodes differing in x (bit 0), y (1), z (2)
 };
 
 // u_{i+1} at a neighbour from its state: u - a (D^-1 w + b D^-1 s_prev)
@@ -917,16 +927,72 @@ __device__ __forceinline__ float next_u(float4 v, float alpha, float beta)
     return fmaf(-alpha, fmaf(beta, v.z, v.y), v.x);
 }
 
-template <int NB, int kStages, int kCtas>
+// A row of the element-coefficient operator from the kappa of the 2^dim elements around the
+// node, kv[a + 2b + 4c] for the element whose upper corner is the node + (a, b, c).  The
+// neighbour at offset o lies in element (a, b, c) when o_x is a - 1 or a (likewise y, z), so its
+// coefficient is T[|o|] times the sum of kappa over the elements with a in A(o_x), b in A(o_y),
+// c in A(o_z), where A(-1) = {0}, A(1) = {1}, A(0) = {0, 1}.  CoefRow keeps the sums over a
+// (sx[o_x + 1][b][c]); coef_at adds the y and z sums and the table entry for band b =
+// (o_x+1) + 3 (o_y+1) + 9 (o_z+1).
+struct CoefRow {
+    float sx[3][2][2];
+};
+
+template <int NB>
+__device__ __forceinline__ void coef_row(const float (&kv)[8], CoefRow& r)
+{
+#pragma unroll
+    for (int b = 0; b < 2; ++b)
+#pragma unroll
+        for (int c = 0; c < (NB == 27 ? 2 : 1); ++c) {
+            const float k0 = kv[0 + 2 * b + 4 * c], k1 = kv[1 + 2 * b + 4 * c];
+            r.sx[0][b][c] = k0;
+            r.sx[1][b][c] = k0 + k1;
+            r.sx[2][b][c] = k1;
+        }
+}
+
+// the sum of kappa over the elements shared by the node and its neighbour of band b
+template <int NB>
+__device__ __forceinline__ float ksum_at(const CoefRow& r, int b)
+{
+    const int x = b % 3, y = (b / 3) % 3, z = b / 9;
+    auto ysum = [&](int c) {
+        return y == 0 ? r.sx[x][0][c] : (y == 2 ? r.sx[x][1][c] : r.sx[x][0][c] + r.sx[x][1][c]);
+    };
+    if (NB == 27) return z == 0 ? ysum(0) : (z == 2 ? ysum(1) : ysum(0) + ysum(1));
+    return ysum(0);
+}
+
+// the Q1 table class of band b: which coordinates differ (bit 0 x, 1 y, 2 z)
+__host__ __device__ constexpr int band_class(int b) { return (b % 3 != 1) + 2 * ((b / 3) % 3 != 1) + 4 * (b / 9 != 1); }
+
+template <int NB>
+__device__ __forceinline__ float coef_at(const CoefRow& r, const float (&T)[8], int b)
+{
+    return T[NB == 27 ? band_class(b) : (band_class(b) & 3)] * ksum_at<NB>(r, b);
+}
+
+// Fused FP32 PCG iteration, two operators:
+//   COEF = false: the tile's band block (FP32 copy of the balanced matrix) is bulk-copied with
+//                 the state windows; the diagonal is its centre band.
+//   COEF = true:  the operator is evaluated from the element coefficients (unbalanced A; the
+//                 Jacobi-preconditioned iteration is the same for any symmetric diagonal scaling
+//                 of the matrix, so the balancing is applied only where the FP64 refinement
+//                 hands residuals and corrections over): windows of khat replace the band
+//                 block (4 instead of 108 bytes per row).  Rows of nodes fixed by the constraint
+//                 are identity rows, solved exactly by the seed; their state stays zero, so
+//                 their columns drop out of every other row without a mask.
+template <int NB, int kStages, int kCtas, bool COEF>
 __global__ void __launch_bounds__(kTile + 32, kCtas) k_f32_cg(const float* __restrict__ band,
                                                               const __grid_constant__ CgArgs ca,
                                                               const float4* V0, const float4* V1,
                                                               float4* W0, float4* W1,
                                                               float* __restrict__ d, ReduceBuf rb, Scal* s, int mode)
 {
-    constexpr int kBand = NB * kTile;
     constexpr int kCenter = NB / 2;
     constexpr int NG = NB / 3;
+    constexpr int NK = NB == 27 ? 8 : 4;  // elements around a node
     extern __shared__ __align__(128) float smem[];
     __shared__ __align__(8) uint64_t full[kStages], empty[kStages];
     __shared__ int bad;
@@ -939,10 +1005,12 @@ __global__ void __launch_bounds__(kTile + 32, kCtas) k_f32_cg(const float* __res
     const int t = threadIdx.x;
     const int lane = t & 31;
     const int warp = t >> 5;
+    const int eoff = lane == 0 ? -1 : (lane == 31 ? 1 : 0);  // the outer x-neighbour of warp edge lanes
     const int64_t n = ca.n;
     const int64_t ntiles = (n + kTile - 1) / kTile;
     const int64_t my_tiles = blockIdx.x < ntiles ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
-    const int stage_floats = kBand + 4 * ca.nwin * ca.wlen;
+    const int kmat = COEF ? ca.nkw * ca.kwlen : NB * kTile;  // floats of the operator's part of a stage
+    const int stage_floats = kmat + 4 * ca.nwin * ca.wlen;
     if (t == 0) {
         for (int k = 0; k < kStages; ++k) {
             mbar_init(&full[k], 1);
@@ -960,7 +1028,7 @@ __global__ void __launch_bounds__(kTile + 32, kCtas) k_f32_cg(const float* __res
     const WaitCtl wc = g_wait_ctl;
     const int polls = wc.polls > 0 ? wc.polls : kDefaultPolls;
     if (warp == kConsumerWarps) {
-        // ---------------- producer: band block and state windows of each tile
+        // ---------------- producer: operator data and state windows of each tile
         if (lane == 0 && !wc.withhold) {
             const uint64_t pol = evict_first_policy();
             const uint32_t wbytes = (uint32_t)ca.wlen * 16u;
@@ -974,11 +1042,17 @@ __global__ void __launch_bounds__(kTile + 32, kCtas) k_f32_cg(const float* __res
                 const int64_t i0 = tile * kTile;
                 float* dst = smem + (size_t)st * stage_floats;
                 const bool in = interior(i0);
-                mbar_expect_tx(&full[st], kBand * 4 + (in ? (uint32_t)ca.nwin * wbytes : 0u));
-                bulk_g2s_hint(dst, band + (size_t)tile * kBand, kBand * 4, &full[st], pol);
+                mbar_expect_tx(&full[st], (uint32_t)kmat * 4u + (in ? (uint32_t)ca.nwin * wbytes : 0u));
+                if (COEF) {
+                    // khat is padded: every tile's windows are in range
+                    for (int w = 0; w < ca.nkw; ++w)
+                        bulk_g2s(dst + w * ca.kwlen, band + (i0 + ca.kwoff[w]), (uint32_t)ca.kwlen * 4u, &full[st]);
+                } else {
+                    bulk_g2s_hint(dst, band + (size_t)tile * NB * kTile, NB * kTile * 4, &full[st], pol);
+                }
                 if (in)
                     for (int w = 0; w < ca.nwin; ++w)
-                        bulk_g2s(dst + kBand + 4 * w * ca.wlen, vin + (i0 + ca.woff[w]), wbytes, &full[st]);
+                        bulk_g2s(dst + kmat + 4 * w * ca.wlen, vin + (i0 + ca.woff[w]), wbytes, &full[st]);
             }
         }
     } else {
@@ -994,26 +1068,50 @@ __global__ void __launch_bounds__(kTile + 32, kCtas) k_f32_cg(const float* __res
                 break;
             }
             const float* bs = smem + (size_t)st * stage_floats;
-            const float4* win = reinterpret_cast<const float4*>(bs + kBand);
+            const float4* win = reinterpret_cast<const float4*>(bs + kmat);
+            // this row's coefficients: formed from the element values (COEF), or read from the
+            // band block where they are used
+            CoefRow cr;
+            bool fixed = false;
+            if constexpr (COEF) {
+                float kv[8];
+#pragma unroll
+                for (int j = 0; j < NK; ++j) kv[j] = bs[ca.kpos[j] + t];
+                fixed = (__float_as_uint(kv[0]) >> 31) != 0;
+#pragma unroll
+                for (int j = 0; j < NK; ++j) kv[j] = fabsf(kv[j]);
+#pragma unroll
+                for (int j = NK; j < 8; ++j) kv[j] = 0.f;
+                coef_row<NB>(kv, cr);
+            }
+            auto coefb = [&](int b) -> float {
+                if constexpr (COEF)
+                    return coef_at<NB>(cr, ca.T, b);
+                else
+                    return bs[b * kTile + t];
+            };
             float acc_u = 0.f, acc_p = 0.f;
             float4 c = make_float4(0.f, 0.f, 0.f, 0.f);  // this row's state
             if (interior(i0) && mode == 0) {
+                // (a row's products are summed in band order: summing them per Q1 table class
+                // and scaling once was measured to cost ~7% more iterations at 128^3, from the
+                // FP32 cancellation of a Laplacian row's nearly zero sum)
 #pragma unroll
                 for (int g = 0; g < NG; ++g) {
                     // u_{i+1} at this lane's dx = 0 neighbour of stencil column g; dx = -1 / +1
-                    // from the lanes beside it, lanes 0 / 31 form that outer value themselves
+                    // from the lanes beside it; lanes 0 / 31 form that outer value themselves
                     const int pc = ca.bpos[3 * g + 1] + t;
                     const float4 vc = win[pc];
                     const float uc = next_u(vc, alpha, beta);
                     float ue = 0.f;
-                    if (lane == 0 || lane == 31) ue = next_u(win[lane == 0 ? pc - 1 : pc + 1], alpha, beta);
-                    float ul = __shfl_up_sync(0xffffffffu, uc, 1);
-                    float ur = __shfl_down_sync(0xffffffffu, uc, 1);
-                    if (lane == 0) ul = ue;
-                    if (lane == 31) ur = ue;
-                    acc_u = fmaf(bs[(3 * g) * kTile + t], ul, acc_u);
-                    acc_u = fmaf(bs[(3 * g + 1) * kTile + t], uc, acc_u);
-                    acc_u = fmaf(bs[(3 * g + 2) * kTile + t], ur, acc_u);
+                    if (lane == 0 || lane == 31) ue = next_u(win[pc + eoff], alpha, beta);
+                    const float up = __shfl_up_sync(0xffffffffu, uc, 1);
+                    const float dn = __shfl_down_sync(0xffffffffu, uc, 1);
+                    const float ul = lane == 0 ? ue : up;
+                    const float ur = lane == 31 ? ue : dn;
+                    acc_u = fmaf(coefb(3 * g), ul, acc_u);
+                    acc_u = fmaf(coefb(3 * g + 1), uc, acc_u);
+                    acc_u = fmaf(coefb(3 * g + 2), ur, acc_u);
                     if (3 * g + 1 == kCenter) c = vc;
                 }
             } else {
@@ -1027,17 +1125,21 @@ __global__ void __launch_bounds__(kTile + 32, kCtas) k_f32_cg(const float* __res
                         const int64_t j = min(max(i + ca.off[b], (int64_t)0), n - 1);
                         nb = __ldg(vin + j);
                     }
-                    const float a = bs[b * kTile + t];
                     if (mode == 0) {
-                        acc_u = fmaf(a, next_u(nb, alpha, beta), acc_u);
+                        acc_u = fmaf(coefb(b), next_u(nb, alpha, beta), acc_u);
                     } else {
-                        acc_u = fmaf(a, nb.x, acc_u);
-                        acc_p = fmaf(a, nb.w, acc_p);
+                        acc_u = fmaf(coefb(b), nb.x, acc_u);
+                        acc_p = fmaf(coefb(b), nb.w, acc_p);
                     }
                     if (b == kCenter) c = nb;
                 }
             }
-            const float diag = bs[kCenter * kTile + t];
+            float diag = coefb(kCenter);
+            if (COEF && fixed) {  // identity row: solved by the seed, state stays zero
+                acc_u = 0.f;
+                acc_p = 0.f;
+                diag = 1.f;
+            }
             __syncwarp();
             if (lane == 0) mbar_arrive(&empty[st]);
             if (i < n) {
@@ -1049,14 +1151,18 @@ __global__ void __launch_bounds__(kTile + 32, kCtas) k_f32_cg(const float* __res
                     d[i] = fmaf(alpha, pn, dold);   // d += alpha p_i
                 } else {
                     pn = c.w;                       // the kept direction (0 when fresh)
-                    spn = acc_p / diag;             // D^-1 A p, formed afresh
+                    spn = __fdividef(acc_p, diag);  // D^-1 A p, formed afresh
                     un = c.x;
                 }
                 const float w = acc_u;              // (A u_{i+1})_i
-                vout[i] = make_float4(un, w / diag, spn, pn);
+                vout[i] = make_float4(un, __fdividef(w, diag), spn, pn);
                 const double du = un, dd = diag, ds = (double)spn * dd;
                 v[0] += dd * du * du;
-                v[1] += (dd * du) * (dd * du);
+                // the segment's stopping norm: |r| of the balanced residual (band copy); for the
+                // unbalanced coefficient operator r.u = r.D^-1 r, which paso's balancing leaves
+                // unchanged and which is |B r|^2 when the balance vector is D^-1/2 (diagonally
+                // dominant rows)
+                v[1] += COEF ? dd * du * du : (dd * du) * (dd * du);
                 v[2] += du * (double)w;
                 v[3] += du * ds;
                 v[4] += (double)pn * (double)w;
@@ -1114,6 +1220,60 @@ __global__ void __launch_bounds__(kTile + 32, kCtas) k_f32_cg(const float* __res
         } else if (!(g > 0.0) || !(pap > 0.0)) {
             atomicMax(&s->status, (int)ST_BREAK);  // read by the host after the start pass
         }
+    }
+}
+
+// The element-coefficient operator's seed: the balanced FP64 residual is unbalanced (r =
+// r64 / bv, scaled by inv_scale); fixed nodes get their exact correction d = r (identity
+// rows) and a zero state; free rows u = r / diag (z, p, d = 0 when fresh).
+template <int NB>
+__global__ void __launch_bounds__(kThreads) k_f32_cg_seed_coef(const __grid_constant__ CgArgs ca,
+                                                               const double* __restrict__ r64,
+                                                               const double* __restrict__ bv,
+                                                               const float* __restrict__ khat, float4* V0,
+                                                               float4* V1,
+                                                               float* __restrict__ d, int fresh, const Scal* s,
+                                                               double inv_scale)
+{
+    constexpr int NK = NB == 27 ? 8 : 4;
+    float4* __restrict__ v = (s->pk & 1) ? V1 : V0;
+    const int64_t n = ca.n;
+    for (int64_t i = gtid(); i < n; i += gstride()) {
+        float kv[8];
+#pragma unroll
+        for (int j = 0; j < NK; ++j) kv[j] = khat[i + ca.kdelta[j]];
+        const bool fixed = (__float_as_uint(kv[0]) >> 31) != 0;
+#pragma unroll
+        for (int j = 0; j < NK; ++j) kv[j] = fabsf(kv[j]);
+#pragma unroll
+        for (int j = NK; j < 8; ++j) kv[j] = 0.f;
+        CoefRow cr;
+        coef_row<NB>(kv, cr);
+        const float r = (float)(r64[i] / bv[i] * inv_scale);
+        float4 c = v[i];
+        if (fixed) {
+            c = make_float4(0.f, 0.f, 0.f, 0.f);
+            d[i] = r;
+        } else {
+            c.x = r / coef_at<NB>(cr, ca.T, NB / 2);
+            if (fresh) {
+                c.y = 0.f;
+                c.z = 0.f;
+                c.w = 0.f;
+                d[i] = 0.f;
+            }
+        }
+        v[i] = c;
+    }
+}
+
+// x64 += scale * d32 / bv (the element-coefficient operator's correction is unbalanced); d32 = 0
+__global__ void k_fold_correction_unbalance(int64_t n, double* __restrict__ x, float* __restrict__ d,
+                                            const double* __restrict__ bv, double scale)
+{
+    for (int64_t i = gtid(); i < n; i += gstride()) {
+        x[i] += scale * (double)d[i] / bv[i];
+        d[i] = 0.f;
     }
 }
 
@@ -1229,7 +1389,7 @@ int run_until_done(Matrix* m, int kind, IterFn step, int chunk, long long cap, l
         return RG_OK;
     }
     if (!w->graph[kind] || w->graph_chunk[kind] != chunk || w->graph_sweeps[kind] != w->sweeps ||
-        w->graph_band64[kind] != w->band64) {
+        w->graph_band64[kind] != w->band64 || w->graph_coef[kind] != w->coef_op) {
         if (w->graph[kind]) cudaGraphExecDestroy(w->graph[kind]);
         w->graph[kind] = nullptr;
         long long before[T_COUNT], after[T_COUNT];
@@ -1253,6 +1413,7 @@ int run_until_done(Matrix* m, int kind, IterFn step, int chunk, long long cap, l
         w->graph_chunk[kind] = chunk;
         w->graph_sweeps[kind] = w->sweeps;
         w->graph_band64[kind] = w->band64;
+        w->graph_coef[kind] = w->coef_op;
         timers_snapshot(after);
         long long undo[T_COUNT];
         for (int k = 0; k < T_COUNT; ++k) {
@@ -1397,8 +1558,10 @@ int sm_count()
     return count;
 }
 
-// configurations of the FP32 iteration pipeline: (stages, CTAs per SM)
+// configurations of the FP32 iteration pipeline: (stages, CTAs per SM), for the band operator
+// and for the element-coefficient operator (whose stages are a quarter of the size)
 constexpr int kSpmvCfg[2][2] = {{3, 1}, {2, 2}};
+constexpr int kCoefCfg[2][2] = {{3, 2}, {2, 2}};
 
 // Window geometry of k_f32_cg for a domain: one window per stencil plane (dz) covering the
 // rows [i0 - NN0 - 1, i0 + kTile + NN0 + 1) when that is shorter than three windows of
@@ -1440,12 +1603,52 @@ CgArgs cg_args(const Domain* d)
         ca.bpos[b] = w * ca.wlen + (int)(d->band_off[b] - ca.woff[w]);
     }
     ca.n = d->n;
+    // element-coefficient operator: khat windows hold the elements around the tile's rows,
+    // corner j = a + 2b + 4c at node offset a + NN0 b + NN0 NN1 c (all >= 0): one window per
+    // element plane (c) when NN0 is short, else one per (b, c); starts rounded down to 4 floats
+    const int nk = three ? 8 : 4;
+    const bool kmerged = nn0 + kTile + 1 <= 2 * (kTile + 1);
+    int64_t knom[4];
+    int64_t klen;
+    if (kmerged) {
+        ca.nkw = three ? 2 : 1;
+        klen = kTile + nn0 + 1;
+        for (int c = 0; c < ca.nkw; ++c) knom[c] = c * nn01;
+    } else {
+        ca.nkw = three ? 4 : 2;
+        klen = kTile + 1;
+        for (int w = 0; w < ca.nkw; ++w) knom[w] = (w & 1) * nn0 + (w >> 1) * nn01;
+    }
+    ca.kwlen = (int)((klen + 3 + 3) & ~(int64_t)3);
+    for (int w = 0; w < ca.nkw; ++w) ca.kwoff[w] = (int)(knom[w] - (knom[w] & 3));
+    for (int j = 0; j < 8; ++j) {
+        const int a = j & 1, b = (j >> 1) & 1, c = j >> 2;
+        const int64_t delta = j < nk ? a + nn0 * b + nn01 * c : 0;
+        ca.kdelta[j] = (int)delta;
+        const int w = j < nk ? (kmerged ? c : b + 2 * c) : 0;
+        ca.kpos[j] = w * ca.kwlen + (int)(delta - ca.kwoff[w]);
+    }
+    // Q1 stiffness of the reference box (exact 1D integrals; the 2-point Gauss rule of the
+    // assembly is exact for them): per axis K = 1/h (same node) or -1/h, M = h/3 or h/6
+    for (int cls = 0; cls < 8; ++cls) {
+        double k1[3], m1[3];
+        for (int ax = 0; ax < 3; ++ax) {
+            const bool diff = (cls >> ax) & 1;
+            const double h = d->dx[ax];
+            k1[ax] = (diff ? -1.0 : 1.0) / h;
+            m1[ax] = diff ? h / 6.0 : h / 3.0;
+        }
+        const double t = three ? k1[0] * m1[1] * m1[2] + m1[0] * k1[1] * m1[2] + m1[0] * m1[1] * k1[2]
+                               : k1[0] * m1[1] + m1[0] * k1[1];
+        ca.T[cls] = (float)t;
+    }
     return ca;
 }
 
-size_t cg_smem(const Domain* d, const CgArgs& ca, int stages)
+size_t cg_smem(const Domain* d, const CgArgs& ca, int stages, bool coef)
 {
-    return sizeof(float) * (size_t)stages * ((size_t)d->nbands * kTile + 4 * (size_t)ca.nwin * ca.wlen);
+    const size_t mat = coef ? (size_t)ca.nkw * ca.kwlen : (size_t)d->nbands * kTile;
+    return sizeof(float) * (size_t)stages * (mat + 4 * (size_t)ca.nwin * ca.wlen);
 }
 
 // largest dynamic shared memory a launch of `kernel` may ask for: the device's opt-in limit
@@ -1461,13 +1664,14 @@ int max_dyn_smem(const void* kernel, int* out)
     return RG_OK;
 }
 
-template <int NB, int S, int CPS>
+template <int NB, int S, int CPS, bool COEF>
 int cg_attribute()
 {
     int lim = 0;
-    int rc = max_dyn_smem((const void*)k_f32_cg<NB, S, CPS>, &lim);
+    int rc = max_dyn_smem((const void*)k_f32_cg<NB, S, CPS, COEF>, &lim);
     if (rc) return rc;
-    RG_CHECK_CUDA(cudaFuncSetAttribute(k_f32_cg<NB, S, CPS>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+    RG_CHECK_CUDA(
+        cudaFuncSetAttribute(k_f32_cg<NB, S, CPS, COEF>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
     return RG_OK;
 }
 
@@ -1476,8 +1680,10 @@ int tma_attributes()
     static bool done = false;
     if (!done) {
         int rc;
-        if ((rc = cg_attribute<27, 3, 1>()) || (rc = cg_attribute<27, 2, 2>()) || (rc = cg_attribute<9, 3, 1>()) ||
-            (rc = cg_attribute<9, 2, 2>()))
+        if ((rc = cg_attribute<27, 3, 1, false>()) || (rc = cg_attribute<27, 2, 2, false>()) ||
+            (rc = cg_attribute<9, 3, 1, false>()) || (rc = cg_attribute<9, 2, 2, false>()) ||
+            (rc = cg_attribute<27, 3, 2, true>()) || (rc = cg_attribute<27, 2, 2, true>()) ||
+            (rc = cg_attribute<9, 3, 2, true>()) || (rc = cg_attribute<9, 2, 2, true>()))
             return rc;
         RG_CHECK_CUDA(cudaFuncSetAttribute(k_band64_bulk<27, band64_stages<27>(), false>,
                                            cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1496,45 +1702,67 @@ int tma_attributes()
     return RG_OK;
 }
 
-template <int NB, int S, int CPS>
-const void* cg_kernel() { return (const void*)k_f32_cg<NB, S, CPS>; }
+template <int NB, int S, int CPS, bool COEF>
+const void* cg_kernel() { return (const void*)k_f32_cg<NB, S, CPS, COEF>; }
 
-const void* cg_kernel_for(int nb, int cfg)
+const void* cg_kernel_for(int nb, int cfg, bool coef)
 {
-    if (nb == 27) return cfg == 0 ? cg_kernel<27, 3, 1>() : cg_kernel<27, 2, 2>();
-    return cfg == 0 ? cg_kernel<9, 3, 1>() : cg_kernel<9, 2, 2>();
+    if (coef) {
+        if (nb == 27) return cfg == 0 ? cg_kernel<27, 3, 2, true>() : cg_kernel<27, 2, 2, true>();
+        return cfg == 0 ? cg_kernel<9, 3, 2, true>() : cg_kernel<9, 2, 2, true>();
+    }
+    if (nb == 27) return cfg == 0 ? cg_kernel<27, 3, 1, false>() : cg_kernel<27, 2, 2, false>();
+    return cfg == 0 ? cg_kernel<9, 3, 1, false>() : cg_kernel<9, 2, 2, false>();
 }
+
+// (stages, CTAs per SM) of configuration cfg of an operator
+const int* cg_cfg(int cfg, bool coef) { return coef ? kCoefCfg[cfg] : kSpmvCfg[cfg]; }
 
 // whether configuration cfg reaches its CTAs per SM with this domain's windows
-bool cg_config_fits(const Domain* d, int cfg)
+bool cg_config_fits(const Domain* d, int cfg, bool coef)
 {
     const CgArgs ca = cg_args(d);
-    const size_t smem = cg_smem(d, ca, kSpmvCfg[cfg][0]);
+    const size_t smem = cg_smem(d, ca, cg_cfg(cfg, coef)[0], coef);
+    const void* kern = cg_kernel_for(d->nbands, cfg, coef);
     int lim = 0;
-    if (max_dyn_smem(cg_kernel_for(d->nbands, cfg), &lim) != RG_OK || smem > (size_t)lim) return false;
+    if (max_dyn_smem(kern, &lim) != RG_OK || smem > (size_t)lim) return false;
     int blocks = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, cg_kernel_for(d->nbands, cfg), kTile + 32, smem) !=
-        cudaSuccess)
-        return false;
-    return blocks >= kSpmvCfg[cfg][1];
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kern, kTile + 32, smem) != cudaSuccess) return false;
+    return blocks >= cg_cfg(cfg, coef)[1];
 }
 
-// one launch of the fused FP32 iteration (mode 0) or of a segment start (mode 1, 2)
+// one launch of the fused FP32 iteration (mode 0) or of a segment start (mode 1, 2) with the
+// workspace's current operator (band copy, or element coefficients when w->coef_op)
+template <int NB, int S, int CPS, bool COEF>
+void launch_cg_k(Matrix* m, const CgArgs& ca, int grid, size_t smem, int mode)
+{
+    Workspace* w = m->ws;
+    const float* op = COEF ? m->coef.khat : m->band32;
+    RG_TIMED(T_F32_SPMV, (k_f32_cg<NB, S, CPS, COEF><<<grid, kTile + 32, smem, stream()>>>(
+                             op, ca, w->v4[0], w->v4[1], w->v4[0], w->v4[1], w->d32, rbuf(w), w->s, mode)));
+}
+
 template <int NB>
 int launch_cg(Matrix* m, int cfg, int mode)
 {
-    Workspace* w = m->ws;
     const Domain* d = m->dom;
+    const bool coef = m->ws->coef_op;
     const CgArgs ca = cg_args(d);
+    const int* sc = cg_cfg(cfg, coef);
     const int64_t ntiles = (d->n + kTile - 1) / kTile;
-    const int grid = (int)std::min<int64_t>(ntiles, (int64_t)sm_count() * kSpmvCfg[cfg][1]);
-    const size_t smem = cg_smem(d, ca, kSpmvCfg[cfg][0]);
-    if (cfg == 0)
-        RG_TIMED(T_F32_SPMV, (k_f32_cg<NB, 3, 1><<<grid, kTile + 32, smem, stream()>>>(
-                                 m->band32, ca, w->v4[0], w->v4[1], w->v4[0], w->v4[1], w->d32, rbuf(w), w->s, mode)));
-    else
-        RG_TIMED(T_F32_SPMV, (k_f32_cg<NB, 2, 2><<<grid, kTile + 32, smem, stream()>>>(
-                                 m->band32, ca, w->v4[0], w->v4[1], w->v4[0], w->v4[1], w->d32, rbuf(w), w->s, mode)));
+    const int grid = (int)std::min<int64_t>(ntiles, (int64_t)sm_count() * sc[1]);
+    const size_t smem = cg_smem(d, ca, sc[0], coef);
+    if (coef) {
+        if (cfg == 0)
+            launch_cg_k<NB, 3, 2, true>(m, ca, grid, smem, mode);
+        else
+            launch_cg_k<NB, 2, 2, true>(m, ca, grid, smem, mode);
+    } else {
+        if (cfg == 0)
+            launch_cg_k<NB, 3, 1, false>(m, ca, grid, smem, mode);
+        else
+            launch_cg_k<NB, 2, 2, false>(m, ca, grid, smem, mode);
+    }
     RG_CHECK_LAUNCH();
     return RG_OK;
 }
@@ -1543,6 +1771,9 @@ int launch_spmv_cfg(Matrix* m, int cfg, int mode = 0)
 {
     return m->dom->nbands == 27 ? launch_cg<27>(m, cfg, mode) : launch_cg<9>(m, cfg, mode);
 }
+
+// the tuned configuration of the workspace's current operator
+int& cfg_slot(Workspace* w) { return w->coef_op ? w->coef_cfg : w->spmv_cfg; }
 
 __global__ void k_fill_state(int64_t n, float4* __restrict__ v0, float4* __restrict__ v1, float* __restrict__ d)
 {
@@ -1559,8 +1790,10 @@ __global__ void k_fill_state(int64_t n, float4* __restrict__ v0, float4* __restr
 int tune_spmv(Matrix* m)
 {
     Workspace* w = m->ws;
-    if (w->spmv_cfg >= 0) return RG_OK;
-    bool fits[2] = {cg_config_fits(m->dom, 0), cg_config_fits(m->dom, 1)};
+    int& slot = cfg_slot(w);
+    if (slot >= 0) return RG_OK;
+    const bool coef = w->coef_op;
+    bool fits[2] = {cg_config_fits(m->dom, 0, coef), cg_config_fits(m->dom, 1, coef)};
     if (!fits[0] && !fits[1]) {
         set_error("FP32 iteration: no pipeline configuration fits the shared memory of one SM");
         return RG_NOT_SUPPORTED;
@@ -1571,7 +1804,7 @@ int tune_spmv(Matrix* m)
     }
     const int fallback = fits[1] ? 1 : 0;
     if (timers_on()) {  // keep the timed launch counts clean: no tuning launches
-        w->spmv_cfg = m->force_spmv >= 0 ? m->force_spmv : fallback;
+        slot = m->force_spmv >= 0 ? m->force_spmv : fallback;
         return RG_OK;
     }
     w->spmv_us[0] = w->spmv_us[1] = 0.0;
@@ -1608,7 +1841,7 @@ int tune_spmv(Matrix* m)
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (rc) return rc;
-    w->spmv_cfg = m->force_spmv >= 0 ? m->force_spmv : best_cfg;
+    slot = m->force_spmv >= 0 ? m->force_spmv : best_cfg;
     w->grid_upd32 = 0;  // the iteration has no separate update kernel
     return RG_OK;
 }
@@ -1616,7 +1849,8 @@ int tune_spmv(Matrix* m)
 int f32_step(Matrix* m)
 {
     Workspace* w = m->ws;
-    return launch_spmv_cfg(m, w->spmv_cfg < 0 ? 0 : w->spmv_cfg, 0);
+    const int cfg = cfg_slot(w);
+    return launch_spmv_cfg(m, cfg < 0 ? 0 : cfg, 0);
 }
 
 // balance (first solve only) and the preconditioner data (paso Solver.cpp:98,177)
@@ -1773,7 +2007,7 @@ int solve_f32(Matrix* m, const rg_solver_opts* o, OuterState& st, rg_diag& dg)
     Workspace* w = m->ws;
     const int64_t n = m->dom->n;
     const int eg = grid_for(n, kThreads, 8);
-    const int chunk = chunk_for(n, 4 * 27 + 40);
+    const int chunk = chunk_for(n, w->coef_op ? 4 + 40 : 4 * 27 + 40);  // bytes per row of an iteration
     // segment reduction factor: 1e-2 keeps the FP32 recurrence within a few ulps of the
     // true residual (smaller factors let it drift and cost iterations)
     const double seg = std::fmin(std::fmax(o->inner_tolerance > 0 ? o->inner_tolerance : 1e-2, 1e-4), 0.5);
@@ -1788,12 +2022,25 @@ int solve_f32(Matrix* m, const rg_solver_opts* o, OuterState& st, rg_diag& dg)
     for (;;) {
         // (re)seed the FP32 recurrence from the FP64 residual, keeping the search direction
         // after the first time; the start pass forms A u and A p and the first step length
-        RG_TIMED(T_VECTOR, (k_f32_cg_seed<<<eg, kThreads, 0, stream()>>>(n, w->r, m->dinv32, w->v4[0], w->v4[1],
-                                                                         w->d32, first ? 1 : 0, w->s, 1.0 / scale)));
+        if (w->coef_op) {
+            const CgArgs ca = cg_args(m->dom);
+            if (m->dom->nbands == 27)
+                RG_TIMED(T_VECTOR, (k_f32_cg_seed_coef<27><<<eg, kThreads, 0, stream()>>>(
+                                       ca, w->r, m->bv, m->coef.khat, w->v4[0], w->v4[1], w->d32, first ? 1 : 0, w->s,
+                                       1.0 / scale)));
+            else
+                RG_TIMED(T_VECTOR, (k_f32_cg_seed_coef<9><<<eg, kThreads, 0, stream()>>>(
+                                       ca, w->r, m->bv, m->coef.khat, w->v4[0], w->v4[1], w->d32, first ? 1 : 0, w->s,
+                                       1.0 / scale)));
+        } else {
+            RG_TIMED(T_VECTOR, (k_f32_cg_seed<<<eg, kThreads, 0, stream()>>>(n, w->r, m->dinv32, w->v4[0], w->v4[1],
+                                                                             w->d32, first ? 1 : 0, w->s, 1.0 / scale)));
+        }
         RG_CHECK_LAUNCH();
         w->hs->status = ST_RUN;
         RG_CHECK_CUDA(cudaMemcpyAsync(&w->s->status, &w->hs->status, sizeof(int), cudaMemcpyHostToDevice, stream()));
-        if ((rc = launch_spmv_cfg(m, w->spmv_cfg < 0 ? 0 : w->spmv_cfg, first ? 1 : 2))) return rc;
+        const int cfg = cfg_slot(w);
+        if ((rc = launch_spmv_cfg(m, cfg < 0 ? 0 : cfg, first ? 1 : 2))) return rc;
         if ((rc = read_scal(w))) return rc;
         if (w->hs->status == ST_BREAK || w->hs->status == ST_TIMEOUT) {
             bool restart = false;
@@ -1816,7 +2063,11 @@ int solve_f32(Matrix* m, const rg_solver_opts* o, OuterState& st, rg_diag& dg)
             return status_from(dst, it, o, st.totIter, &restart);
         }
         // fold the FP32 correction into x and test the FP64 true residual
-        RG_TIMED(T_VECTOR, (k_fold_correction<<<eg, kThreads, 0, stream()>>>(n, w->x, w->d32, scale)));
+        if (w->coef_op)
+            RG_TIMED(T_VECTOR, (k_fold_correction_unbalance<<<eg, kThreads, 0, stream()>>>(n, w->x, w->d32, m->bv,
+                                                                                          scale)));
+        else
+            RG_TIMED(T_VECTOR, (k_fold_correction<<<eg, kThreads, 0, stream()>>>(n, w->x, w->d32, scale)));
         RG_CHECK_LAUNCH();
         st.last2 = n2r;
         st.lastm = nmr;
@@ -1847,7 +2098,7 @@ int solver_config(const Matrix* m, int* spmv_cfg, int* update_grid, double* spmv
 {
     if (spmv_us)
         for (int c = 0; c < 2; ++c) spmv_us[c] = m->ws ? m->ws->spmv_us[c] : 0.0;
-    if (spmv_cfg) *spmv_cfg = m->ws ? m->ws->spmv_cfg : -1;
+    if (spmv_cfg) *spmv_cfg = m->ws ? (m->ws->coef_op ? m->ws->coef_cfg : m->ws->spmv_cfg) : -1;
     if (update_grid) *update_grid = m->ws ? m->ws->grid_upd32 : 0;
     return RG_OK;
 }
@@ -1859,7 +2110,7 @@ int solver_set_config(Matrix* m, int spmv_cfg)
         return RG_INVALID_ARG;
     }
     m->force_spmv = spmv_cfg;
-    if (m->ws) m->ws->spmv_cfg = -1;  // re-tune (and apply) at the next FP32 solve
+    if (m->ws) m->ws->spmv_cfg = m->ws->coef_cfg = -1;  // re-tune (and apply) at the next FP32 solve
     return RG_OK;
 }
 
@@ -2016,8 +2267,20 @@ int solve_impl(Matrix* m, const double* rhs, double* x, const rg_solver_opts* o,
     // solve independent of anything an earlier, interrupted one left behind
     RG_CHECK_CUDA(cudaMemsetAsync(w->counter, 0, sizeof(unsigned), stream()));
     const bool band64 = !fp32 && o->layout == RG_LAYOUT_BAND;
-    if ((rc = prepare(m, fp32, band64))) return rc;
+    if (!fp32 && o->layout == RG_LAYOUT_COEF) {
+        set_error("solver: RG_LAYOUT_COEF evaluates the FP32 inner operator; FP64 solves use RG_LAYOUT_CSR or "
+                  "RG_LAYOUT_BAND");
+        return RG_NOT_SUPPORTED;
+    }
+    // the FP32 iterations evaluate the operator from the element coefficients when asked and
+    // when the matrix's values are what the coefficient record describes; else the band copy
+    bool coef = false;
+    if (fp32 && o->layout == RG_LAYOUT_COEF && (rc = coef_usable(m, &coef))) return rc;
+    if ((rc = prepare(m, fp32 && !coef, band64))) return rc;
+    if (coef && (rc = tma_attributes())) return rc;
     w->band64 = band64;
+    w->coef_op = coef;
+    dg.inner_operator = coef ? 1 : 0;
     const double t_setup = now_s();
     dg.set_up_time = t_setup - t_start;
 

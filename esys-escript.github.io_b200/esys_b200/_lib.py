@@ -21,7 +21,7 @@ RG_METHOD_PCG = 10
 RG_PRECOND_JACOBI = 20
 RG_MODE_PASO, RG_MODE_STANDARD = 0, 1
 RG_PREC_FP64, RG_PREC_FP32_REFINE = 0, 1
-RG_LAYOUT_CSR, RG_LAYOUT_BAND = 0, 1
+RG_LAYOUT_CSR, RG_LAYOUT_BAND, RG_LAYOUT_COEF = 0, 1, 2
 
 
 class PasoException(RuntimeError):
@@ -58,7 +58,8 @@ class rg_diag(C.Structure):
                 ("residual_norm", C.c_double), ("residual_max", C.c_double),
                 ("rhs_norm", C.c_double), ("converged", C.c_int), ("time", C.c_double),
                 ("set_up_time", C.c_double), ("net_time", C.c_double),
-                ("guess_residual", C.c_double), ("guess_rejected", C.c_int), ("fp64_fallback", C.c_int)]
+                ("guess_residual", C.c_double), ("guess_rejected", C.c_int), ("fp64_fallback", C.c_int),
+                ("inner_operator", C.c_int)]
 
 
 _lib = None

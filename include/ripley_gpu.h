@@ -193,6 +193,19 @@ int rg_save_mm(rg_matrix* mat, const char* path);
                                      layout stream an FP64 band copy (8 bytes per coefficient
                                      against the CSR's 12).  Scalar PDEs only: systems
                                      (block size 2, 3) always use the block CSR            */
+#define RG_LAYOUT_COEF 2          /* FP32_REFINE only: the FP32 inner PCG evaluates the operator
+                                     from the element coefficients instead of streaming stored
+                                     values (4 bytes per row instead of 108), when the matrix's
+                                     values are what the library recorded while building them:
+                                     interior assemblies of A = kappa I per element (CONSTANT,
+                                     PER_ELEMENT, or EXPANDED with one value per element) with
+                                     no B, C, D, then insertConstraint.  Otherwise (other
+                                     coefficients, face terms, nullifyRowsAndCols, reduced
+                                     order) the band copy is used (rg_diag.inner_operator).
+                                     Values changed through rg_matrix_values' pointer are not
+                                     seen: the FP64 outer residual then stops improving and
+                                     the solve finishes in FP64 (rg_diag.fp64_fallback), so
+                                     results stay correct.  FP64 solves: RG_NOT_SUPPORTED. */
 
 typedef struct {
     int method;                 /* RG_METHOD_PCG                                            */
@@ -229,6 +242,8 @@ typedef struct {
                                    and the solve started from zero instead                  */
     int fp64_fallback;          /* FP32_REFINE: 1 when the FP32 corrections stopped reducing
                                    the FP64 residual and the solve finished in FP64 PCG     */
+    int inner_operator;         /* FP32_REFINE: the operator of the FP32 iterations, 1 = the
+                                   element coefficients (RG_LAYOUT_COEF), 0 = the band copy */
 } rg_diag;
 
 void rg_solver_opts_default(rg_solver_opts* opts);

@@ -41,20 +41,25 @@ def _problem(ne, seed):
     return d, m, rhs, keep, (pat, val, rr)
 
 
-@pytest.mark.parametrize("mode,precision,tol", [
-    (L.RG_MODE_PASO, L.RG_PREC_FP64, 1e-8),        # k_band64_bulk (paso PCG on the FP64 band copy)
-    (L.RG_MODE_STANDARD, L.RG_PREC_FP32_REFINE, 1e-7),  # k_f32_spmv_tma (FP32 inner PCG)
+@pytest.mark.parametrize("mode,precision,layout,tol", [
+    # k_band64_bulk (paso PCG on the FP64 band copy)
+    (L.RG_MODE_PASO, L.RG_PREC_FP64, L.RG_LAYOUT_BAND, 1e-8),
+    # k_f32_cg on the FP32 band copy, and on the element coefficients
+    (L.RG_MODE_STANDARD, L.RG_PREC_FP32_REFINE, L.RG_LAYOUT_BAND, 1e-7),
+    (L.RG_MODE_STANDARD, L.RG_PREC_FP32_REFINE, L.RG_LAYOUT_COEF, 1e-7),
 ])
-def test_band_kernel_wait_timeout_is_reported_and_recoverable(cuda, mode, precision, tol):
+def test_band_kernel_wait_timeout_is_reported_and_recoverable(cuda, mode, precision, layout, tol):
     d, m, rhs, _keep, (pat, val, rr) = _problem((24, 20, 18), 31)
     ref = O.solve_paso(pat, val.copy(), rr, tol=1e-10)  # balances its copy in place
     assert ref.converged
-    o = R.opts(tolerance=1e-10, mode=mode, precision=precision, layout=L.RG_LAYOUT_BAND)
+    o = R.opts(tolerance=1e-10, mode=mode, precision=precision, layout=layout)
     x = torch.zeros(d.n, dtype=torch.float64, device="cuda")
     # a normal solve first: the FP32 tuner and the captured iteration graphs exist before the
     # waits are shortened, so the interrupted solve replays graphs captured earlier
     st, dg = R.solve(m, rhs, x, o)
     assert st == 0 and dg.converged
+    if layout == L.RG_LAYOUT_COEF:
+        assert dg.inner_operator == 1
     first = x.clone()
     lib = R.lib()
     x.fill_(7.0)
