@@ -526,7 +526,7 @@ class SolverOptions:
     # solver modes and precisions of this implementation
     MODE_PASO, MODE_STANDARD = L.RG_MODE_PASO, L.RG_MODE_STANDARD
     PRECISION_FP64, PRECISION_FP32_REFINE = L.RG_PREC_FP64, L.RG_PREC_FP32_REFINE
-    LAYOUT_CSR, LAYOUT_BAND = L.RG_LAYOUT_CSR, L.RG_LAYOUT_BAND
+    LAYOUT_CSR, LAYOUT_BAND, LAYOUT_COEF = L.RG_LAYOUT_CSR, L.RG_LAYOUT_BAND, L.RG_LAYOUT_COEF
 
 
 class SolverBuddy:
@@ -646,11 +646,14 @@ class SolverBuddy:
         return self.__precision
 
     def setMatrixLayout(self, layout):
-        """LAYOUT_CSR (default: the SpMV of FP64 solves reads the paso CSR values) or
+        """LAYOUT_CSR (default: the SpMV of FP64 solves reads the paso CSR values),
         LAYOUT_BAND (FP64 solves of scalar PDEs read an FP64 27-band copy of the balanced
-        matrix instead: the same arithmetic with fewer bytes).  FP32 refinement always uses
-        its FP32 band copy.  No reference counterpart."""
-        if layout not in (SolverOptions.LAYOUT_CSR, SolverOptions.LAYOUT_BAND):
+        matrix instead: the same arithmetic with fewer bytes; FP32 refinement uses its FP32
+        band copy with either of these two), or LAYOUT_COEF (FP32 refinement only: the FP32
+        iterations evaluate the operator from the element coefficients, when the matrix was
+        built from A = kappa I per element and a constraint; otherwise the band copy is used,
+        diagnostic 'inner_operator').  No reference counterpart."""
+        if layout not in (SolverOptions.LAYOUT_CSR, SolverOptions.LAYOUT_BAND, SolverOptions.LAYOUT_COEF):
             raise ValueError("unknown matrix layout %r" % (layout,))
         self.__layout = layout
 
@@ -677,7 +680,7 @@ class SolverBuddy:
         self.__diag = {"num_iter": 0, "num_level": 0, "num_inner_iter": 0, "time": 0.0,
                        "set_up_time": 0.0, "net_time": 0.0, "residual_norm": 0.0,
                        "converged": False, "num_outer": 0, "guess_rejected": False,
-                       "guess_residual": 0.0, "fp64_fallback": False}
+                       "guess_residual": 0.0, "fp64_fallback": False, "inner_operator": 0}
         if all or not cum:
             cum = {"cum_num_iter": 0, "cum_time": 0.0, "cum_set_up_time": 0.0,
                    "cum_net_time": 0.0, "cum_num_inner_iter": 0}
@@ -689,7 +692,7 @@ class SolverBuddy:
                            time=float(d.time), set_up_time=float(d.set_up_time),
                            net_time=float(d.net_time), guess_rejected=bool(d.guess_rejected),
                            guess_residual=float(d.guess_residual),
-                           fp64_fallback=bool(d.fp64_fallback))
+                           fp64_fallback=bool(d.fp64_fallback), inner_operator=int(d.inner_operator))
         self.__diag["cum_num_iter"] += int(d.num_iter)
         self.__diag["cum_time"] += float(d.time)
         self.__diag["cum_set_up_time"] += float(d.set_up_time)

@@ -289,6 +289,30 @@ def test_matrix_layout_through_solver_options(domain):
         pde.getSolverOptions().setMatrixLayout(7)
 
 
+def test_coefficient_layout_through_solver_options(domain):
+    """SolverOptions.setMatrixLayout(LAYOUT_COEF) with FP32 refinement: A = I (kronecker) and a
+    Dirichlet face evaluate the FP32 operator from the coefficients (diagnostic
+    inner_operator = 1) and give the FP64 solution; a D term makes the values not representable
+    and the band copy is used (inner_operator = 0), with the same accuracy."""
+    x = Solution(domain).getX()
+    ref = LinearPDE(domain)
+    ref.setValue(A=kronecker(domain), Y=1.0, q=whereZero(x[0]))
+    ref.getSolverOptions().setTolerance(1e-10)
+    u_ref = ref.getSolution()
+    for extra, expect in (({}, 1), ({"D": 0.5}, 0)):
+        p = LinearPDE(domain)
+        p.setValue(A=kronecker(domain), Y=1.0, q=whereZero(x[0]), **extra)
+        so = p.getSolverOptions()
+        so.setSolverMode(SolverOptions.MODE_STANDARD)
+        so.setPrecision(SolverOptions.PRECISION_FP32_REFINE)
+        so.setMatrixLayout(SolverOptions.LAYOUT_COEF)
+        so.setTolerance(1e-10)
+        u = p.getSolution()
+        assert so.getDiagnostics("inner_operator") == expect
+        if not extra:
+            assert Lsup(u - u_ref) <= 1e-8 * Lsup(u_ref)
+
+
 # ---- LinearPDE coefficient handling, after escriptcore/test/python/test_linearPDEs.py
 # (Test_LinearPDE: test_setCoefficient_*_Scalar / _System, test_reducedOn,
 # test_setCoefficient_WithIllegalFunctionSpace, test_resetCoefficient_WithWrongShape)
