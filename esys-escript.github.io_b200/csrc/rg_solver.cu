@@ -1267,6 +1267,51 @@ __global__ void __launch_bounds__(kThreads) k_f32_cg_seed_coef(const __grid_cons
     }
 }
 
+// k_cheb_step on the element-coefficient operator (when the FP32 solve evaluates its operator
+// from the coefficients there is no band copy): the balanced operator is bv_i sum_j a_ij bv_j
+// x_j with a_ij from kappa (FP32 coefficients, FP64 vectors); rows and columns of fixed nodes
+// (the sign bit of khat) are those of the identity.
+template <int NB>
+__global__ void __launch_bounds__(kThreads) k_cheb_step_coef(const __grid_constant__ CgArgs ca,
+                                                             const float* __restrict__ khat,
+                                                             const double* __restrict__ bv,
+                                                             const double* __restrict__ dinv,
+                                                             const double* __restrict__ x,
+                                                             const double* __restrict__ bb, double c_d, double c_r,
+                                                             double* __restrict__ d, double* __restrict__ y)
+{
+    constexpr int NK = NB == 27 ? 8 : 4;
+    const int64_t n = ca.n;
+    for (int64_t i = gtid(); i < n; i += gstride()) {
+        float kv[8];
+#pragma unroll
+        for (int j = 0; j < NK; ++j) kv[j] = __ldg(khat + i + ca.kdelta[j]);
+        const bool fixed = (__float_as_uint(kv[0]) >> 31) != 0;
+#pragma unroll
+        for (int j = 0; j < NK; ++j) kv[j] = fabsf(kv[j]);
+#pragma unroll
+        for (int j = NK; j < 8; ++j) kv[j] = 0.f;
+        CoefRow cr;
+        coef_row<NB>(kv, cr);
+        double acc;
+        if (fixed) {
+            acc = x[i];
+        } else {
+            acc = 0.0;
+#pragma unroll
+            for (int b = 0; b < NB; ++b) {
+                const float c = coef_at<NB>(cr, ca.T, b);
+                const int64_t j = min(max(i + ca.off[b], (int64_t)0), n - 1);
+                if (c != 0.f && (__float_as_uint(__ldg(khat + j)) >> 31) == 0) acc = fma((double)c, bv[j] * x[j], acc);
+            }
+            acc *= bv[i];
+        }
+        const double dn = c_d * (c_d != 0.0 ? d[i] : 0.0) + c_r * dinv[i] * (bb[i] - acc);
+        d[i] = dn;
+        y[i] = x[i] + dn;
+    }
+}
+
 // x64 += scale * d32 / bv (the element-coefficient operator's correction is unbalanced); d32 = 0
 __global__ void k_fold_correction_unbalance(int64_t n, double* __restrict__ x, float* __restrict__ d,
                                             const double* __restrict__ bv, double scale)
@@ -2343,7 +2388,16 @@ int solve_impl(Matrix* m, const double* rhs, double* x, const rg_solver_opts* o,
                         c_r = 2.0 * rho_n / delta;
                         rho = rho_n;
                     }
-                    if (m->band32 && m->band32_ok) {
+                    if (w->coef_op) {
+                        // the operator from the element coefficients (no band copy on this path)
+                        const CgArgs ca = cg_args(dm);
+                        if (dm->nbands == 27)
+                            RG_TIMED(T_VECTOR, (k_cheb_step_coef<27><<<eg, kThreads, 0, stream()>>>(
+                                                   ca, m->coef.khat, m->bv, m->dinv, src, w->bb, c_d, c_r, w->z, dst)));
+                        else
+                            RG_TIMED(T_VECTOR, (k_cheb_step_coef<9><<<eg, kThreads, 0, stream()>>>(
+                                                   ca, m->coef.khat, m->bv, m->dinv, src, w->bb, c_d, c_r, w->z, dst)));
+                    } else if (m->band32 && m->band32_ok) {
                         // the FP32 band copy streams a third of the bytes of the FP64 CSR
                         TmaBandArgs ta{};
                         for (int b = 0; b < dm->nbands; ++b) ta.off[b] = (int)dm->band_off[b];

@@ -172,6 +172,156 @@ __global__ void __launch_bounds__(kConvThreads) k_conv3(const __grid_constant__ 
     if (bad && threadIdx.x == 0) atomicOr(a.err, 1);
 }
 
+// ------------------------------------------------------------------ box-reuse forward convolution
+// The same convolution for grids whose tiles are 8 (w) x 16 (h) x 2 (z) output positions and
+// Cout <= 64.  A GEMM row is an output position, w fastest, so one 256-byte atom of the
+// 32-byte-swizzled K-major operand is one h-row of 8 positions.  A tap's h and z shifts then
+// move the operand by whole atoms: the A operand of tap (kw, kh, kd) for output slice zz is
+// 16 consecutive atoms of an input box that the producer loads once per 16-channel chunk and
+// per kw (8 x 18 x 4 positions: the tile plus its h and z halo), starting at atom
+// kh + 18 (kd + zz).  Per chunk: 3 TMA boxes (55 KB) and the chunk's 27 weight slices instead
+// of 27 shifted 4 KB boxes per 128 positions, and 54 UMMAs (two 128 x Cout accumulators in
+// tensor memory, one per output z slice).
+constexpr int kBoxW = 8, kBoxH = 16, kBoxZ = 2;
+constexpr int kBoxRows = kBoxW * (kBoxH + 2) * (kBoxZ + 2);  // 576 input positions per kw box
+constexpr int kBoxBytes = kBoxRows * 32;                      // 18 KB
+constexpr int kBoxA = 3 * kBoxBytes;                          // the three kw boxes
+
+template <int COUT, int S>
+struct BoxSmem {
+    static constexpr int kB = 27 * COUT * 32;  // the chunk's weight slices of every tap
+    static constexpr int kStage = (kBoxA + kB + 1023) / 1024 * 1024;
+    static constexpr int kBytes = S * kStage + 1024;  // + alignment slack
+};
+
+template <int COUT, int S>
+__global__ void __launch_bounds__(kConvThreads) k_conv3_box(const __grid_constant__ ConvArgs a)
+{
+    using M = BoxSmem<COUT, S>;
+    constexpr int kTmemCols = 2 * COUT <= 32 ? 32 : (2 * COUT <= 64 ? 64 : 128);
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    __shared__ __align__(8) uint64_t full[S], empty[S], acc_full;
+    __shared__ uint32_t tmem_slot;
+    __shared__ int bad;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    int tile = blockIdx.x;
+    const int tw = tile % a.tiles_w;
+    tile /= a.tiles_w;
+    const int th = tile % a.tiles_h;
+    const int tz = tile / a.tiles_h;
+    const int per_sample = a.D / kBoxZ;
+    const int w0 = tw * kBoxW, h0 = th * kBoxH;
+    const int z0 = (tz / per_sample) * (a.D + 2) + 1 + (tz % per_sample) * kBoxZ;
+    const int chunks = a.Cin / 16;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < S; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(&acc_full, 1);
+        bad = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        tmem_alloc(&tmem_slot, kTmemCols);
+        tmem_relinquish();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = tmem_slot;
+
+    if (warp == 0 && lane == 0) {
+        // ---------------- producer: per chunk the three kw boxes and the 27 weight slices
+        for (int k = 0; k < chunks; ++k) {
+            const int s = k % S;
+            if (k >= S && !mbar_wait(&empty[s], (uint32_t)(((k / S) - 1) & 1))) {
+                bad = 1;
+                break;
+            }
+            uint8_t* st = smem + s * M::kStage;
+            mbar_expect_tx(&full[s], kBoxA + M::kB);
+            for (int kw = 0; kw < 3; ++kw)
+                tma_load_4d(st + kw * kBoxBytes, &a.xmap, k * 16, w0 + kw - 1, h0 - 1, z0 - 1, &full[s]);
+            for (int t = 0; t < 27; ++t) tma_load_2d(st + kBoxA + t * COUT * 32, &a.wmap, k * 16, t * COUT, &full[s]);
+        }
+    } else if (warp == 1 && lane == 0) {
+        // ---------------- MMA issuer
+        constexpr uint32_t idesc = idesc_bf16(COUT, 0, 0);
+        bool ok = true;
+        for (int k = 0; k < chunks; ++k) {
+            const int s = k % S;
+            if (!mbar_wait(&full[s], (uint32_t)((k / S) & 1))) {
+                bad = 1;
+                ok = false;
+                break;
+            }
+            tc_fence_after();
+            const uint8_t* st = smem + s * M::kStage;
+#pragma unroll 1
+            for (int zz = 0; zz < kBoxZ; ++zz)
+#pragma unroll 1
+                for (int t = 0; t < 27; ++t) {
+                    const int kw = t % 3, kh = (t / 3) % 3, kd = t / 9;
+                    const uint64_t ad = smem_desc(st + kw * kBoxBytes + (kh + (kBoxH + 2) * (kd + zz)) * 256, 16, 256,
+                                                  LAYOUT_SW32);
+                    const uint64_t bd = smem_desc(st + kBoxA + t * COUT * 32, 16, 256, LAYOUT_SW32);
+                    umma_f16(tmem + (uint32_t)(zz * COUT), ad, bd, idesc, (k > 0 || t > 0) ? 1u : 0u);
+                }
+            umma_commit(&empty[s]);
+        }
+        if (ok) umma_commit(&acc_full);
+    } else if (warp >= 2) {
+        // ---------------- epilogue: TMEM lane quarter (warp % 4) -> 32 output positions
+        const int q = warp & 3;
+        const int m = 32 * q + lane;  // GEMM row: w = m % 8, h = m / 8
+        const bool ready = __all_sync(0xffffffffu, mbar_wait(&acc_full, 0));
+        tc_fence_after();
+        if (!ready) {
+            bad = 1;
+        } else {
+            const int w = w0 + (m % kBoxW);
+            const int h = h0 + m / kBoxW;
+#pragma unroll 1
+            for (int zz = 0; zz < kBoxZ; ++zz) {
+                const size_t row = ((size_t)(z0 + zz) * a.H + h) * a.W + w;
+                __nv_bfloat16* o = a.out + row * COUT;
+                const __nv_bfloat16* mk = a.mask ? a.mask + row * COUT : nullptr;
+#pragma unroll
+                for (int c0 = 0; c0 < COUT; c0 += 16) {
+                    float v[16];
+                    tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(zz * COUT + c0), v);
+                    __align__(16) __nv_bfloat16 ob[16];
+                    __align__(16) __nv_bfloat16 mb[16];
+                    if (mk) {
+                        *reinterpret_cast<uint4*>(mb) = *reinterpret_cast<const uint4*>(mk + c0);
+                        *reinterpret_cast<uint4*>(mb + 8) = *reinterpret_cast<const uint4*>(mk + c0 + 8);
+                    }
+#pragma unroll
+                    for (int i = 0; i < 16; ++i) {
+                        float x = v[i] + (a.bias ? a.bias[c0 + i] : 0.f);
+                        if (a.relu) x = fmaxf(x, 0.f);
+                        if (mk && !(__bfloat162float(mb[i]) > 0.f)) x = 0.f;
+                        ob[i] = __float2bfloat16_rn(x);
+                    }
+                    *reinterpret_cast<uint4*>(o + c0) = *reinterpret_cast<const uint4*>(ob);
+                    *reinterpret_cast<uint4*>(o + c0 + 8) = *reinterpret_cast<const uint4*>(ob + 8);
+                }
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        tc_fence_after();
+        tmem_dealloc(tmem, kTmemCols);
+    }
+    if (bad && threadIdx.x == 0) atomicOr(a.err, 1);
+}
+
 // ------------------------------------------------------------------ weight gradient
 // dW[tap][co][ci] = sum_pos X[pos + off(tap)][ci] * G[pos][co] as a GEMM with
 //   M = 128 rows = 8 (tap, 16-channel chunk) pairs x 16 channels,  N = Cout,  K = positions.
@@ -379,6 +529,28 @@ int make_act_map(CUtensorMap* map, const void* base, int C, int W, int H, int Z,
     return RG_OK;
 }
 
+// activation map with the box-reuse kernel's input box (16, 8, 18, 4), 32-byte swizzle
+int make_box_map(CUtensorMap* map, const void* base, int C, int W, int H, int Z)
+{
+    EncodeTiled enc;
+    int rc = encode_fn(&enc);
+    if (rc) return rc;
+    RG_REQUIRE(C % 16 == 0, "activation map: C must be a multiple of 16");
+    RG_REQUIRE((reinterpret_cast<uintptr_t>(base) & 15) == 0, "activation map: base must be 16-byte aligned");
+    cuuint64_t dims[4] = {(cuuint64_t)C, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)Z};
+    cuuint64_t strides[3] = {(cuuint64_t)C * 2, (cuuint64_t)W * C * 2, (cuuint64_t)H * W * C * 2};
+    cuuint32_t box[4] = {16, (cuuint32_t)kBoxW, (cuuint32_t)(kBoxH + 2), (cuuint32_t)(kBoxZ + 2)};
+    cuuint32_t es[4] = {1, 1, 1, 1};
+    CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void*>(base), dims, strides, box, es,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_32B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        set_error("cuTensorMapEncodeTiled (activation box) failed with code " + std::to_string((int)r));
+        return RG_CUDA_ERROR;
+    }
+    return RG_OK;
+}
+
 // weight map: [rows][K] bf16 (K contiguous), box (16, box_rows), 32-byte swizzle
 int make_weight_map(CUtensorMap* map, const void* base, int K, int rows, int box_rows)
 {
@@ -425,6 +597,27 @@ int launch_conv3(ConvArgs& a, int ntiles)
     return RG_OK;
 }
 
+template <int COUT, int S>
+int launch_conv3_box(ConvArgs& a, int ntiles)
+{
+    static bool attr = false;
+    if (!attr) {
+        RG_CHECK_CUDA(cudaFuncSetAttribute(k_conv3_box<COUT, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           BoxSmem<COUT, S>::kBytes));
+        attr = true;
+    }
+    RG_TIMED(T_WS_CONV, (k_conv3_box<COUT, S><<<ntiles, kConvThreads, BoxSmem<COUT, S>::kBytes, stream()>>>(a)));
+    RG_CHECK_LAUNCH();
+    return RG_OK;
+}
+
+template <int COUT>
+int launch_conv3_box_any(ConvArgs& a, int ntiles)
+{
+    // one stage when there is one chunk (several CTAs per SM overlap instead), else two
+    return a.Cin == 16 ? launch_conv3_box<COUT, 1>(a, ntiles) : launch_conv3_box<COUT, 2>(a, ntiles);
+}
+
 template <int COUT>
 int launch_wgrad(WgradArgs& a, int grid)
 {
@@ -464,12 +657,41 @@ extern "C" int rg_ws_conv3(const rg_act* x, const void* weights, const float* bi
                "rg_ws_conv3: output channels must be 16, 32, 48, 64, 80, 112 or 128");
     RG_REQUIRE(!mask || (mask->c == cout && mask->n == y->n && mask->d == y->d && mask->h == y->h && mask->w == y->w),
                "rg_ws_conv3: mask shape must equal the output shape");
+    ws::ConvArgs a;
+    const int Z = x->n * (x->d + 2);
+    if (x->w % ws::kBoxW == 0 && x->h % ws::kBoxH == 0 && x->d % ws::kBoxZ == 0 && cout <= 64) {
+        // box-reuse kernel: 8 x 16 x 2 output tiles, the input box loaded once per kw and chunk
+        int rc = ws::make_box_map(&a.xmap, x->ptr, x->c, x->w, x->h, Z);
+        if (rc) return rc;
+        rc = ws::make_weight_map(&a.wmap, weights, x->c, 27 * cout, cout);
+        if (rc) return rc;
+        a.bias = bias;
+        a.out = static_cast<__nv_bfloat16*>(y->ptr);
+        a.mask = mask ? static_cast<const __nv_bfloat16*>(mask->ptr) : nullptr;
+        a.W = x->w;
+        a.H = x->h;
+        a.D = x->d;
+        a.Cin = x->c;
+        a.BW = ws::kBoxW;
+        a.BH = ws::kBoxH;
+        a.BZ = ws::kBoxZ;
+        a.tiles_w = x->w / ws::kBoxW;
+        a.tiles_h = x->h / ws::kBoxH;
+        a.tiles_z = x->n * x->d / ws::kBoxZ;
+        a.relu = relu;
+        a.err = err_dev;
+        const int ntiles = a.tiles_w * a.tiles_h * a.tiles_z;
+        switch (cout) {
+        case 16: return ws::launch_conv3_box_any<16>(a, ntiles);
+        case 32: return ws::launch_conv3_box_any<32>(a, ntiles);
+        case 48: return ws::launch_conv3_box_any<48>(a, ntiles);
+        default: return ws::launch_conv3_box_any<64>(a, ntiles);
+        }
+    }
     int bw, bh, bz;
     ws::tile_box(x->w, x->h, x->d, &bw, &bh, &bz);
     RG_REQUIRE(x->w % bw == 0 && x->h % bh == 0 && x->d % bz == 0 && bw * bh * bz == 128,
                "rg_ws_conv3: spatial sizes must tile into 128-position boxes");
-    ws::ConvArgs a;
-    const int Z = x->n * (x->d + 2);
     int rc = ws::make_act_map(&a.xmap, x->ptr, x->c, x->w, x->h, Z, bw, bh, bz, 128);
     if (rc) return rc;
     rc = ws::make_weight_map(&a.wmap, weights, x->c, 27 * cout, cout);

@@ -247,3 +247,25 @@ def test_fp64_solves_refuse_the_coefficient_layout(cuda):
     case = Case(3, (6, 5, 4), seed=10)
     st, _, _ = case.solve(precision=L.RG_PREC_FP64)
     assert st == L.RG_NOT_SUPPORTED
+
+
+def test_guess_smoothing_on_the_coefficient_operator(cuda):
+    """Chebyshev smoothing of an initial guess (standard mode) runs on the coefficient operator
+    when the band copy is not built: the smoothed guess's residual equals the one smoothed on
+    the band copy (both FP32 operators, FP64 vectors) to FP32 accuracy, fixed nodes included,
+    and both solves meet the tolerance."""
+    case = Case(3, (36, 30, 24), seed=12, qmode="scatter")
+    rng = np.random.default_rng(13)
+    ref = case.reference()
+    g = torch.tensor(ref * (1.0 + 0.3 * rng.standard_normal(case.d.n)), device="cuda")
+    res = {}
+    for layout in (L.RG_LAYOUT_COEF, L.RG_LAYOUT_BAND):
+        o = R.opts(tolerance=1e-10, **{**COEF, "layout": layout})
+        o.initial_guess = g.data_ptr()
+        o.guess_sweeps = 8
+        x = torch.zeros(case.d.n, dtype=torch.float64, device="cuda")
+        st, dg = R.solve(case.m, case.rhs, x, o)
+        assert st == 0 and dg.converged and not dg.fp64_fallback
+        assert rel(x.cpu().numpy(), ref) < 1e-8
+        res[layout] = dg.guess_residual
+    assert abs(res[L.RG_LAYOUT_COEF] - res[L.RG_LAYOUT_BAND]) <= 1e-4 * res[L.RG_LAYOUT_BAND]
