@@ -264,6 +264,8 @@ def run_ours(args):
         return o
 
     fast = opts(L.RG_MODE_STANDARD, L.RG_PREC_FP32_REFINE)
+    if args.inner == "band":  # profiling runs: the FP32 iterations on the band copy
+        fast.layout = L.RG_LAYOUT_BAND
     if args.inner_tol > 0:
         fast.inner_tolerance = args.inner_tol
     plain = opts(L.RG_MODE_PASO, L.RG_PREC_FP64)
@@ -797,8 +799,12 @@ def main():
     ap.add_argument("--no-batched", dest="batched", action="store_false",
                     help="skip the batched 64-system workload")
     ap.add_argument("--spmv-config", type=int, choices=[-1, 0, 1], default=-1,
-                    help="FP32 SpMV pipeline: -1 tuned (default), 0 = 3 stages x 1 CTA/SM, "
+                    help="FP32 iteration pipeline: -1 tuned (default); band copy 0 = 3 stages x 1 CTA/SM, "
+                         "1 = 2 stages x 2 CTAs/SM; element coefficients 0 = 3 stages x 2 CTAs/SM, "
                          "1 = 2 stages x 2 CTAs/SM")
+    ap.add_argument("--inner", choices=["coef", "band"], default="coef",
+                    help="operator of the FP32 iterations of --path fp32 (--only fast profiling "
+                         "runs): element coefficients (the timed path) or the FP32 band copy")
     ap.add_argument("--only", choices=["all", "fast", "plain", "plain_band"], default="all",
                     help="profiling runs: only the fast path, or only the plain FP64 paso solve "
                          "(CSR, or the FP64 band copy)")

@@ -1,11 +1,13 @@
 """Both pipeline configurations of the fused FP32 iteration of the FP32_REFINE solve, forced
-one at a time through rg_solver_set_config (0: 3 stages x 1 CTA/SM, 1: 2 stages x 2
-CTAs/SM), on Bricks and Rectangles with interior and ragged edge tiles, with one window per
-stencil plane (short x-lines) and one per stencil column (x-lines longer than a tile).  Each solution is within 1e-7 relative
-of the FP64 PCG solution at tol 1e-10, the forced configuration is the one used, and the
-iteration counts agree within 3% (an inner operator that differed from A would show as
-extra iterations or an FP64 fallback, since the FP64 refinement still drives the true
-residual down)."""
+one at a time through rg_solver_set_config, for both inner operators: the band copy (0: 3
+stages x 1 CTA/SM, 1: 2 stages x 2 CTAs/SM) and the element coefficients (0: 3 stages x 2
+CTAs/SM, 1: 2 stages x 2 CTAs/SM).  On Bricks and Rectangles with interior and ragged edge
+tiles, with one window per stencil plane (short x-lines) and one per stencil column (x-lines
+longer than a tile).
+Each solution is within 1e-7 relative of the FP64 PCG solution at tol 1e-10, the forced
+configuration is the one used, and the iteration counts agree within 3% (an inner operator
+that differed from A would show as extra iterations or an FP64 fallback, since the FP64
+refinement still drives the true residual down)."""
 import ctypes as C
 
 import numpy as np
@@ -45,8 +47,9 @@ def _config(m):
     return cfg.value, ug.value, list(us)
 
 
-@pytest.mark.parametrize("ne", [(40, 33, 27), (64, 48, 33), (7, 5, 130), (300, 211)])
-def test_forced_spmv_configs_agree(cuda, ne):
+@pytest.mark.parametrize("layout", [L.RG_LAYOUT_BAND, L.RG_LAYOUT_COEF], ids=["band", "coef"])
+@pytest.mark.parametrize("ne", [(40, 33, 27), (64, 48, 33), (7, 5, 130), (300, 211), (300, 9, 8), (96, 64, 70)])
+def test_forced_spmv_configs_agree(cuda, ne, layout):
     d, m64, rhs = _problem(ne, seed=11)
     x64 = torch.zeros(d.n, dtype=torch.float64, device="cuda")
     st, _ = R.solve(m64, rhs.clone(), x64, R.opts(tolerance=1e-10, precision=L.RG_PREC_FP64))
@@ -58,14 +61,21 @@ def test_forced_spmv_configs_agree(cuda, ne):
         assert _config(m)[0] == -1  # not tuned before the first FP32 solve
         L.check(R.lib().rg_solver_set_config(m.h, cfg))
         x = torch.zeros(d.n, dtype=torch.float64, device="cuda")
-        st, dg = R.solve(m, b, x, R.opts(tolerance=1e-10, precision=L.RG_PREC_FP32_REFINE))
+        st, dg = R.solve(m, b, x, R.opts(tolerance=1e-10, precision=L.RG_PREC_FP32_REFINE, layout=layout))
+        if st == L.RG_INVALID_ARG:
+            # the configuration's shared memory does not reach its CTAs per SM on this grid
+            assert "does not fit" in L.last_error()
+            continue
         assert st == 0 and dg.converged and not dg.fp64_fallback
+        assert dg.inner_operator == (1 if layout == L.RG_LAYOUT_COEF else 0)
         used, ug, us = _config(m)
         assert used == cfg and ug == 0  # one kernel per iteration: no separate update grid
-        assert all(v > 0 for v in us)  # the tuner timed both configurations
+        assert us[cfg] > 0  # the tuner timed the configuration it was given
         err = np.linalg.norm(x.cpu().numpy() - ref) / np.linalg.norm(ref)
         assert err < 1e-7, (cfg, err)
         iters[cfg] = int(dg.num_iter)
+    # long x-lines in 3D (one window per stencil column) leave room for one configuration only
+    assert len(iters) == (1 if len(ne) == 3 and ne[0] >= 258 else 2), iters
     assert max(iters.values()) <= min(iters.values()) * 1.03 + 2, iters
 
 
