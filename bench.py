@@ -517,12 +517,13 @@ def run_ours(args):
     peak_note = "of measured" if hbm else "of fallback"
     hbm = hbm or 6650.0
     achieved = algo_bytes / avg_s / 1e9 if avg_s > 0 else 0.0
-    traffic = None
+    # DRAM bytes per launch of the same kernel from one ncu capture (profiles/traffic.json)
+    tr_all = {}
     tr_path = os.path.join(REPO, "profiles", "traffic.json")
     if os.path.exists(tr_path):
-        tr = json.load(open(tr_path)).get("f32_spmv")
-        if tr and tr.get("ne") == ne:
-            traffic = tr.get("bytes_per_launch")
+        tr_all = {k: v for k, v in json.load(open(tr_path)).items() if v.get("ne") == ne}
+    tr = tr_all.get("f32_cg_coef" if coef_used else "f32_cg_band", {})
+    traffic, limiter = tr.get("bytes_per_launch"), tr.get("limiter")
     roofline = {"bound": "hbm",
                 "kernel": ("k_f32_cg<27, element coefficients> (one fused FP32 PCG iteration: operator from kappa per "
                            "element, vector updates, one reduction)" if coef_used else
@@ -531,8 +532,20 @@ def run_ours(args):
                 "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
                 "frac": round(achieved / hbm, 4), "peak_source": peak_note,
                 "algorithmic_bytes_per_launch": algo_bytes, "avg_launch_us": round(avg_s * 1e6, 2),
-                "launches_timed": spmv_t, "traffic": traffic,
+                "launches_timed": spmv_t, "traffic": traffic, "limiter": limiter,
                 "timing": f"CUDA events around each launch over {n_prof} steps (graphs off: {ms_events:.1f} ms/step)"}
+
+    # the pipeline configuration the tuner chose for the timed path's operator (read before
+    # another solve switches the matrix's workspace to another operator)
+    cfg, ug = C.c_int(), C.c_int()
+    spmv_us = (C.c_double * 2)()
+    lib.rg_solver_config(mat, C.byref(cfg), C.byref(ug), spmv_us)
+    spmv_names = ({0: "k_f32_cg<27, element coefficients, 3 stages x 2 CTAs/SM>",
+                   1: "k_f32_cg<27, element coefficients, 2 stages x 2 CTAs/SM>"} if coef_used else
+                  {0: "k_f32_cg<27, band, 3 stages x 1 CTA/SM>", 1: "k_f32_cg<27, band, 2 stages x 2 CTAs/SM>"})
+    roofline["kernel"] = spmv_names.get(cfg.value, roofline["kernel"])
+    roofline["tuned"] = {"spmv_config": cfg.value, "update_grid": ug.value,
+                         "spmv_us_per_config": [round(v, 2) for v in spmv_us]}
 
     # --- textbook FP64 PCG on the same input (information: iteration count of CG without smoothing)
     d_std = step(opts(L.RG_MODE_STANDARD, L.RG_PREC_FP64))
@@ -627,20 +640,12 @@ def run_ours(args):
 
     kernels = {k: {"launches_per_step": v[0] // n_prof, "ms_per_step": round(v[2] / n_prof, 3)}
                for k, v in tm.items() if v[0]}
-    cfg, ug = C.c_int(), C.c_int()
-    spmv_us = (C.c_double * 2)()
-    lib.rg_solver_config(mat, C.byref(cfg), C.byref(ug), spmv_us)
-    spmv_names = ({0: "k_f32_cg<27, element coefficients, 3 stages x 2 CTAs/SM>",
-                   1: "k_f32_cg<27, element coefficients, 2 stages x 2 CTAs/SM>"} if coef_used else
-                  {0: "k_f32_cg<27, band, 3 stages x 1 CTA/SM>", 1: "k_f32_cg<27, band, 2 stages x 2 CTAs/SM>"})
-    roofline["kernel"] = spmv_names.get(cfg.value, roofline["kernel"])
     band_bytes = F32_SPMV_BYTES_PER_ROW * n
     roofline_band = {"kernel": "k_f32_cg<27, band> (the same iteration streaming the FP32 band copy)",
                      "algorithmic_bytes_per_launch": band_bytes, "avg_launch_us": round(band_us, 2),
                      "achieved": round(band_bytes / (band_us * 1e-6) / 1e9, 1), "peak": hbm, "unit": "GB/s",
-                     "frac": round(band_bytes / (band_us * 1e-6) / 1e9 / hbm, 4), "peak_source": peak_note}
-    roofline["tuned"] = {"spmv_config": cfg.value, "update_grid": ug.value,
-                         "spmv_us_per_config": [round(v, 2) for v in spmv_us]}
+                     "frac": round(band_bytes / (band_us * 1e-6) / 1e9 / hbm, 4), "peak_source": peak_note,
+                     "traffic": tr_all.get("f32_cg_band", {}).get("bytes_per_launch")}
 
     # --- batched workload: 64 Bricks with edges from {32,48,64,80,96} per axis, 8 right hand
     # sides each, FP32-inner/FP64-refinement PCG to rtol 1e-8, one batch (timed separately)

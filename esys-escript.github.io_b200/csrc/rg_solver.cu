@@ -973,16 +973,6 @@ __device__ __forceinline__ float coef_at(const CoefRow& r, const float (&T)[8], 
     return T[NB == 27 ? band_class(b) : (band_class(b) & 3)] * ksum_at<NB>(r, b);
 }
 
-// Fused FP32 PCG iteration, two operators:
-//   COEF = false: the tile's band block (FP32 copy of the balanced matrix) is bulk-copied with
-//                 the state windows; the diagonal is its centre band.
-//   COEF = true:  the operator is evaluated from the element coefficients (unbalanced A; the
-//                 Jacobi-preconditioned iteration is the same for any symmetric diagonal scaling
-//                 of the matrix, so the balancing is applied only where the FP64 refinement
-//                 hands residuals and corrections over): windows of khat replace the band
-//                 block (4 instead of 108 bytes per row).  Rows of nodes fixed by the constraint
-//                 are identity rows, solved exactly by the seed; their state stays zero, so
-//                 their columns drop out of every other row without a mask.
 // The scalars of the next FP32 iteration from the six sums of one (the grid reduction's result,
 // thread 0 of the last CTA): a, b, r.u and the stopping test.
 __device__ void cg_scalars(Scal* s, const double* tt, int mode)
@@ -1024,6 +1014,16 @@ __device__ void cg_scalars(Scal* s, const double* tt, int mode)
     }
 }
 
+// Fused FP32 PCG iteration, two operators:
+//   COEF = false: the tile's band block (FP32 copy of the balanced matrix) is bulk-copied with
+//                 the state windows; the diagonal is its centre band.
+//   COEF = true:  the operator is evaluated from the element coefficients (unbalanced A; the
+//                 Jacobi-preconditioned iteration is the same for any symmetric diagonal scaling
+//                 of the matrix, so the balancing is applied only where the FP64 refinement
+//                 hands residuals and corrections over): windows of khat replace the band
+//                 block (4 instead of 108 bytes per row).  Rows of nodes fixed by the constraint
+//                 are identity rows, solved exactly by the seed; their state stays zero, so
+//                 their columns drop out of every other row without a mask.
 template <int NB, int kStages, int kCtas, bool COEF>
 __global__ void __launch_bounds__(kTile + 32, kCtas) k_f32_cg(const float* __restrict__ band,
                                                               const __grid_constant__ CgArgs ca,
