@@ -152,8 +152,6 @@ __device__ __forceinline__ int64_t gstride() { return (int64_t)gridDim.x * block
 
 __device__ __forceinline__ double2 ld2(const double* p, int64_t v) { return reinterpret_cast<const double2*>(p)[v]; }
 __device__ __forceinline__ void st2(double* p, int64_t v, double2 a) { reinterpret_cast<double2*>(p)[v] = a; }
-__device__ __forceinline__ float4 ld4(const float* p, int64_t v) { return reinterpret_cast<const float4*>(p)[v]; }
-__device__ __forceinline__ void st4(float* p, int64_t v, float4 a) { reinterpret_cast<float4*>(p)[v] = a; }
 
 // CSR row-group loop: each group of kLpr lanes owns one row per trip; the trip count is
 // uniform over a warp so the shuffles stay converged.
@@ -289,11 +287,6 @@ __global__ void __launch_bounds__(kThreads) k_gershgorin(int64_t n, const int32_
     }
     double t[1];
     if (grid_reduce<1, 1u>(v, rb, t) && threadIdx.x == 0) *out = t[0];
-}
-
-__global__ void k_fill32(int64_t n, float* __restrict__ a, float v)
-{
-    for (int64_t i = gtid(); i < n; i += gstride()) a[i] = v;
 }
 
 __global__ void k_mul(int64_t n, const double* __restrict__ a, const double* __restrict__ b,

@@ -16,6 +16,7 @@
 // apply ReLU and/or the ReLU mask of the layer below (data gradient), and store bf16.
 #include <cuda.h>
 
+#include <algorithm>
 #include <string>
 
 #include "rg_internal.cuh"
@@ -198,7 +199,9 @@ template <int COUT, int S>
 __global__ void __launch_bounds__(kConvThreads) k_conv3_box(const __grid_constant__ ConvArgs a)
 {
     using M = BoxSmem<COUT, S>;
-    constexpr int kTmemCols = 2 * COUT <= 32 ? 32 : (2 * COUT <= 64 ? 64 : 128);
+    constexpr int kAcc = kBoxZ * COUT;  // TMEM columns: one accumulator per output z slice
+    constexpr int kTmemCols = kAcc <= 32 ? 32 : (kAcc <= 64 ? 64 : (kAcc <= 128 ? 128 : 256));
+    static_assert(kAcc <= 256, "the accumulators must fit 256 TMEM columns");
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     __shared__ __align__(8) uint64_t full[S], empty[S], acc_full;
@@ -261,14 +264,18 @@ __global__ void __launch_bounds__(kConvThreads) k_conv3_box(const __grid_constan
             }
             tc_fence_after();
             const uint8_t* st = smem + s * M::kStage;
-#pragma unroll 1
-            for (int zz = 0; zz < kBoxZ; ++zz)
-#pragma unroll 1
-                for (int t = 0; t < 27; ++t) {
+            // the output slices' accumulations alternate: consecutive UMMAs are independent; the
+            // descriptors are the stage's plus constant offsets (the loops unroll), so that the
+            // one issuing thread spends a few instructions per UMMA
+            const uint64_t ad0 = smem_desc(st, 16, 256, LAYOUT_SW32);
+            const uint64_t bd0 = smem_desc(st + kBoxA, 16, 256, LAYOUT_SW32);
+#pragma unroll
+            for (int t = 0; t < 27; ++t)
+#pragma unroll
+                for (int zz = 0; zz < kBoxZ; ++zz) {
                     const int kw = t % 3, kh = (t / 3) % 3, kd = t / 9;
-                    const uint64_t ad = smem_desc(st + kw * kBoxBytes + (kh + (kBoxH + 2) * (kd + zz)) * 256, 16, 256,
-                                                  LAYOUT_SW32);
-                    const uint64_t bd = smem_desc(st + kBoxA + t * COUT * 32, 16, 256, LAYOUT_SW32);
+                    const uint64_t ad = desc_add(ad0, kw * kBoxBytes + (kh + (kBoxH + 2) * (kd + zz)) * 256);
+                    const uint64_t bd = desc_add(bd0, t * COUT * 32);
                     umma_f16(tmem + (uint32_t)(zz * COUT), ad, bd, idesc, (k > 0 || t > 0) ? 1u : 0u);
                 }
             umma_commit(&empty[s]);
@@ -311,6 +318,199 @@ __global__ void __launch_bounds__(kConvThreads) k_conv3_box(const __grid_constan
                     *reinterpret_cast<uint4*>(o + c0 + 8) = *reinterpret_cast<const uint4*>(ob + 8);
                 }
             }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        tc_fence_after();
+        tmem_dealloc(tmem, kTmemCols);
+    }
+    if (bad && threadIdx.x == 0) atomicOr(a.err, 1);
+}
+
+// ------------------------------------------------------------------ persistent box-reuse forward convolution
+// k_conv3_box's tiles and operands, with each CTA walking tiles blockIdx.x, + gridDim.x, ...:
+// the weights of every 16-channel chunk are loaded once and stay in shared memory, the input
+// boxes of consecutive (tile, chunk) steps stream through an S-stage ring, and the
+// accumulators of consecutive tiles alternate between two TMEM buffers, so that the box loads
+// of the next tile, its UMMAs and the epilogue of the previous tile overlap (k_conv3_box runs
+// the three one after the other, once per CTA).  Every wait is bounded; a wait that runs out
+// sets the error flag and the CTA stops.
+template <int COUT>
+struct BoxPSmem {
+    static constexpr int kB = 27 * COUT * 32;                 // one chunk's weight slices
+    static constexpr int kBPad = (kB + 1023) / 1024 * 1024;
+    static constexpr int bytes(int chunks, int stages) { return chunks * kBPad + stages * kBoxA + 1024; }
+};
+
+template <int COUT, int S>
+__global__ void __launch_bounds__(kConvThreads) k_conv3_boxp(const __grid_constant__ ConvArgs a)
+{
+    using M = BoxPSmem<COUT>;
+    constexpr int kAcc = kBoxZ * COUT;  // TMEM columns of one tile (one accumulator per output z slice)
+    constexpr int kTmemCols =
+        2 * kAcc <= 32 ? 32 : (2 * kAcc <= 64 ? 64 : (2 * kAcc <= 128 ? 128 : (2 * kAcc <= 256 ? 256 : 512)));
+    static_assert(2 * kAcc <= 512, "two tiles' accumulators must fit the 512 TMEM columns");
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    __shared__ __align__(8) uint64_t full[S], empty[S], wfull, acc_full[2], acc_empty[2];
+    __shared__ uint32_t tmem_slot;
+    __shared__ int bad;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int chunks = a.Cin / 16;
+    const int ntiles = a.tiles_w * a.tiles_h * a.tiles_z;
+    const int per_sample = a.D / kBoxZ;
+    uint8_t* wsm = smem;                             // chunks x kBPad: the weights
+    uint8_t* ring = smem + chunks * M::kBPad;        // S x kBoxA: the input boxes
+    // origin of tile `tile`: first output w, h and the row z of its first output slice
+    auto origin = [&](int tile, int& w0, int& h0, int& z0) {
+        const int tw = tile % a.tiles_w;
+        tile /= a.tiles_w;
+        const int th = tile % a.tiles_h;
+        const int tz = tile / a.tiles_h;
+        w0 = tw * kBoxW;
+        h0 = th * kBoxH;
+        z0 = (tz / per_sample) * (a.D + 2) + 1 + (tz % per_sample) * kBoxZ;
+    };
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < S; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(&wfull, 1);
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&acc_full[b], 1);
+            mbar_init(&acc_empty[b], 4);  // the four epilogue warps
+        }
+        bad = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        tmem_alloc(&tmem_slot, kTmemCols);
+        tmem_relinquish();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = tmem_slot;
+
+    if (warp == 0 && lane == 0) {
+        // ---------------- producer: the weights once, then per (tile, chunk) the three kw boxes
+        mbar_expect_tx(&wfull, (uint32_t)(chunks * M::kB));
+        for (int k = 0; k < chunks; ++k)
+            for (int t = 0; t < 27; ++t)
+                tma_load_2d(wsm + k * M::kBPad + t * COUT * 32, &a.wmap, k * 16, t * COUT, &wfull);
+        int it = 0;
+        bool ok = true;
+        for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+            int w0, h0, z0;
+            origin(tile, w0, h0, z0);
+            for (int k = 0; k < chunks; ++k, ++it) {
+                const int s = it % S;
+                if (it >= S && !mbar_wait(&empty[s], (uint32_t)(((it / S) - 1) & 1))) {
+                    ok = false;
+                    break;
+                }
+                uint8_t* st = ring + s * kBoxA;
+                mbar_expect_tx(&full[s], kBoxA);
+                for (int kw = 0; kw < 3; ++kw)
+                    tma_load_4d(st + kw * kBoxBytes, &a.xmap, k * 16, w0 + kw - 1, h0 - 1, z0 - 1, &full[s]);
+            }
+        }
+        if (!ok) bad = 1;
+    } else if (warp == 1 && lane == 0) {
+        // ---------------- MMA issuer: tile j accumulates into TMEM buffer j & 1
+        constexpr uint32_t idesc = idesc_bf16(COUT, 0, 0);
+        bool ok = mbar_wait(&wfull, 0);
+        int it = 0, j = 0;
+        for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x, ++j) {
+            const int b = j & 1;
+            // the epilogue has read out what tile j - 2 left in this buffer
+            if (j >= 2 && !mbar_wait(&acc_empty[b], (uint32_t)(((j >> 1) - 1) & 1))) {
+                ok = false;
+                break;
+            }
+            tc_fence_after();
+            for (int k = 0; k < chunks; ++k, ++it) {
+                const int s = it % S;
+                if (!mbar_wait(&full[s], (uint32_t)((it / S) & 1))) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                const uint8_t* st = ring + s * kBoxA;
+                const uint8_t* wk = wsm + k * M::kBPad;
+                // the output slices' accumulations alternate: consecutive UMMAs are independent;
+                // descriptors are the stage's plus constant offsets (the loops unroll): the
+                // issuing thread, not the tensor pipe, set the pace with descriptors built per UMMA
+                const uint64_t ad0 = smem_desc(st, 16, 256, LAYOUT_SW32);
+                const uint64_t bd0 = smem_desc(wk, 16, 256, LAYOUT_SW32);
+                const uint32_t d0 = tmem + (uint32_t)(b * kAcc);
+#pragma unroll
+                for (int t = 0; t < 27; ++t)
+#pragma unroll
+                    for (int zz = 0; zz < kBoxZ; ++zz) {
+                        const int kw = t % 3, kh = (t / 3) % 3, kd = t / 9;
+                        const uint64_t ad = desc_add(ad0, kw * kBoxBytes + (kh + (kBoxH + 2) * (kd + zz)) * 256);
+                        const uint64_t bd = desc_add(bd0, t * COUT * 32);
+                        umma_f16(d0 + (uint32_t)(zz * COUT), ad, bd, idesc, (k > 0 || t > 0) ? 1u : 0u);
+                    }
+                umma_commit(&empty[s]);  // the stage is free once these UMMAs have read it
+            }
+            if (!ok) break;
+            umma_commit(&acc_full[b]);   // tile j's accumulators are complete
+        }
+        if (!ok) bad = 1;
+    } else if (warp >= 2) {
+        // ---------------- epilogue: TMEM lane quarter (warp % 4) -> 32 output positions
+        const int q = warp & 3;
+        const int m = 32 * q + lane;  // GEMM row: w = m % 8, h = m / 8
+        int j = 0;
+        for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++j) {
+            const int b = j & 1;
+            const bool ready = __all_sync(0xffffffffu, mbar_wait(&acc_full[b], (uint32_t)((j >> 1) & 1)));
+            if (!ready) {
+                bad = 1;
+                break;
+            }
+            tc_fence_after();
+            int w0, h0, z0;
+            origin(tile, w0, h0, z0);
+            const int w = w0 + (m % kBoxW);
+            const int h = h0 + m / kBoxW;
+#pragma unroll 1
+            for (int zz = 0; zz < kBoxZ; ++zz) {
+                const size_t row = ((size_t)(z0 + zz) * a.H + h) * a.W + w;
+                __nv_bfloat16* o = a.out + row * COUT;
+                const __nv_bfloat16* mk = a.mask ? a.mask + row * COUT : nullptr;
+#pragma unroll
+                for (int c0 = 0; c0 < COUT; c0 += 16) {
+                    float v[16];
+                    tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(b * kAcc + zz * COUT + c0), v);
+                    __align__(16) __nv_bfloat16 ob[16];
+                    __align__(16) __nv_bfloat16 mb[16];
+                    if (mk) {
+                        *reinterpret_cast<uint4*>(mb) = *reinterpret_cast<const uint4*>(mk + c0);
+                        *reinterpret_cast<uint4*>(mb + 8) = *reinterpret_cast<const uint4*>(mk + c0 + 8);
+                    }
+#pragma unroll
+                    for (int i = 0; i < 16; ++i) {
+                        float x = v[i] + (a.bias ? a.bias[c0 + i] : 0.f);
+                        if (a.relu) x = fmaxf(x, 0.f);
+                        if (mk && !(__bfloat162float(mb[i]) > 0.f)) x = 0.f;
+                        ob[i] = __float2bfloat16_rn(x);
+                    }
+                    *reinterpret_cast<uint4*>(o + c0) = *reinterpret_cast<const uint4*>(ob);
+                    *reinterpret_cast<uint4*>(o + c0 + 8) = *reinterpret_cast<const uint4*>(ob + 8);
+                }
+            }
+            // this warp's lanes of buffer b are read: the MMA issuer may overwrite them
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&acc_empty[b]);
         }
     }
     tc_fence_before();
@@ -618,6 +818,49 @@ int launch_conv3_box_any(ConvArgs& a, int ntiles)
     return a.Cin == 16 ? launch_conv3_box<COUT, 1>(a, ntiles) : launch_conv3_box<COUT, 2>(a, ntiles);
 }
 
+// stages of the persistent kernel's input-box ring
+constexpr int kBoxPStages = 2;
+
+// whether the persistent kernel's shared memory (all weights resident) fits one CTA
+bool boxp_fits(int cout, int cin)
+{
+    const int chunks = cin / 16;
+    int b = 0;
+    switch (cout) {
+    case 16: b = BoxPSmem<16>::bytes(chunks, kBoxPStages); break;
+    case 32: b = BoxPSmem<32>::bytes(chunks, kBoxPStages); break;
+    case 48: b = BoxPSmem<48>::bytes(chunks, kBoxPStages); break;
+    case 64: b = BoxPSmem<64>::bytes(chunks, kBoxPStages); break;
+    default: return false;
+    }
+    return b <= 227 * 1024;
+}
+
+template <int COUT>
+int launch_conv3_boxp(ConvArgs& a, int ntiles)
+{
+    constexpr int S = kBoxPStages;
+    const int bytes = BoxPSmem<COUT>::bytes(a.Cin / 16, S);
+    // host-side setup once per shared-memory size (the launches of a network come back to back)
+    static int attr = 0, last_bytes = -1, slots = 0;
+    if (bytes > attr) {
+        RG_CHECK_CUDA(cudaFuncSetAttribute(k_conv3_boxp<COUT, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+        attr = bytes;
+    }
+    if (bytes != last_bytes) {
+        int per_sm = 0, dev = 0, sms = 0;
+        RG_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_conv3_boxp<COUT, S>, kConvThreads, bytes));
+        RG_CHECK_CUDA(cudaGetDevice(&dev));
+        RG_CHECK_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        slots = std::max(per_sm, 1) * sms;
+        last_bytes = bytes;
+    }
+    const int grid = std::min(ntiles, slots);
+    RG_TIMED(T_WS_CONV, (k_conv3_boxp<COUT, S><<<grid, kConvThreads, bytes, stream()>>>(a)));
+    RG_CHECK_LAUNCH();
+    return RG_OK;
+}
+
 template <int COUT>
 int launch_wgrad(WgradArgs& a, int grid)
 {
@@ -681,6 +924,15 @@ extern "C" int rg_ws_conv3(const rg_act* x, const void* weights, const float* bi
         a.relu = relu;
         a.err = err_dev;
         const int ntiles = a.tiles_w * a.tiles_h * a.tiles_z;
+        if (ws::boxp_fits(cout, x->c)) {
+            // persistent: weights resident, box loads, UMMAs and epilogues of consecutive tiles overlap
+            switch (cout) {
+            case 16: return ws::launch_conv3_boxp<16>(a, ntiles);
+            case 32: return ws::launch_conv3_boxp<32>(a, ntiles);
+            case 48: return ws::launch_conv3_boxp<48>(a, ntiles);
+            default: return ws::launch_conv3_boxp<64>(a, ntiles);
+            }
+        }
         switch (cout) {
         case 16: return ws::launch_conv3_box_any<16>(a, ntiles);
         case 32: return ws::launch_conv3_box_any<32>(a, ntiles);

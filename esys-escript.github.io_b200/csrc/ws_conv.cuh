@@ -154,6 +154,10 @@ __device__ __forceinline__ uint64_t smem_desc(const void* start, uint32_t lbo_by
     return d;
 }
 
+// the descriptor of the operand `bytes` (a multiple of 16) past the one of d: the start address
+// field holds the address >> 4, and shared-memory addresses stay far below its 14-bit range
+__device__ __forceinline__ uint64_t desc_add(uint64_t d, uint32_t bytes) { return d + (uint64_t)(bytes >> 4); }
+
 // instruction descriptor: bf16 x bf16 -> fp32, M = 128, N, operand majors (0 = K, 1 = MN)
 __host__ __device__ constexpr uint32_t idesc_bf16(int n, int a_mn_major, int b_mn_major)
 {

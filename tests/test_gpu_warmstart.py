@@ -35,6 +35,11 @@ def ref_conv(x, w27, b, relu, mask=None):
     (1, (64, 64, 64), 16, 16, True, False),
     (1, (8, 8, 8), 64, 64, False, True),
     (2, (16, 16, 16), 48, 112, True, False),
+    # the persistent kernel (weights resident, two TMEM accumulators): several tiles per CTA,
+    # two input chunks, two samples, 64 output channels
+    (1, (64, 64, 64), 32, 16, True, True),
+    (2, (32, 32, 16), 16, 32, False, False),
+    (1, (16, 16, 16), 32, 64, True, True),
 ])
 def test_conv3_matches_torch(cuda, n, dhw, cin, cout, relu, use_mask):
     torch.manual_seed(0)
