@@ -89,7 +89,7 @@ struct Workspace {
     int coef_cfg = -1;   // the same for the element-coefficient operator (kCoefCfg)
     bool coef_op = false;  // the current FP32 solve evaluates the operator from the coefficients
     int grid_upd32 = 0;  // kept for rg_solver_config: the FP32 iteration has no separate update kernel
-    double spmv_us[2] = {0, 0};  // tuner's time per launch of each SpMV configuration
+    double spmv_us[2][2] = {};   // tuner's time per launch of each configuration [coef_op][cfg]
 };
 
 namespace {
@@ -1860,7 +1860,8 @@ int tune_spmv(Matrix* m)
         slot = m->force_spmv >= 0 ? m->force_spmv : fallback;
         return RG_OK;
     }
-    w->spmv_us[0] = w->spmv_us[1] = 0.0;
+    double* us = w->spmv_us[coef ? 1 : 0];
+    us[0] = us[1] = 0.0;
     int rc = RG_OK;
     cudaEvent_t e0, e1;
     RG_CHECK_CUDA(cudaEventCreate(&e0));
@@ -1885,7 +1886,7 @@ int tune_spmv(Matrix* m)
         RG_CHECK_CUDA(cudaEventSynchronize(e1));
         float ms = 0;
         cudaEventElapsedTime(&ms, e0, e1);
-        w->spmv_us[cfg] = 1e3 * ms / 8;
+        us[cfg] = 1e3 * ms / 8;
         if (rc == RG_OK && ms < best) {
             best = ms;
             best_cfg = cfg;
@@ -2150,7 +2151,7 @@ int solve_f32(Matrix* m, const rg_solver_opts* o, OuterState& st, rg_diag& dg)
 int solver_config(const Matrix* m, int* spmv_cfg, int* update_grid, double* spmv_us)
 {
     if (spmv_us)
-        for (int c = 0; c < 2; ++c) spmv_us[c] = m->ws ? m->ws->spmv_us[c] : 0.0;
+        for (int c = 0; c < 2; ++c) spmv_us[c] = m->ws ? m->ws->spmv_us[m->ws->coef_op ? 1 : 0][c] : 0.0;
     if (spmv_cfg) *spmv_cfg = m->ws ? (m->ws->coef_op ? m->ws->coef_cfg : m->ws->spmv_cfg) : -1;
     if (update_grid) *update_grid = m->ws ? m->ws->grid_upd32 : 0;
     return RG_OK;

@@ -254,12 +254,14 @@ int rg_solve(rg_matrix* mat, const double* rhs, double* x, const rg_solver_opts*
 
 
 /* The FP32 path's configuration chosen at the matrix's first FP32_REFINE solve (no reference
-   counterpart; diagnostics and tests): spmv_config 0/1 = the pipeline of the fused FP32 PCG
-   iteration (one kernel per iteration: band SpMV, vector updates and one reduction) with 3
-   stages x 1 CTA per SM / 2 stages x 2 CTAs per SM (-1: not tuned yet); update_grid: 0 (the
-   iteration has no separate vector-update kernel); spmv_us (NULL or 2 entries): the tuner's
-   time per iteration of each configuration, 0 where not timed (a configuration whose shared
-   memory does not fit the grid's windows is not timed).  Any output pointer may be NULL. */
+   counterpart; diagnostics and tests), for the inner operator of the matrix's latest solve:
+   spmv_config 0/1 = the pipeline of the fused FP32 PCG iteration (one kernel per iteration:
+   operator product, vector updates and one reduction) with 3 stages x 1 CTA per SM / 2 stages
+   x 2 CTAs per SM on the band copy, 3 stages x 2 CTAs per SM / 2 stages x 2 CTAs per SM on the
+   element coefficients (-1: not tuned yet); update_grid: 0 (the iteration has no separate
+   vector-update kernel); spmv_us (NULL or 2 entries): the tuner's time per iteration of each
+   configuration, 0 where not timed (a configuration whose shared memory does not fit the
+   grid's windows is not timed).  Any output pointer may be NULL. */
 int rg_solver_config(const rg_matrix* mat, int* spmv_config, int* update_grid, double* spmv_us);
 
 /* Fixes the FP32 iteration configuration used from the next FP32_REFINE solve on (-1 restores
