@@ -599,7 +599,9 @@ int rg_solver_set_config(rg_matrix* mat, int spmv_config)
 
 int rg_test_wait_limit(int max_polls, int withhold_copies)
 {
-    return rg::set_wait_control(max_polls, withhold_copies);
+    const int rc = rg::set_wait_control(max_polls, withhold_copies);
+    if (rc) return rc;
+    return rg::ws::set_conv_wait_control(max_polls, withhold_copies);
 }
 
 int rg_solve(rg_matrix* mat, const double* rhs, double* x, const rg_solver_opts* opts, rg_diag* diag)

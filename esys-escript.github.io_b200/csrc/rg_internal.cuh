@@ -261,6 +261,10 @@ int solver_set_config(Matrix* m, int spmv_cfg);
 // poll limit of the band kernels' bounded waits (0: default) and whether their producer
 // withholds its copies (rg_test_wait_limit)
 int set_wait_control(int polls, int withhold);
+namespace ws {
+// the same test hook for the persistent convolution (ws_conv.cu)
+int set_conv_wait_control(int polls, int withhold);
+}  // namespace ws
 void free_workspace(Matrix* m);
 // hands the matrix's solver vectors to its domain for the next matrix there (one is kept; a
 // further one is freed), instead of freeing them: a fresh matrix on the same grid then

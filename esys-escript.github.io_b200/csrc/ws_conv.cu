@@ -337,6 +337,14 @@ __global__ void __launch_bounds__(kConvThreads) k_conv3_box(const __grid_constan
 // of the next tile, its UMMAs and the epilogue of the previous tile overlap (k_conv3_box runs
 // the three one after the other, once per CTA).  Every wait is bounded; a wait that runs out
 // sets the error flag and the CTA stops.
+// test hook of the persistent convolution's bounded waits (rg_test_wait_limit): a poll limit
+// (0: the default) and a switch that makes the producer issue no copies
+struct ConvWaitCtl {
+    int polls;
+    int withhold;
+};
+__device__ ConvWaitCtl g_conv_wait = {0, 0};
+
 template <int COUT>
 struct BoxPSmem {
     static constexpr int kB = 27 * COUT * 32;                 // one chunk's weight slices
@@ -360,6 +368,8 @@ __global__ void __launch_bounds__(kConvThreads) k_conv3_boxp(const __grid_consta
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int chunks = a.Cin / 16;
+    const ConvWaitCtl wc = g_conv_wait;
+    const int polls = wc.polls > 0 ? wc.polls : 1 << 22;
     const int ntiles = a.tiles_w * a.tiles_h * a.tiles_z;
     const int per_sample = a.D / kBoxZ;
     uint8_t* wsm = smem;                             // chunks x kBPad: the weights
@@ -397,7 +407,7 @@ __global__ void __launch_bounds__(kConvThreads) k_conv3_boxp(const __grid_consta
     tc_fence_after();
     const uint32_t tmem = tmem_slot;
 
-    if (warp == 0 && lane == 0) {
+    if (warp == 0 && lane == 0 && !wc.withhold) {
         // ---------------- producer: the weights once, then per (tile, chunk) the three kw boxes
         mbar_expect_tx(&wfull, (uint32_t)(chunks * M::kB));
         for (int k = 0; k < chunks; ++k)
@@ -410,7 +420,7 @@ __global__ void __launch_bounds__(kConvThreads) k_conv3_boxp(const __grid_consta
             origin(tile, w0, h0, z0);
             for (int k = 0; k < chunks; ++k, ++it) {
                 const int s = it % S;
-                if (it >= S && !mbar_wait(&empty[s], (uint32_t)(((it / S) - 1) & 1))) {
+                if (it >= S && !mbar_wait(&empty[s], (uint32_t)(((it / S) - 1) & 1), polls)) {
                     ok = false;
                     break;
                 }
@@ -424,19 +434,19 @@ __global__ void __launch_bounds__(kConvThreads) k_conv3_boxp(const __grid_consta
     } else if (warp == 1 && lane == 0) {
         // ---------------- MMA issuer: tile j accumulates into TMEM buffer j & 1
         constexpr uint32_t idesc = idesc_bf16(COUT, 0, 0);
-        bool ok = mbar_wait(&wfull, 0);
+        bool ok = mbar_wait(&wfull, 0, polls);
         int it = 0, j = 0;
         for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x, ++j) {
             const int b = j & 1;
             // the epilogue has read out what tile j - 2 left in this buffer
-            if (j >= 2 && !mbar_wait(&acc_empty[b], (uint32_t)(((j >> 1) - 1) & 1))) {
+            if (j >= 2 && !mbar_wait(&acc_empty[b], (uint32_t)(((j >> 1) - 1) & 1), polls)) {
                 ok = false;
                 break;
             }
             tc_fence_after();
             for (int k = 0; k < chunks; ++k, ++it) {
                 const int s = it % S;
-                if (!mbar_wait(&full[s], (uint32_t)((it / S) & 1))) {
+                if (!mbar_wait(&full[s], (uint32_t)((it / S) & 1), polls)) {
                     ok = false;
                     break;
                 }
@@ -471,7 +481,7 @@ __global__ void __launch_bounds__(kConvThreads) k_conv3_boxp(const __grid_consta
         int j = 0;
         for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++j) {
             const int b = j & 1;
-            const bool ready = __all_sync(0xffffffffu, mbar_wait(&acc_full[b], (uint32_t)((j >> 1) & 1)));
+            const bool ready = __all_sync(0xffffffffu, mbar_wait(&acc_full[b], (uint32_t)((j >> 1) & 1), polls));
             if (!ready) {
                 bad = 1;
                 break;
@@ -816,6 +826,14 @@ int launch_conv3_box_any(ConvArgs& a, int ntiles)
 {
     // one stage when there is one chunk (several CTAs per SM overlap instead), else two
     return a.Cin == 16 ? launch_conv3_box<COUT, 1>(a, ntiles) : launch_conv3_box<COUT, 2>(a, ntiles);
+}
+
+int set_conv_wait_control(int polls, int withhold)
+{
+    const ConvWaitCtl c = {polls, withhold ? 1 : 0};
+    RG_CHECK_CUDA(cudaDeviceSynchronize());  // no convolution may be running while it changes
+    RG_CHECK_CUDA(cudaMemcpyToSymbol(g_conv_wait, &c, sizeof(c)));
+    return RG_OK;
 }
 
 // stages of the persistent kernel's input-box ring

@@ -56,10 +56,10 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
     return ok != 0;
 }
 
-// bounded wait (about a second); false when it gave up
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity)
+// bounded wait (by default about a second); false when it gave up
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int polls = 1 << 22)
 {
-    for (int tries = 0; tries < (1 << 22); ++tries)
+    for (int tries = 0; tries < polls; ++tries)
         if (mbar_try_wait(bar, parity)) return true;
     return false;
 }

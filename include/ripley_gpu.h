@@ -270,14 +270,14 @@ int rg_solver_config(const rg_matrix* mat, int* spmv_config, int* update_grid, d
    reports them. */
 int rg_solver_set_config(rg_matrix* mat, int spmv_config);
 
-/* Test hook for the timeout path of the band SpMV kernels (no reference counterpart; paso
-   has no device waits).  max_polls > 0 caps the polls of each bounded wait of the
-   warp-specialised band kernels (FP32_REFINE, and FP64 with RG_LAYOUT_BAND); 0 restores the
-   default limit.  withhold_copies != 0 makes their producer issue no copies, so every
-   consumer wait runs out with nothing in flight: the solve then returns RG_TIMEOUT and the
-   matrix, its domain and the library stay usable.  Applies to all matrices on the current
-   device from the next launch on; it waits for the device to be idle first.  Not for use
-   in production code. */
+/* Test hook for the timeout path of the warp-specialised kernels (no reference counterpart;
+   paso has no device waits).  max_polls > 0 caps the polls of each bounded wait of the band
+   kernels (FP32_REFINE, and FP64 with RG_LAYOUT_BAND) and of the persistent convolution of
+   rg_ws_conv3; 0 restores the default limit.  withhold_copies != 0 makes their producers
+   issue no copies, so every wait runs out with nothing in flight: a solve then returns
+   RG_TIMEOUT, a convolution sets its device error flag, and the matrix, its domain and the
+   library stay usable.  Applies to all matrices on the current device from the next launch
+   on; it waits for the device to be idle first.  Not for use in production code. */
 int rg_test_wait_limit(int max_polls, int withhold_copies);
 
 /* ---- batched solves (no reference counterpart: many independent systems at once) ------- */

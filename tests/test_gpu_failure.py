@@ -2,7 +2,9 @@
 kernels are made to run out (their producer withholds every copy, so nothing is ever in
 flight), the solve must return RG_TIMEOUT, and the next solve on the same matrix and domain
 must match the oracle, i.e. nothing the interrupted launch left behind (the grid-reduction
-counter, the device scalars, the captured iteration graphs) leaks into later work.
+counter, the device scalars, the captured iteration graphs) leaks into later work.  The same
+hook makes the persistent tcgen05 convolution's waits run out: it must set its device error
+flag, free its tensor memory, and the next convolution must be correct.
 
 The paso status mapping the library follows is paso/src/solve.cpp:119-142 (a solver status
 becomes an exception); RG_TIMEOUT has no paso counterpart because paso has no device waits.
@@ -93,3 +95,38 @@ def test_wait_limit_arguments_are_checked(cuda):
     lib = R.lib()
     assert lib.rg_test_wait_limit(-1, 0) == L.RG_INVALID_ARG
     L.check(lib.rg_test_wait_limit(0, 0))
+
+
+def test_conv_wait_timeout_sets_error_flag_and_recovers(cuda):
+    """The persistent tcgen05 convolution (64^3, 16 -> 16 channels) with its producer withholding
+    every copy: the MMA issuer's and the epilogue warps' bounded waits run out (nothing is in
+    flight, no UMMA is issued), the kernel releases its tensor memory and sets the device error
+    flag; with the limits restored the next convolution matches the fp32 reference."""
+    import torch.nn.functional as F
+    from esys_b200 import warmstart as W
+    torch.manual_seed(1)
+    d = 64
+    x = W.new_act(1, d, d, d, 16)
+    xv = torch.randn(1, d, d, d, 16, device="cuda").to(torch.bfloat16)
+    W.interior(x).copy_(xv)
+    wt = (torch.randn(27, 16, 16, device="cuda") * 0.05).to(torch.bfloat16).contiguous()
+    b = torch.randn(16, device="cuda")
+    y = W.new_act(1, d, d, d, 16)
+    lib = R.lib()
+    err = W.DeviceError()
+    L.check(lib.rg_test_wait_limit(64, 1))
+    try:
+        W.conv3(x, wt, b, y, relu=True, err=err)
+        torch.cuda.synchronize()
+        with pytest.raises(L.RipleyGPUError):
+            err.check()
+    finally:
+        L.check(lib.rg_test_wait_limit(0, 0))
+    ok = W.DeviceError()
+    W.conv3(x, wt, b, y, relu=True, err=ok)
+    torch.cuda.synchronize()
+    ok.check()
+    w5 = wt.float().cpu().reshape(3, 3, 3, 16, 16).permute(3, 4, 0, 1, 2)  # (Cout, Cin, kd, kh, kw)
+    ref = torch.relu(F.conv3d(xv.float().cpu().permute(0, 4, 1, 2, 3), w5, b.cpu(), padding=1)).permute(0, 2, 3, 4, 1)
+    got = W.interior(y).float().cpu()
+    assert (got - ref).abs().max().item() <= 2e-2 * ref.abs().max().item()
