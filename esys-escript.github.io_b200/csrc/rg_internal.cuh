@@ -289,9 +289,6 @@ int coef_on_constraint(Matrix* m, const double* q);                        // in
 // whether the record describes the values (reads the device flag: synchronises the stream)
 int coef_usable(Matrix* m, bool* usable);
 void free_coef(Matrix* m);
-// l2 norm of b - A x with the matrix's values as they are (unbalance: undo an in-place
-// balancing on the fly); synchronises the stream
-int residual_l2(Matrix* m, const double* b, const double* x, bool unbalance, double* l2);
 
 }  // namespace rg
 

@@ -35,22 +35,6 @@ int ensure_residual_scratch(Matrix* m)
     return RG_OK;
 }
 
-int residual_l2(Matrix* m, const double* b, const double* x, bool unbalance, double* l2)
-{
-    int rc = ensure_residual_scratch(m);
-    if (rc) return rc;
-    const Domain* d = m->dom;
-    RG_TIMED(T_NORMS, (residual::k_residual_norms<<<residual::grid(d->n), residual::kThreads, 0, stream()>>>(
-                          d->n, d->ptr, d->idx, m->val, unbalance && m->balanced ? m->bv : nullptr, b, x,
-                          ReduceBuf{m->rs->partials, m->rs->counter}, m->rs->out)));
-    RG_CHECK_LAUNCH();
-    double h[2];
-    RG_CHECK_CUDA(cudaMemcpyAsync(h, m->rs->out, sizeof(h), cudaMemcpyDeviceToHost, stream()));
-    RG_CHECK_CUDA(cudaStreamSynchronize(stream()));
-    *l2 = std::sqrt(h[0]);
-    return RG_OK;
-}
-
 }  // namespace rg
 
 using namespace rg;

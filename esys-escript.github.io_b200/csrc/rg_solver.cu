@@ -1273,18 +1273,30 @@ __global__ void __launch_bounds__(kThreads) k_f32_cg_seed_coef(const __grid_cons
     }
 }
 
+// zb_i = bv_i x_i, 0 on the nodes the constraint fixes (the sign bit of khat): the vector
+// k_cheb_step_coef gathers
+__global__ void k_mask_scale(int64_t n, const float* __restrict__ khat, const double* __restrict__ bv,
+                             const double* __restrict__ x, double* __restrict__ zb)
+{
+    for (int64_t i = gtid(); i < n; i += gstride())
+        zb[i] = (__float_as_uint(khat[i]) >> 31) ? 0.0 : bv[i] * x[i];
+}
+
 // k_cheb_step on the element-coefficient operator (when the FP32 solve evaluates its operator
 // from the coefficients there is no band copy): the balanced operator is bv_i sum_j a_ij bv_j
 // x_j with a_ij from kappa (FP32 coefficients, FP64 vectors); rows and columns of fixed nodes
-// (the sign bit of khat) are those of the identity.
+// (the sign bit of khat) are those of the identity.  The neighbours' bv_j x_j come masked in
+// zx (k_mask_scale, then each step's zy for the next): one gathered load per neighbour.
 template <int NB>
 __global__ void __launch_bounds__(kThreads) k_cheb_step_coef(const __grid_constant__ CgArgs ca,
                                                              const float* __restrict__ khat,
                                                              const double* __restrict__ bv,
                                                              const double* __restrict__ dinv,
                                                              const double* __restrict__ x,
+                                                             const double* __restrict__ zx,
                                                              const double* __restrict__ bb, double c_d, double c_r,
-                                                             double* __restrict__ d, double* __restrict__ y)
+                                                             double* __restrict__ d, double* __restrict__ y,
+                                                             double* __restrict__ zy)
 {
     constexpr int NK = NB == 27 ? 8 : 4;
     const int64_t n = ca.n;
@@ -1308,13 +1320,15 @@ __global__ void __launch_bounds__(kThreads) k_cheb_step_coef(const __grid_consta
             for (int b = 0; b < NB; ++b) {
                 const float c = coef_at<NB>(cr, ca.T, b);
                 const int64_t j = min(max(i + ca.off[b], (int64_t)0), n - 1);
-                if (c != 0.f && (__float_as_uint(__ldg(khat + j)) >> 31) == 0) acc = fma((double)c, bv[j] * x[j], acc);
+                if (c != 0.f) acc = fma((double)c, __ldg(zx + j), acc);
             }
             acc *= bv[i];
         }
         const double dn = c_d * (c_d != 0.0 ? d[i] : 0.0) + c_r * dinv[i] * (bb[i] - acc);
         d[i] = dn;
-        y[i] = x[i] + dn;
+        const double yi = x[i] + dn;
+        y[i] = yi;
+        zy[i] = fixed ? 0.0 : bv[i] * yi;
     }
 }
 
@@ -2398,14 +2412,24 @@ int solve_impl(Matrix* m, const double* rhs, double* x, const rg_solver_opts* o,
                         rho = rho_n;
                     }
                     if (w->coef_op) {
-                        // the operator from the element coefficients (no band copy on this path)
+                        // the operator from the element coefficients (no band copy on this path);
+                        // the masked bv x of the source ping-pongs between p and q
                         const CgArgs ca = cg_args(dm);
+                        double* zs = (k & 1) ? w->q : w->p;
+                        double* zd = (k & 1) ? w->p : w->q;
+                        if (k == 0) {
+                            RG_TIMED(T_VECTOR, (k_mask_scale<<<eg, kThreads, 0, stream()>>>(n, m->coef.khat, m->bv, src,
+                                                                                            zs)));
+                            RG_CHECK_LAUNCH();
+                        }
                         if (dm->nbands == 27)
                             RG_TIMED(T_VECTOR, (k_cheb_step_coef<27><<<eg, kThreads, 0, stream()>>>(
-                                                   ca, m->coef.khat, m->bv, m->dinv, src, w->bb, c_d, c_r, w->z, dst)));
+                                                   ca, m->coef.khat, m->bv, m->dinv, src, zs, w->bb, c_d, c_r, w->z,
+                                                   dst, zd)));
                         else
                             RG_TIMED(T_VECTOR, (k_cheb_step_coef<9><<<eg, kThreads, 0, stream()>>>(
-                                                   ca, m->coef.khat, m->bv, m->dinv, src, w->bb, c_d, c_r, w->z, dst)));
+                                                   ca, m->coef.khat, m->bv, m->dinv, src, zs, w->bb, c_d, c_r, w->z,
+                                                   dst, zd)));
                     } else if (m->band32 && m->band32_ok) {
                         // the FP32 band copy streams a third of the bytes of the FP64 CSR
                         TmaBandArgs ta{};
@@ -2428,8 +2452,12 @@ int solve_impl(Matrix* m, const double* rhs, double* x, const rg_solver_opts* o,
                         cudaMemcpyAsync(w->x, w->x2, sizeof(double) * n, cudaMemcpyDeviceToDevice, stream()));
             }
             // a guess whose residual exceeds the right hand side's is worse than zero: drop it
-            double r0;
-            if ((rc = residual_l2(m, w->bb, w->x, false, &r0))) return rc;
+            // (the residual kernel of the outer test: r = B b - A x with its norms)
+            RG_TIMED(T_NORMS, (k_residual<<<w->grid_rows, kThreads, 0, stream()>>>(
+                                  n, m->dom->ptr, m->dom->idx, m->val, w->x, w->bb, w->r, rbuf(w), w->s)));
+            RG_CHECK_LAUNCH();
+            if ((rc = read_scal(w))) return rc;
+            const double r0 = std::sqrt(w->hs->n2);
             dg.guess_residual = r0;
             if (!(r0 <= st.n2b)) {
                 RG_CHECK_CUDA(cudaMemsetAsync(w->x, 0, sizeof(double) * n, stream()));
