@@ -293,23 +293,26 @@ def run_ours(args):
         cy = cY if Y_dev is None else L.rg_coef(Y_dev.data_ptr(), L.RG_COEF_EXPANDED)
         qq = q_d if q_dev is None else q_dev
         if o is learned:
-            # the network (tensor-core convolutions) runs on a second stream while the
-            # assembly (memory-bound) runs on the main one; the solve waits for both.
-            # network input: kappa (A's first diagonal entry) and Y per element
+            side.wait_stream(stream)  # the inputs are on the main stream
+        # the assembly (memory-bound) is queued first on the main stream, so that it runs
+        # while the host queues the network's launches on the second stream
+        L.set_stream_from_torch()
+        L.check(lib.rg_matrix_reset(mat))
+        rhs.zero_()
+        L.check(lib.rg_assemble_single(mat, C.c_void_p(rhs.data_ptr()), C.byref(ca), C.byref(empty),
+                                       C.byref(empty), C.byref(empty), C.byref(empty), C.byref(cy)))
+        L.check(lib.rg_insert_constraint(mat, C.c_void_p(rhs.data_ptr()), C.c_void_p(qq.data_ptr()), None, 0))
+        if o is learned:
+            # the network (tensor-core convolutions) on the second stream; the solve waits for
+            # both.  Network input: kappa (A's first diagonal entry) and Y per element
             Ad = A_d if A_dev is None else A_dev
             Yd = Y_d if Y_dev is None else Y_dev
-            side.wait_stream(stream)
             with torch.cuda.stream(side):
                 L.set_stream_from_torch()
                 L.check(lib.rg_ws_element_fields(C.c_void_p(Ad.data_ptr()), 9, C.c_void_p(Yd.data_ptr()), 8,
                                                  nel, C.c_void_p(kap32.data_ptr()), C.c_void_p(y32.data_ptr())))
                 warm.guess(kap32, y32, (ne, ne, ne), q=qq, out=guess)
             L.set_stream_from_torch()  # library work back on the main stream
-        L.check(lib.rg_matrix_reset(mat))
-        rhs.zero_()
-        L.check(lib.rg_assemble_single(mat, C.c_void_p(rhs.data_ptr()), C.byref(ca), C.byref(empty),
-                                       C.byref(empty), C.byref(empty), C.byref(empty), C.byref(cy)))
-        L.check(lib.rg_insert_constraint(mat, C.c_void_p(rhs.data_ptr()), C.c_void_p(qq.data_ptr()), None, 0))
         d = L.rg_diag()
         if o is learned:
             stream.wait_stream(side)
