@@ -1,5 +1,6 @@
 """Multi-process paths of bench.py on CPU (gloo, world size 2): the job time is the maximum
-over ranks, and the reference arm runs on rank 0 only."""
+over ranks, and the reference arm runs on rank 0 only (rank 1 exits without output, rank 0
+prints the job's one line)."""
 import datetime
 import os
 import socket
@@ -49,3 +50,20 @@ def test_reference_arm_other_ranks_exit_without_work():
                        env=env, capture_output=True, text=True, timeout=120)
     assert r.returncode == 0
     assert r.stdout.strip() == ""
+
+
+def test_reference_arm_rank0_prints_one_line_for_the_job():
+    """Rank 0 of a 2-rank job runs the reference's CPU path alone (small grid here) and prints
+    the one JSON line, with the job's GPU count."""
+    import json
+    env = dict(os.environ, RANK="0", WORLD_SIZE="2", LOCAL_RANK="0")
+    r = subprocess.run([sys.executable, os.path.join(REPO, "bench.py"), "--impl", "reference", "--gpus", "2",
+                        "--ne", "12", "--steps", "1", "--warmup", "3"],
+                       env=env, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [l for l in r.stdout.splitlines() if l.strip()]
+    assert len(lines) == 1
+    out = json.loads(lines[0])
+    assert out["impl"] == "reference" and out["n_gpus"] == 2 and out["higher_is_better"] is False
+    assert out["value"] > 0 and out["config"]["ne"] == [12, 12, 12] and out["config"]["iterations"] > 0
+    assert out["e2e"]["value"] == out["value"] and out["cpu_baseline"]["kind"] in ("reference", "port")
