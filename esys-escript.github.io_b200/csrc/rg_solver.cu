@@ -1099,8 +1099,8 @@ __global__ void __launch_bounds__(kTile + 32, kCtas) k_f32_cg(const float* __res
         }
     } else {
         // ---------------- consumers: row i0 + t of every tile
-        for (int64_t k = 0; k < my_tiles; ++k) {
-            const int st = (int)(k % kStages);
+        for (int k = 0; k < (int)my_tiles; ++k) {  // (32-bit tile count: cheaper stage arithmetic)
+            const int st = k % kStages;
             const int64_t i0 = tile_of(k) * (int64_t)kTile;
             const int64_t i = i0 + t;
             // the correction is only read and written by this row: load it while the stage fills
@@ -1109,7 +1109,7 @@ __global__ void __launch_bounds__(kTile + 32, kCtas) k_f32_cg(const float* __res
                 bad = 1;
                 break;
             }
-            const float* bs = smem + (size_t)st * stage_floats;
+            const float* bs = smem + st * stage_floats;
             const float4* win = reinterpret_cast<const float4*>(bs + kmat);
             // this row's coefficients: formed from the element values (COEF), or read from the
             // band block where they are used
@@ -1201,10 +1201,10 @@ __global__ void __launch_bounds__(kTile + 32, kCtas) k_f32_cg(const float* __res
                 const double du = un, dd = diag, ds = (double)spn * dd;
                 v[0] += dd * du * du;
                 // the segment's stopping norm: |r| of the balanced residual (band copy); for the
-                // unbalanced coefficient operator r.u = r.D^-1 r, which paso's balancing leaves
-                // unchanged and which is |B r|^2 when the balance vector is D^-1/2 (diagonally
-                // dominant rows)
-                v[1] += COEF ? dd * du * du : (dd * du) * (dd * du);
+                // unbalanced coefficient operator r.u = r.D^-1 r (= v[0], copied after the
+                // reduction), which paso's balancing leaves unchanged and which is |B r|^2 when
+                // the balance vector is D^-1/2 (diagonally dominant rows)
+                if (!COEF) v[1] += (dd * du) * (dd * du);
                 v[2] += du * (double)w;
                 v[3] += du * ds;
                 v[4] += (double)pn * (double)w;
@@ -1226,7 +1226,10 @@ __global__ void __launch_bounds__(kTile + 32, kCtas) k_f32_cg(const float* __res
         for (int j = 0; j < 6; ++j) v[j] = 0.0;
     }
     double tt[6];
-    if (grid_reduce<6>(v, rb, tt) && threadIdx.x == 0) cg_scalars(s, tt, mode);
+    if (grid_reduce<6>(v, rb, tt) && threadIdx.x == 0) {
+        if (COEF) tt[1] = tt[0];
+        cg_scalars(s, tt, mode);
+    }
 }
 
 // The element-coefficient operator's seed: the balanced FP64 residual is unbalanced (r =
